@@ -1,0 +1,237 @@
+"""B200-native multishift QZ behind the PDHGEQZ interface.
+
+Host-side mirror of the reference's operator interface
+(``src/pdhgeqz/PDHGEQZ.f:15-31``).  All numerical work runs in the CUDA
+library ``libb200qz.so`` built next to this file (``build.py``); importing
+this module does not need a GPU, but every solve does and fails loudly
+without the library or a device.
+
+Entry points
+------------
+``pdhgeqz(job, compq, compz, H, T, Q, Z, ilo=1, ihi=None, nb=64)``
+    Same argument meaning and INFO codes as the Fortran routine on a 1x1
+    grid; arrays are Fortran-ordered numpy float64 and are overwritten in
+    place.  Goes through the exported ``pdhgeqz_`` symbol (the drop-in).
+``Solver`` (device context)
+    ``solve_device`` works on CUDA buffers that already live in HBM
+    (column-major, one leading dimension), ``solve_host`` copies numpy
+    arrays in and out.
+"""
+from __future__ import annotations
+
+import ctypes
+import importlib.util
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libb200qz.so")
+
+_lib = None
+
+
+def _pencils():
+    name = "gevp_pdhgeqz_b200_pencils"
+    if name in sys.modules:
+        return sys.modules[name]
+    spec = importlib.util.spec_from_file_location(name, os.path.join(HERE, "pencils.py"))
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+pencils = _pencils()
+
+_i = ctypes.c_int
+_d = ctypes.c_double
+_pd = ctypes.POINTER(ctypes.c_double)
+_pi = ctypes.POINTER(ctypes.c_int)
+_vp = ctypes.c_void_p
+_c = ctypes.c_char
+
+EXPORTS = (
+    "pdhgeqz_", "kkqzconf_", "b200qz_create", "b200qz_destroy", "b200qz_solve_dev",
+    "b200qz_solve_host", "b200qz_get_stats", "b200qz_set_params", "b200qz_aed_window",
+    "b200qz_chase_window", "b200qz_update",
+)
+
+STAT_NAMES = ("seconds", "iters", "aeds", "aed_deflations", "sweeps", "chains", "windows",
+              "endgames", "inf_steps", "shifts", "update_flops", "window_bytes")
+
+
+def lib() -> ctypes.CDLL:
+    """Load libb200qz.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(
+            "libb200qz.so is missing: run `python gevp-pdhgeqz_b200/build.py` "
+            "(there is no CPU fallback)")
+    L = ctypes.CDLL(LIB_PATH)
+    L.pdhgeqz_.restype = None
+    L.pdhgeqz_.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, _pi, _pi, _pi,
+                           _pd, _pi, _pd, _pi, _pd, _pd, _pd, _pd, _pi, _pd, _pi, _pd, _pi, _pi, _pi,
+                           _pi, ctypes.c_size_t, ctypes.c_size_t, ctypes.c_size_t]
+    L.kkqzconf_.restype = None
+    L.kkqzconf_.argtypes = [_pd]
+    L.b200qz_create.restype = _i
+    L.b200qz_create.argtypes = [ctypes.POINTER(_vp), _i]
+    L.b200qz_destroy.restype = None
+    L.b200qz_destroy.argtypes = [_vp]
+    L.b200qz_solve_dev.restype = _i
+    L.b200qz_solve_dev.argtypes = [_vp, _c, _c, _c, _i, _i, _i, _vp, _vp, _vp, _vp, _i, _vp, _vp, _vp]
+    L.b200qz_solve_host.restype = _i
+    L.b200qz_solve_host.argtypes = [_vp, _c, _c, _c, _i, _i, _i, _pd, _i, _pd, _i, _pd, _i, _pd, _i,
+                                    _pd, _pd, _pd]
+    L.b200qz_get_stats.restype = _i
+    L.b200qz_get_stats.argtypes = [_vp, _pd, _i]
+    L.b200qz_set_params.restype = _i
+    L.b200qz_set_params.argtypes = [_vp, _i, _i, _i, _i, _i, _i]
+    L.b200qz_aed_window.restype = _i
+    L.b200qz_aed_window.argtypes = [_vp, _vp, _vp, _i, _i, _i, _i, _vp, _vp, _vp, _pi]
+    L.b200qz_chase_window.restype = _i
+    L.b200qz_chase_window.argtypes = [_vp, _vp, _vp, _i, _i, _i, _i, _pi, _pd, _i, _i, _vp, _vp]
+    L.b200qz_update.restype = _i
+    L.b200qz_update.argtypes = [_vp, _c, _vp, _i, _i, _i, _i, _vp, _i, _i]
+    _lib = L
+    return L
+
+
+def _p(a: np.ndarray):
+    return a.ctypes.data_as(_pd)
+
+
+def _ip(v: int):
+    return ctypes.byref(ctypes.c_int(int(v)))
+
+
+def descriptor(n: int, nb: int, lld: int, ctxt: int = 0) -> np.ndarray:
+    """ScaLAPACK array descriptor of a full n x n matrix on a 1x1 grid:
+    [DTYPE=1, CTXT, M, N, MB, NB, RSRC=0, CSRC=0, LLD]."""
+    return np.array([1, ctxt, n, n, nb, nb, 0, 0, max(1, lld)], dtype=np.int32)
+
+
+def kkqzconf(eps: float = np.finfo(np.float64).eps) -> None:
+    """Accepted no-op (see include/b200qz.h)."""
+    lib().kkqzconf_(ctypes.byref(ctypes.c_double(eps)))
+
+
+def pdhgeqz(job, compq, compz, H, T, Q=None, Z=None, ilo=1, ihi=None, nb=64,
+            ldwork=None, liwork=None, descs=None):
+    """Call the ``pdhgeqz_`` drop-in exactly as a Fortran caller would.
+
+    H, T (and Q, Z when COMPQ/COMPZ are not 'N') are Fortran-ordered float64
+    numpy arrays, overwritten in place.  Returns (alphar, alphai, beta, info);
+    with ldwork == -1 or liwork == -1 the workspace sizes come back in
+    place of alphar/alphai as (dwork[0], iwork[0])."""
+    L = lib()
+    n = H.shape[0]
+    if ihi is None:
+        ihi = n
+    for nm, a in (("H", H), ("T", T), ("Q", Q), ("Z", Z)):
+        if a is not None and not (a.dtype == np.float64 and a.flags.f_contiguous):
+            raise ValueError("%s must be a Fortran-ordered float64 array" % nm)
+    Qa = Q if Q is not None else np.zeros((1, 1), order="F")
+    Za = Z if Z is not None else np.zeros((1, 1), order="F")
+    if descs is None:
+        descs = [descriptor(n, nb, a.shape[0]) for a in (H, T, Qa, Za)]
+    ar = np.zeros(max(1, n))
+    ai = np.zeros(max(1, n))
+    be = np.zeros(max(1, n))
+    if ldwork is None:
+        ldwork = max(1, n * nb)
+    if liwork is None:
+        liwork = max(1, 2 * n)
+    dwork = np.zeros(max(1, ldwork if ldwork > 0 else 1))
+    iwork = np.zeros(max(1, liwork if liwork > 0 else 1), dtype=np.int32)
+    info = ctypes.c_int(0)
+    dp = [d.ctypes.data_as(_pi) for d in descs]
+    L.pdhgeqz_(job.encode(), compq.encode(), compz.encode(), _ip(n), _ip(ilo), _ip(ihi),
+               _p(H), dp[0], _p(T), dp[1], _p(ar), _p(ai), _p(be), _p(Qa), dp[2], _p(Za), dp[3],
+               _p(dwork), _ip(ldwork), iwork.ctypes.data_as(_pi), _ip(liwork), ctypes.byref(info),
+               1, 1, 1)
+    if ldwork == -1 or liwork == -1:
+        return dwork[0], iwork[0], None, info.value
+    return ar[:n], ai[:n], be[:n], info.value
+
+
+class Solver:
+    """A device context (stream + workspace) of the CUDA solver."""
+
+    def __init__(self, device: int = 0):
+        L = lib()
+        h = _vp()
+        rc = L.b200qz_create(ctypes.byref(h), int(device))
+        if rc != 0:
+            raise RuntimeError("b200qz_create failed with CUDA error %d" % rc)
+        self._h = h
+        self.device = device
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().b200qz_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def set_params(self, nw_max=-1, w_chase=-1, nmin=-1, nibble=-1, ns_max=-1, maxit_factor=-1):
+        rc = lib().b200qz_set_params(self._h, nw_max, w_chase, nmin, nibble, ns_max, maxit_factor)
+        if rc != 0:
+            raise ValueError("b200qz_set_params: bad argument %d" % -rc)
+
+    def stats(self) -> dict:
+        out = np.zeros(len(STAT_NAMES))
+        k = lib().b200qz_get_stats(self._h, _p(out), len(STAT_NAMES))
+        return dict(zip(STAT_NAMES[:k], out[:k].tolist()))
+
+    def solve_device(self, h_ptr, t_ptr, q_ptr, z_ptr, ld, n, ar_ptr, ai_ptr, be_ptr,
+                     job="S", compq="I", compz="I", ilo=1, ihi=None) -> int:
+        """Solve on column-major device buffers given as integer pointers
+        (e.g. ``tensor.data_ptr()``).  Returns INFO."""
+        if ihi is None:
+            ihi = n
+        return lib().b200qz_solve_dev(self._h, job.encode(), compq.encode(), compz.encode(), n, ilo, ihi,
+                                      _vp(h_ptr), _vp(t_ptr), _vp(q_ptr), _vp(z_ptr), ld,
+                                      _vp(ar_ptr), _vp(ai_ptr), _vp(be_ptr))
+
+    def solve_host(self, H, T, Q=None, Z=None, job="S", compq="I", compz="I", ilo=1, ihi=None):
+        """Host-array solve (copies in and out).  Returns (alphar, alphai, beta, info)."""
+        n = H.shape[0]
+        if ihi is None:
+            ihi = n
+        Qa = Q if Q is not None else np.zeros((max(1, n), 1), order="F")
+        Za = Z if Z is not None else np.zeros((max(1, n), 1), order="F")
+        ar = np.zeros(n)
+        ai = np.zeros(n)
+        be = np.zeros(n)
+        info = lib().b200qz_solve_host(self._h, job.encode(), compq.encode(), compz.encode(), n, ilo, ihi,
+                                       _p(H), H.shape[0], _p(T), T.shape[0], _p(Qa), Qa.shape[0], _p(Za),
+                                       Za.shape[0], _p(ar), _p(ai), _p(be))
+        return ar, ai, be, info
+
+
+def solve(H, T, job="S", compq="I", compz="I", device=0):
+    """Convenience: copy, solve on the GPU, return (S, P, Q, Z, alphar, alphai, beta, info)."""
+    n = H.shape[0]
+    S = np.array(H, dtype=np.float64, order="F", copy=True)
+    P = np.array(T, dtype=np.float64, order="F", copy=True)
+    Q = np.eye(n, order="F")
+    Z = np.eye(n, order="F")
+    s = Solver(device)
+    try:
+        ar, ai, be, info = s.solve_host(S, P, Q, Z, job=job, compq=compq, compz=compz)
+    finally:
+        s.close()
+    return S, P, Q, Z, ar, ai, be, info

@@ -1,0 +1,465 @@
+// C-ABI of the B200 multishift QZ: context, device backend of the QZ
+// iteration, and the PDHGEQZ-compatible drop-in.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cctype>
+#include <cfloat>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+
+#include "../../include/b200qz.h"
+#include "kernels.h"
+#include "qz_solver.h"
+
+using namespace qz;
+
+namespace {
+constexpr int kAedMax = 512;  // largest AED / small-solve window supported
+}
+
+struct b200qz_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  double* Ua = nullptr;  // AED window factors (kAedMax^2)
+  double* Va = nullptr;
+  double* Uc = nullptr;  // chase / zero-chase window factors
+  double* Vc = nullptr;
+  double* shifts = nullptr;    // 3*kAedMax
+  double* gscratch = nullptr;  // 2*kAedMax^2 (windows above the smem limit)
+  double* norms = nullptr;     // 2
+  int* dinfo = nullptr;        // 8 ints
+  int* hinfo = nullptr;        // pinned mirror
+  double* hshifts = nullptr;   // pinned 3*kAedMax
+  double* hnorms = nullptr;    // pinned 2
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  SolveParams params;
+  SolveStats stats;
+  double seconds = 0.0;
+  int ka = 0;  // size of the AED factors in Ua/Va
+  int kc = 0;  // size of the chase factors in Uc/Vc
+  cudaError_t err = cudaSuccess;
+};
+
+namespace {
+
+#define QZ_CK(x)                                 \
+  do {                                           \
+    cudaError_t e_ = (x);                        \
+    if (e_ != cudaSuccess) {                     \
+      if (c->err == cudaSuccess) c->err = e_;    \
+    }                                            \
+  } while (0)
+
+// Device backend of qz_iterate (see qz_solver.h for the interface).
+struct GpuBackend {
+  b200qz_ctx* c;
+  double *H, *T, *Q, *Z;
+  int64_t ld;
+  int n;
+  bool wantq, wantz;
+  Tol tol;
+
+  void scan(int ifirst, int kbot, int* out) {
+    launch_scan(c->stream, H, T, ld, ifirst, kbot, tol, c->dinfo);
+    QZ_CK(cudaMemcpyAsync(c->hinfo, c->dinfo, 4 * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    QZ_CK(cudaStreamSynchronize(c->stream));
+    if (c->err != cudaSuccess) { out[0] = ifirst; out[1] = 0; out[2] = -1; out[3] = -1; return; }
+    for (int i = 0; i < 4; ++i) out[i] = c->hinfo[i];
+  }
+  void aed(int ktop, int kwtop, int kbot, int* info3, double* sh) {
+    int nw = kbot - kwtop + 1;
+    launch_aed(c->stream, H, T, ld, ktop, kwtop, nw, tol, c->Ua, c->Va, c->shifts, c->dinfo + 4, c->gscratch);
+    QZ_CK(cudaMemcpyAsync(c->hinfo + 4, c->dinfo + 4, 3 * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    QZ_CK(cudaMemcpyAsync(c->hshifts, c->shifts, 3 * nw * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    QZ_CK(cudaStreamSynchronize(c->stream));
+    c->ka = nw;
+    if (c->err != cudaSuccess) { info3[0] = nw; info3[1] = 1; info3[2] = 0; return; }
+    info3[0] = c->hinfo[4];
+    info3[1] = c->hinfo[5];
+    info3[2] = c->hinfo[6];
+    int m = std::min(info3[0], nw);
+    for (int i = 0; i < m; ++i) {
+      sh[i] = c->hshifts[i];
+      sh[m + i] = c->hshifts[nw + i];
+      sh[2 * m + i] = c->hshifts[2 * nw + i];
+    }
+    c->stats.win_bytes += 2.0 * 2.0 * 8.0 * nw * nw + 2.0 * 8.0 * nw * nw;
+  }
+  void chase(int w, int wk, int last, const Bulge* bl, int nb, int tmax) {
+    launch_chase(c->stream, H, T, ld, w, wk, last, bl, nb, tmax, c->Uc, c->Vc);
+    c->kc = wk;
+    c->stats.win_bytes += 2.0 * 2.0 * 8.0 * wk * wk + 2.0 * 8.0 * wk * wk;
+  }
+  void inf_window(int w, int wk, int top, int jz, int stop, bool deflate) {
+    launch_inf(c->stream, H, T, ld, w, wk, top, jz, stop, deflate ? 1 : 0, c->Uc, c->Vc);
+    c->kc = wk;
+    c->stats.win_bytes += 2.0 * 2.0 * 8.0 * wk * wk + 2.0 * 8.0 * wk * wk;
+  }
+  void inf_top(int f) { launch_inf_top(c->stream, H, T, Q, ld, n, f, wantq ? 1 : 0); }
+  // off-diagonal updates with the factors of the last window kernel
+  void update(int w, int wk, int which) {
+    const double* U = which == 0 ? c->Ua : c->Uc;
+    const double* V = which == 0 ? c->Va : c->Vc;
+    int tile = update_tile(wk);
+    UpdBatch L;
+    L.k = wk;
+    L.njobs = 0;
+    int right_len = n - (w + wk);
+    if (right_len > 0) {
+      for (double* M : {H, T}) {
+        UpdJob& j = L.job[L.njobs++];
+        j.M = M; j.ld = ld; j.r0 = w; j.c0 = w + wk; j.len = right_len; j.W = U; j.ldw = wk;
+        j.tiles = (right_len + tile - 1) / tile;
+      }
+      c->stats.upd_flops += 2.0 * 2.0 * wk * wk * right_len;
+    }
+    UpdBatch R;
+    R.k = wk;
+    R.njobs = 0;
+    if (w > 0) {
+      for (double* M : {H, T}) {
+        UpdJob& j = R.job[R.njobs++];
+        j.M = M; j.ld = ld; j.r0 = 0; j.c0 = w; j.len = w; j.W = V; j.ldw = wk;
+        j.tiles = (w + tile - 1) / tile;
+      }
+      c->stats.upd_flops += 2.0 * 2.0 * wk * wk * w;
+    }
+    if (wantq) {
+      UpdJob& j = R.job[R.njobs++];
+      j.M = Q; j.ld = ld; j.r0 = 0; j.c0 = w; j.len = n; j.W = U; j.ldw = wk;
+      j.tiles = (n + tile - 1) / tile;
+      c->stats.upd_flops += 2.0 * wk * wk * n;
+    }
+    if (wantz) {
+      UpdJob& j = R.job[R.njobs++];
+      j.M = Z; j.ld = ld; j.r0 = 0; j.c0 = w; j.len = n; j.W = V; j.ldw = wk;
+      j.tiles = (n + tile - 1) / tile;
+      c->stats.upd_flops += 2.0 * wk * wk * n;
+    }
+    if (L.njobs) launch_update(c->stream, L, 0);
+    if (R.njobs) launch_update(c->stream, R, 1);
+  }
+};
+
+bool is(char a, char b) { return std::toupper((unsigned char)a) == b; }
+
+int check_args(char job, char compq, char compz, int n, int ilo, int ihi) {
+  if (!is(job, 'E') && !is(job, 'S')) return -1;
+  if (!is(compq, 'N') && !is(compq, 'V') && !is(compq, 'I')) return -2;
+  if (!is(compz, 'N') && !is(compz, 'V') && !is(compz, 'I')) return -3;
+  if (n < 0) return -4;
+  if (ilo < 1) return -5;
+  if (ihi > n || ihi < ilo - 1) return -6;
+  return 0;
+}
+
+int solve_dev_impl(b200qz_ctx* c, char job, char compq, char compz, int n, int ilo, int ihi, double* h, double* t,
+                   double* q, double* z, int ld, double* ar, double* ai, double* be) {
+  c->stats = SolveStats();
+  c->seconds = 0.0;
+  c->err = cudaSuccess;
+  {
+    const char* v = std::getenv("B200QZ_VERBOSE");
+    c->params.verbose = (v && *v && *v != '0') ? 1 : 0;
+  }
+  QZ_CK(cudaSetDevice(c->device));
+  bool wantq = !is(compq, 'N'), wantz = !is(compz, 'N');
+  if (is(compq, 'I')) launch_identity(c->stream, q, ld, n);
+  if (is(compz, 'I')) launch_identity(c->stream, z, ld, n);
+  QZ_CK(cudaEventRecord(c->ev0, c->stream));
+  int nh = ihi - ilo + 1;
+  // /PREC/ constants (PDHGEQZ.f:449-458): ulp, smlnum, Frobenius norms
+  QZ_CK(cudaMemsetAsync(c->norms, 0, 2 * sizeof(double), c->stream));
+  launch_sumsq(c->stream, h, ld, ilo - 1, nh, c->norms);
+  launch_sumsq(c->stream, t, ld, ilo - 1, nh, c->norms + 1);
+  QZ_CK(cudaMemcpyAsync(c->hnorms, c->norms, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  QZ_CK(cudaStreamSynchronize(c->stream));
+  if (c->err != cudaSuccess) return 10001;
+  GpuBackend bk;
+  bk.c = c;
+  bk.H = h; bk.T = t; bk.Q = q; bk.Z = z;
+  bk.ld = ld;
+  bk.n = n;
+  bk.wantq = wantq;
+  bk.wantz = wantz;
+  Tol& tol = bk.tol;
+  tol.safmin = DBL_MIN;
+  tol.ulp = DBL_EPSILON;
+  tol.smlnum = DBL_MIN * ((double)nh / DBL_EPSILON);
+  tol.htol = std::max(DBL_MIN, DBL_EPSILON * std::sqrt(c->hnorms[0]));
+  tol.ttol = std::max(DBL_MIN, DBL_EPSILON * std::sqrt(c->hnorms[1]));
+  int info = 0;
+  if (nh > 0) info = qz_iterate(bk, n, ilo - 1, ihi - 1, c->params, c->stats);
+  launch_finalize(c->stream, h, t, z, ld, n, wantz ? 1 : 0, ar, ai, be);
+  QZ_CK(cudaGetLastError());
+  QZ_CK(cudaEventRecord(c->ev1, c->stream));
+  QZ_CK(cudaEventSynchronize(c->ev1));
+  float ms = 0.f;
+  QZ_CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+  c->seconds = ms * 1e-3;
+  (void)job;
+  if (c->err != cudaSuccess) return 10001;
+  return info;
+}
+
+}  // namespace
+
+extern "C" {
+
+int b200qz_create(b200qz_ctx** out, int device) {
+  if (!out) return -1;
+  *out = nullptr;
+  b200qz_ctx* c = new b200qz_ctx();
+  c->device = device;
+  cudaError_t e = cudaSetDevice(device);
+  if (e == cudaSuccess) e = kernels_init();
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  size_t a2 = (size_t)kAedMax * kAedMax * sizeof(double);
+  size_t w2 = (size_t)kWinSmemMax * kWinSmemMax * sizeof(double);
+  if (e == cudaSuccess) e = cudaMalloc(&c->Ua, a2);
+  if (e == cudaSuccess) e = cudaMalloc(&c->Va, a2);
+  if (e == cudaSuccess) e = cudaMalloc(&c->Uc, w2);
+  if (e == cudaSuccess) e = cudaMalloc(&c->Vc, w2);
+  if (e == cudaSuccess) e = cudaMalloc(&c->shifts, 3 * kAedMax * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc(&c->gscratch, 2 * a2);
+  if (e == cudaSuccess) e = cudaMalloc(&c->norms, 2 * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc(&c->dinfo, 8 * sizeof(int));
+  if (e == cudaSuccess) e = cudaMallocHost(&c->hinfo, 8 * sizeof(int));
+  if (e == cudaSuccess) e = cudaMallocHost(&c->hshifts, 3 * kAedMax * sizeof(double));
+  if (e == cudaSuccess) e = cudaMallocHost(&c->hnorms, 2 * sizeof(double));
+  if (e == cudaSuccess) e = cudaEventCreate(&c->ev0);
+  if (e == cudaSuccess) e = cudaEventCreate(&c->ev1);
+  if (e != cudaSuccess) {
+    b200qz_destroy(c);
+    return (int)e;
+  }
+  *out = c;
+  return 0;
+}
+
+void b200qz_destroy(b200qz_ctx* c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  cudaFree(c->Ua); cudaFree(c->Va); cudaFree(c->Uc); cudaFree(c->Vc);
+  cudaFree(c->shifts); cudaFree(c->gscratch); cudaFree(c->norms); cudaFree(c->dinfo);
+  if (c->hinfo) cudaFreeHost(c->hinfo);
+  if (c->hshifts) cudaFreeHost(c->hshifts);
+  if (c->hnorms) cudaFreeHost(c->hnorms);
+  if (c->ev0) cudaEventDestroy(c->ev0);
+  if (c->ev1) cudaEventDestroy(c->ev1);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+}
+
+int b200qz_set_params(b200qz_ctx* c, int nw_max, int w_chase, int nmin, int nibble, int ns_max, int maxit_factor) {
+  if (!c) return -1;
+  if (nw_max > kWinSmemMax) return -2;
+  if (w_chase > kWinSmemMax || (w_chase >= 0 && w_chase < 12)) return -3;
+  if (nmin > kAedMax) return -4;
+  if (nibble > 100) return -5;
+  if (nw_max >= 0) c->params.nw_max = std::max(4, nw_max);
+  if (w_chase >= 0) c->params.w_chase = w_chase;
+  if (nmin >= 0) c->params.nmin = std::max(4, nmin);
+  if (nibble >= 0) c->params.nibble = nibble;
+  if (ns_max >= 0) c->params.ns_max = ns_max;
+  if (maxit_factor >= 0) c->params.maxit_factor = std::max(1, maxit_factor);
+  c->params.chain_max = std::min(kMaxChain, std::max(1, (c->params.w_chase - 4) / 6));
+  return 0;
+}
+
+int b200qz_solve_dev(b200qz_ctx* c, char job, char compq, char compz, int n, int ilo, int ihi, double* h, double* t,
+                     double* q, double* z, int ld, double* ar, double* ai, double* be) {
+  if (!c) return 10001;
+  int a = check_args(job, compq, compz, n, ilo, ihi);
+  if (a != 0) return a;
+  if (n == 0) return 0;
+  if (ld < std::max(1, n)) return -(7 * 1000 + 9);
+  return solve_dev_impl(c, job, compq, compz, n, ilo, ihi, h, t, q, z, ld, ar, ai, be);
+}
+
+int b200qz_solve_host(b200qz_ctx* c, char job, char compq, char compz, int n, int ilo, int ihi, double* h, int ldh,
+                      double* t, int ldt, double* q, int ldq, double* z, int ldz, double* ar, double* ai,
+                      double* be) {
+  if (!c) return 10001;
+  int a = check_args(job, compq, compz, n, ilo, ihi);
+  if (a != 0) return a;
+  if (n == 0) return 0;
+  if (ldh < std::max(1, n)) return -(7 * 1000 + 9);
+  if (ldt < std::max(1, n)) return -(9 * 1000 + 9);
+  bool wantq = !is(compq, 'N'), wantz = !is(compz, 'N');
+  if (wantq && ldq < std::max(1, n)) return -(14 * 1000 + 9);
+  if (wantz && ldz < std::max(1, n)) return -(16 * 1000 + 9);
+  c->err = cudaSuccess;
+  QZ_CK(cudaSetDevice(c->device));
+  int ldd = (n + 31) & ~31;
+  size_t bytes = (size_t)ldd * n * sizeof(double);
+  double *dh = nullptr, *dt = nullptr, *dq = nullptr, *dz = nullptr, *de = nullptr;
+  QZ_CK(cudaMalloc(&dh, bytes));
+  QZ_CK(cudaMalloc(&dt, bytes));
+  QZ_CK(cudaMalloc(&dq, bytes));
+  QZ_CK(cudaMalloc(&dz, bytes));
+  QZ_CK(cudaMalloc(&de, 3 * (size_t)n * sizeof(double)));
+  int info = 10001;
+  if (c->err == cudaSuccess) {
+    size_t w = (size_t)n * sizeof(double);
+    QZ_CK(cudaMemcpy2DAsync(dh, ldd * sizeof(double), h, (size_t)ldh * sizeof(double), w, n, cudaMemcpyHostToDevice, c->stream));
+    QZ_CK(cudaMemcpy2DAsync(dt, ldd * sizeof(double), t, (size_t)ldt * sizeof(double), w, n, cudaMemcpyHostToDevice, c->stream));
+    if (is(compq, 'V'))
+      QZ_CK(cudaMemcpy2DAsync(dq, ldd * sizeof(double), q, (size_t)ldq * sizeof(double), w, n, cudaMemcpyHostToDevice, c->stream));
+    if (is(compz, 'V'))
+      QZ_CK(cudaMemcpy2DAsync(dz, ldd * sizeof(double), z, (size_t)ldz * sizeof(double), w, n, cudaMemcpyHostToDevice, c->stream));
+    if (c->err == cudaSuccess) {
+      info = solve_dev_impl(c, job, compq, compz, n, ilo, ihi, dh, dt, dq, dz, ldd, de, de + n, de + 2 * n);
+      QZ_CK(cudaMemcpy2DAsync(h, (size_t)ldh * sizeof(double), dh, ldd * sizeof(double), w, n, cudaMemcpyDeviceToHost, c->stream));
+      QZ_CK(cudaMemcpy2DAsync(t, (size_t)ldt * sizeof(double), dt, ldd * sizeof(double), w, n, cudaMemcpyDeviceToHost, c->stream));
+      if (wantq)
+        QZ_CK(cudaMemcpy2DAsync(q, (size_t)ldq * sizeof(double), dq, ldd * sizeof(double), w, n, cudaMemcpyDeviceToHost, c->stream));
+      if (wantz)
+        QZ_CK(cudaMemcpy2DAsync(z, (size_t)ldz * sizeof(double), dz, ldd * sizeof(double), w, n, cudaMemcpyDeviceToHost, c->stream));
+      QZ_CK(cudaMemcpyAsync(ar, de, w, cudaMemcpyDeviceToHost, c->stream));
+      QZ_CK(cudaMemcpyAsync(ai, de + n, w, cudaMemcpyDeviceToHost, c->stream));
+      QZ_CK(cudaMemcpyAsync(be, de + 2 * n, w, cudaMemcpyDeviceToHost, c->stream));
+      QZ_CK(cudaStreamSynchronize(c->stream));
+    }
+  }
+  cudaFree(dh); cudaFree(dt); cudaFree(dq); cudaFree(dz); cudaFree(de);
+  if (c->err != cudaSuccess) return 10001;
+  return info;
+}
+
+int b200qz_get_stats(const b200qz_ctx* c, double* out, int nout) {
+  if (!c || !out) return 0;
+  const SolveStats& s = c->stats;
+  double v[12] = {c->seconds, (double)s.iters, (double)s.aeds, (double)s.aed_defl, (double)s.sweeps,
+                  (double)s.chains, (double)s.windows, (double)s.endgames, (double)s.infs, (double)s.shifts,
+                  s.upd_flops, s.win_bytes};
+  int k = std::min(nout, 12);
+  for (int i = 0; i < k; ++i) out[i] = v[i];
+  return k;
+}
+
+int b200qz_aed_window(b200qz_ctx* c, double* h, double* t, int ld, int ktop, int kwtop, int kbot, double* qw,
+                      double* zw, double* shifts, int* info3) {
+  if (!c) return 10001;
+  int nw = kbot - kwtop + 1;
+  if (nw < 1 || nw > kAedMax || ktop > kwtop || kwtop < 0) return -1;
+  c->err = cudaSuccess;
+  QZ_CK(cudaSetDevice(c->device));
+  // norms of the whole leading (kbot+1) block give the tolerances
+  int nh = kbot + 1;
+  QZ_CK(cudaMemsetAsync(c->norms, 0, 2 * sizeof(double), c->stream));
+  launch_sumsq(c->stream, h, ld, 0, nh, c->norms);
+  launch_sumsq(c->stream, t, ld, 0, nh, c->norms + 1);
+  QZ_CK(cudaMemcpyAsync(c->hnorms, c->norms, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  QZ_CK(cudaStreamSynchronize(c->stream));
+  Tol tol;
+  tol.safmin = DBL_MIN;
+  tol.ulp = DBL_EPSILON;
+  tol.smlnum = DBL_MIN * ((double)nh / DBL_EPSILON);
+  tol.htol = std::max(DBL_MIN, DBL_EPSILON * std::sqrt(c->hnorms[0]));
+  tol.ttol = std::max(DBL_MIN, DBL_EPSILON * std::sqrt(c->hnorms[1]));
+  launch_aed(c->stream, h, t, ld, ktop, kwtop, nw, tol, qw, zw, shifts, c->dinfo + 4, c->gscratch);
+  QZ_CK(cudaMemcpyAsync(c->hinfo + 4, c->dinfo + 4, 3 * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  QZ_CK(cudaStreamSynchronize(c->stream));
+  QZ_CK(cudaGetLastError());
+  if (c->err != cudaSuccess) return 10001;
+  for (int i = 0; i < 3; ++i) info3[i] = c->hinfo[4 + i];
+  return 0;
+}
+
+int b200qz_chase_window(b200qz_ctx* c, double* h, double* t, int ld, int w, int wk, int last, const int* bulges,
+                        const double* coef, int nb, int tmax, double* u, double* v) {
+  if (!c) return 10001;
+  if (wk < 4 || wk > kWinSmemMax || nb < 1 || nb > kMaxChain || last >= wk) return -1;
+  c->err = cudaSuccess;
+  QZ_CK(cudaSetDevice(c->device));
+  Bulge bl[kMaxChain];
+  for (int b = 0; b < nb; ++b) {
+    bl[b].base = bulges[4 * b];
+    bl[b].tlo = bulges[4 * b + 1];
+    bl[b].thi = bulges[4 * b + 2];
+    bl[b].intro = bulges[4 * b + 3];
+    bl[b].c2 = coef[3 * b];
+    bl[b].c1 = coef[3 * b + 1];
+    bl[b].c0 = coef[3 * b + 2];
+  }
+  launch_chase(c->stream, h, t, ld, w, wk, last, bl, nb, tmax, u, v);
+  QZ_CK(cudaGetLastError());
+  QZ_CK(cudaStreamSynchronize(c->stream));
+  return c->err == cudaSuccess ? 0 : 10001;
+}
+
+int b200qz_update(b200qz_ctx* c, char side, double* m, int ldm, int r0, int c0, int len, const double* w, int ldw,
+                  int k) {
+  if (!c) return 10001;
+  if (k < 1 || k > kAedMax || len < 0) return -1;
+  c->err = cudaSuccess;
+  QZ_CK(cudaSetDevice(c->device));
+  UpdBatch B;
+  B.k = k;
+  B.njobs = 1;
+  UpdJob& j = B.job[0];
+  j.M = m; j.ld = ldm; j.r0 = r0; j.c0 = c0; j.len = len; j.W = w; j.ldw = ldw;
+  int tile = update_tile(k);
+  j.tiles = (len + tile - 1) / tile;
+  if (is(side, 'L')) launch_update(c->stream, B, 0);
+  else if (is(side, 'R')) launch_update(c->stream, B, 1);
+  else return -2;
+  QZ_CK(cudaGetLastError());
+  QZ_CK(cudaStreamSynchronize(c->stream));
+  return c->err == cudaSuccess ? 0 : 10001;
+}
+
+// ---------------------------------------------------------------------------
+// Fortran drop-in
+// ---------------------------------------------------------------------------
+static std::mutex g_mu;
+static b200qz_ctx* g_ctx = nullptr;
+
+void kkqzconf_(const double* eps) { (void)eps; }
+
+void pdhgeqz_(const char* job, const char* compq, const char* compz, const int* n, const int* ilo, const int* ihi,
+              double* h, const int* desch, double* t, const int* desct, double* alphar, double* alphai,
+              double* beta, double* q, const int* descq, double* z, const int* descz, double* dwork,
+              const int* ldwork, int* iwork, const int* liwork, int* info, size_t len_job, size_t len_compq,
+              size_t len_compz) {
+  (void)len_job; (void)len_compq; (void)len_compz;
+  const int N = *n, ILO = *ilo, IHI = *ihi;
+  // quick return (PDHGEQZ.f:320-323)
+  if (N <= 0 || IHI < ILO) { *info = 0; return; }
+  // descriptor fields (1-based in Fortran): MB_=5, NB_=6, LLD_=9
+  int a = check_args(*job, *compq, *compz, N, ILO, IHI);
+  if (a == 0 && desch[5] < 5) a = -7;
+  if (a == 0 && desch[5] != desch[4]) a = -8;
+  if (a != 0) { *info = a; return; }
+  int nb = desch[5];
+  // workspace (same order as PDHGEQZ1.f:369-372)
+  int ldwmin = std::max(1, N * nb), liwmin = std::max(1, 2 * N);
+  if (*ldwork == -1 || *liwork == -1) {
+    dwork[0] = (double)ldwmin;
+    iwork[0] = liwmin;
+    *info = 0;
+    return;
+  }
+  if (*ldwork < ldwmin) { *info = -9; return; }
+  if (*liwork < liwmin) { *info = -10; return; }
+  int ldh = desch[8], ldt = desct[8], ldq = descq[8], ldz = descz[8];
+  // ALPHAR/ALPHAI/BETA(ILO:IHI) = -1 on entry (PDHGEQZ.f:469-471)
+  for (int i = ILO - 1; i < IHI; ++i) { alphar[i] = -1.0; alphai[i] = -1.0; beta[i] = -1.0; }
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (!g_ctx) {
+    int dev = 0;
+    const char* e = std::getenv("B200QZ_DEVICE");
+    if (e) dev = std::atoi(e);
+    if (b200qz_create(&g_ctx, dev) != 0) { g_ctx = nullptr; *info = 10001; return; }
+  }
+  *info = b200qz_solve_host(g_ctx, *job, *compq, *compz, N, ILO, IHI, h, ldh, t, ldt, q, ldq, z, ldz, alphar,
+                            alphai, beta);
+}
+
+}  // extern "C"

@@ -1,0 +1,387 @@
+// sm_100a kernels of the multishift QZ path.
+//
+//   k_aed_win     one CTA: window Schur form + spike test + reordering +
+//                 re-reduction (AED, PDHGEQZ2/QZEARLY) or a full small
+//                 solve (endgame, PDHGEQZ4/KKQZ) with the window in smem
+//   k_chase_win   one CTA: a chain of bulges through one window (PDHGEQZ5/
+//                 A/B, DHGEQZ5) accumulating U, V in smem
+//   k_inf_win     one CTA: zero chasing of an infinite eigenvalue through a
+//                 window (PDHGEQZ7/8, DHGEQZ7)
+//   k_update_*    in-place off-diagonal updates on DMMA (PDHGEQZ6)
+//   k_scan        deflation search (PDLASMSUB) + zero T-diagonal detection
+//   k_inf_top     top deflation of an infinite eigenvalue (one rotation)
+//   k_signs, k_eigs   sign normalisation (beta >= 0) and alpha/beta output
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#define QZ_DEFINE_UPDATE_KERNELS
+#include "qz_chase.cuh"
+#include "update.cuh"
+#include "kernels.h"
+
+namespace qz {
+
+struct DevExec {
+  int tid, nt;
+  int* si;
+  double* sd;
+  __device__ void sync() { __syncthreads(); }
+};
+
+// shared-memory scratch carved at the end of the dynamic smem block
+constexpr int kSi = 64;
+
+__device__ __forceinline__ double& G(double* p, int64_t ld, int i, int j) { return p[i + (int64_t)j * ld]; }
+
+// ---------------------------------------------------------------------------
+// AED / small-solve window kernel
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kWinThreads) k_aed_win(double* H, double* T, int64_t ld, int ktop, int kwtop,
+                                                         int nw, Tol tol, double* Qw, double* Zw, double* shifts,
+                                                         int* info, double* gscratch, int maxit) {
+  extern __shared__ double smem[];
+  const int n = nw;
+  double* Hs;
+  double* Ts;
+  double* Qs;
+  double* Zs;
+  double* sd;
+  if (n <= kWinSmemMax) {
+    Hs = smem;
+    Ts = Hs + n * n;
+    Qs = Ts + n * n;
+    Zs = Qs + n * n;
+    sd = Zs + n * n;
+  } else {
+    Hs = gscratch;
+    Ts = gscratch + (int64_t)n * n;
+    Qs = Qw;
+    Zs = Zw;
+    sd = smem;
+  }
+  int* si = (int*)(sd + 64 + 4 * n);
+  DevExec x{(int)threadIdx.x, (int)blockDim.x, si, sd};
+  for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
+    int i = idx % n, j = idx / n;
+    Hs[idx] = G(H, ld, kwtop + i, kwtop + j);
+    Ts[idx] = G(T, ld, kwtop + i, kwtop + j);
+    Qs[idx] = (i == j) ? 1.0 : 0.0;
+    Zs[idx] = (i == j) ? 1.0 : 0.0;
+  }
+  double s = (kwtop > ktop) ? G(H, ld, kwtop, kwtop - 1) : 0.0;
+  __syncthreads();
+  WinState w;
+  w.n = n;
+  w.H = MatV{Hs, n};
+  w.T = MatV{Ts, n};
+  w.Q = MatV{Qs, n};
+  w.Z = MatV{Zs, n};
+  w.wantq = true;
+  w.wantz = true;
+  w.tol = tol;
+  cta_aed(x, w, s, shifts, shifts + n, shifts + 2 * n, maxit);
+  __syncthreads();
+  const int m = si[8], st = si[9], tr = si[10];
+  if (st == 0 && tr) {
+    for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
+      int i = idx % n, j = idx / n;
+      G(H, ld, kwtop + i, kwtop + j) = Hs[idx];
+      G(T, ld, kwtop + i, kwtop + j) = Ts[idx];
+      if (n <= kWinSmemMax) {
+        Qw[idx] = Qs[idx];
+        Zw[idx] = Zs[idx];
+      }
+    }
+    if (threadIdx.x == 0 && kwtop > ktop) G(H, ld, kwtop, kwtop - 1) = s * Qs[0];
+  }
+  if (threadIdx.x == 0) {
+    info[0] = m;
+    info[1] = st;
+    info[2] = tr;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// chase kernel
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kWinThreads) k_chase_win(double* H, double* T, int64_t ld, int w0, int wk, int last,
+                                                           const BulgeArr bl_g, int nb, int tmax, double* U, double* V) {
+  extern __shared__ double smem[];
+  double* Hs = smem;
+  double* Ts = Hs + wk * wk;
+  double* Us = Ts + wk * wk;
+  double* Vs = Us + wk * wk;
+  Bulge* bl = (Bulge*)(Vs + wk * wk);
+  BulgeRec* rec = (BulgeRec*)(bl + kMaxChain);
+  int* si = (int*)(rec + kMaxChain);
+  DevExec x{(int)threadIdx.x, (int)blockDim.x, si, nullptr};
+  for (int idx = threadIdx.x; idx < wk * wk; idx += blockDim.x) {
+    int i = idx % wk, j = idx / wk;
+    Hs[idx] = G(H, ld, w0 + i, w0 + j);
+    Ts[idx] = G(T, ld, w0 + i, w0 + j);
+    Us[idx] = (i == j) ? 1.0 : 0.0;
+    Vs[idx] = (i == j) ? 1.0 : 0.0;
+  }
+  for (int b = threadIdx.x; b < nb; b += blockDim.x) bl[b] = bl_g.b[b];
+  __syncthreads();
+  cta_chase_window(x, wk, last, MatV{Hs, wk}, MatV{Ts, wk}, MatV{Us, wk}, MatV{Vs, wk}, bl, nb, tmax, rec);
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < wk * wk; idx += blockDim.x) {
+    int i = idx % wk, j = idx / wk;
+    G(H, ld, w0 + i, w0 + j) = Hs[idx];
+    G(T, ld, w0 + i, w0 + j) = Ts[idx];
+    U[idx] = Us[idx];
+    V[idx] = Vs[idx];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// infinite-eigenvalue zero chase through a window
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kWinThreads) k_inf_win(double* H, double* T, int64_t ld, int w0, int wk, int top,
+                                                         int jz, int stop, int deflate, double* U, double* V) {
+  extern __shared__ double smem[];
+  double* Hs = smem;
+  double* Ts = Hs + wk * wk;
+  double* Us = Ts + wk * wk;
+  double* Vs = Us + wk * wk;
+  int* si = (int*)(Vs + wk * wk);
+  DevExec x{(int)threadIdx.x, (int)blockDim.x, si, nullptr};
+  for (int idx = threadIdx.x; idx < wk * wk; idx += blockDim.x) {
+    int i = idx % wk, j = idx / wk;
+    Hs[idx] = G(H, ld, w0 + i, w0 + j);
+    Ts[idx] = G(T, ld, w0 + i, w0 + j);
+    Us[idx] = (i == j) ? 1.0 : 0.0;
+    Vs[idx] = (i == j) ? 1.0 : 0.0;
+  }
+  __syncthreads();
+  cta_inf_window(x, wk, top, jz, stop, deflate != 0, MatV{Hs, wk}, MatV{Ts, wk}, MatV{Us, wk}, MatV{Vs, wk});
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < wk * wk; idx += blockDim.x) {
+    int i = idx % wk, j = idx / wk;
+    G(H, ld, w0 + i, w0 + j) = Hs[idx];
+    G(T, ld, w0 + i, w0 + j) = Ts[idx];
+    U[idx] = Us[idx];
+    V[idx] = Vs[idx];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// deflation scan: ktop = largest k in (ifirst, kbot] with negligible
+// H(k,k-1) (zeroed), then zero T-diagonal entries in [ktop, kbot].
+// out = {ktop, ninf, jmax, jmin}
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(1024) k_scan(double* H, double* T, int64_t ld, int ifirst, int kbot, Tol tol,
+                                               int* out) {
+  __shared__ int s_best;
+  __shared__ int s_cnt, s_jmax, s_jmin;
+  if (threadIdx.x == 0) { s_best = -1; s_cnt = 0; s_jmax = -1; s_jmin = 0x7fffffff; }
+  __syncthreads();
+  for (int base = kbot; base > ifirst; base -= blockDim.x) {
+    int k = base - (int)threadIdx.x;
+    if (k > ifirst) {
+      if (negligible_sub(G(H, ld, k, k - 1), G(H, ld, k - 1, k - 1), G(H, ld, k, k), tol)) atomicMax(&s_best, k);
+    }
+    __syncthreads();
+    if (s_best >= 0) break;
+    __syncthreads();
+  }
+  int ktop = (s_best >= 0) ? s_best : ifirst;
+  __syncthreads();
+  if (threadIdx.x == 0 && ktop > ifirst) G(H, ld, ktop, ktop - 1) = 0.0;
+  for (int j = ktop + (int)threadIdx.x; j <= kbot; j += blockDim.x) {
+    double t = G(T, ld, j, j);
+    if (fabs(t) <= tol.ttol) {
+      G(T, ld, j, j) = 0.0;
+      atomicAdd(&s_cnt, 1);
+      atomicMax(&s_jmax, j);
+      atomicMin(&s_jmin, j);
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    out[0] = ktop;
+    out[1] = s_cnt;
+    out[2] = s_jmax;
+    out[3] = (s_cnt > 0) ? s_jmin : -1;
+  }
+}
+
+// top deflation: T(f,f) = 0; rotation of rows f, f+1 zeroing H(f+1,f)
+__global__ void __launch_bounds__(1024) k_inf_top(double* H, double* T, double* Q, int64_t ld, int n, int f, int wantq) {
+  double c, s, r;
+  lartg(G(H, ld, f, f), G(H, ld, f + 1, f), c, s, r);
+  __syncthreads();
+  for (int j = f + 1 + (int)threadIdx.x; j < n; j += blockDim.x) {
+    double a = G(H, ld, f, j), b = G(H, ld, f + 1, j);
+    G(H, ld, f, j) = c * a + s * b;
+    G(H, ld, f + 1, j) = -s * a + c * b;
+    a = G(T, ld, f, j); b = G(T, ld, f + 1, j);
+    G(T, ld, f, j) = c * a + s * b;
+    G(T, ld, f + 1, j) = -s * a + c * b;
+  }
+  if (wantq)
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      double a = G(Q, ld, i, f), b = G(Q, ld, i, f + 1);
+      G(Q, ld, i, f) = c * a + s * b;
+      G(Q, ld, i, f + 1) = -s * a + c * b;
+    }
+  if (threadIdx.x == 0) { G(H, ld, f, f) = r; G(H, ld, f + 1, f) = 0.0; }
+}
+
+// ---------------------------------------------------------------------------
+// finalisation
+// ---------------------------------------------------------------------------
+// 1x1 blocks with T(j,j) < 0: negate column j of H, T (rows 0..j) and Z
+__global__ void k_signs(double* H, double* T, double* Z, int64_t ld, int n, int wantz) {
+  int j = blockIdx.x;
+  bool below = (j + 1 < n) && G(H, ld, j + 1, j) != 0.0;
+  bool above = (j > 0) && G(H, ld, j, j - 1) != 0.0;
+  if (below || above) return;
+  if (!(G(T, ld, j, j) < 0.0)) return;
+  __syncthreads();
+  for (int i = threadIdx.x; i <= j; i += blockDim.x) {
+    G(H, ld, i, j) = -G(H, ld, i, j);
+    G(T, ld, i, j) = -G(T, ld, i, j);
+  }
+  if (wantz)
+    for (int i = threadIdx.x; i < n; i += blockDim.x) G(Z, ld, i, j) = -G(Z, ld, i, j);
+}
+
+__global__ void k_eigs(const double* H, const double* T, int64_t ld, int n, double* ar, double* ai, double* be) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  bool below = (j + 1 < n) && G((double*)H, ld, j + 1, j) != 0.0;
+  bool above = (j > 0) && G((double*)H, ld, j, j - 1) != 0.0;
+  if (!below && !above) {
+    ar[j] = G((double*)H, ld, j, j);
+    ai[j] = 0.0;
+    be[j] = G((double*)T, ld, j, j);
+    return;
+  }
+  int f = below ? j : j - 1;
+  double a[4] = {G((double*)H, ld, f, f), G((double*)H, ld, f + 1, f), G((double*)H, ld, f, f + 1),
+                 G((double*)H, ld, f + 1, f + 1)};
+  double o_ar[2], o_ai[2], o_be[2];
+  eig2_complex(a, G((double*)T, ld, f, f), G((double*)T, ld, f + 1, f + 1), o_ar, o_ai, o_be);
+  int e = j - f;
+  ar[j] = o_ar[e];
+  ai[j] = o_ai[e];
+  be[j] = o_be[e];
+}
+
+__global__ void k_set_identity(double* Q, int64_t ld, int n) {
+  int64_t total = (int64_t)n * n;
+  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total; idx += (int64_t)gridDim.x * blockDim.x) {
+    int i = (int)(idx % n), j = (int)(idx / n);
+    G(Q, ld, i, j) = (i == j) ? 1.0 : 0.0;
+  }
+}
+
+// sum of squares of the n x n block at (o, o)
+__global__ void k_sumsq(const double* A, int64_t ld, int o, int n, double* out) {
+  double acc = 0.0;
+  int64_t total = (int64_t)n * n;
+  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total; idx += (int64_t)gridDim.x * blockDim.x) {
+    int i = (int)(idx % n), j = (int)(idx / n);
+    double v = A[(o + i) + (int64_t)(o + j) * ld];
+    acc += v * v;
+  }
+  for (int off = 16; off > 0; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
+  __shared__ double red[32];
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) red[wid] = acc;
+  __syncthreads();
+  if (wid == 0) {
+    acc = (lane < (int)(blockDim.x >> 5)) ? red[lane] : 0.0;
+    for (int off = 16; off > 0; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
+    if (lane == 0) atomicAdd(out, acc);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
+size_t aed_smem_bytes(int nw) {
+  size_t d = (nw <= kWinSmemMax) ? (size_t)4 * nw * nw : 0;
+  d += 64 + 4 * (size_t)nw;
+  return d * sizeof(double) + kSi * sizeof(int);
+}
+size_t chase_smem_bytes(int wk) {
+  return (size_t)4 * wk * wk * sizeof(double) + kMaxChain * (sizeof(Bulge) + sizeof(BulgeRec)) + kSi * sizeof(int);
+}
+size_t inf_smem_bytes(int wk) { return (size_t)4 * wk * wk * sizeof(double) + kSi * sizeof(int); }
+
+static size_t upd_smem(int k, int side) {
+  int kp = (k + 15) & ~15;
+  if (k > kUpdMaxK) return (size_t)k * kUpdGenTile * sizeof(double);
+  if (side == 0) return ((size_t)kp * (kp + 4) + (size_t)kp * 36) * sizeof(double);
+  return ((size_t)kp * (kp + 4) + (size_t)32 * (kp + 4)) * sizeof(double);
+}
+
+cudaError_t kernels_init() {
+  cudaError_t e;
+  e = cudaFuncSetAttribute(k_aed_win, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)aed_smem_bytes(kWinSmemMax));
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(k_chase_win, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)chase_smem_bytes(kWinSmemMax));
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(k_inf_win, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)inf_smem_bytes(kWinSmemMax));
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(k_update_left, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)upd_smem(kUpdMaxK, 0));
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(k_update_right, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)upd_smem(kUpdMaxK, 1));
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(k_update_left_gen, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(k_update_right_gen, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  return e;
+}
+
+void launch_aed(cudaStream_t st, double* H, double* T, int64_t ld, int ktop, int kwtop, int nw, const Tol& tol,
+                double* Qw, double* Zw, double* shifts, int* info, double* gscratch) {
+  k_aed_win<<<1, kWinThreads, aed_smem_bytes(nw), st>>>(H, T, ld, ktop, kwtop, nw, tol, Qw, Zw, shifts, info, gscratch,
+                                                       30 * nw);
+}
+void launch_chase(cudaStream_t st, double* H, double* T, int64_t ld, int w0, int wk, int last, const Bulge* bl, int nb,
+                  int tmax, double* U, double* V) {
+  BulgeArr arr;
+  for (int b = 0; b < nb && b < kMaxChain; ++b) arr.b[b] = bl[b];
+  k_chase_win<<<1, kWinThreads, chase_smem_bytes(wk), st>>>(H, T, ld, w0, wk, last, arr, nb, tmax, U, V);
+}
+void launch_inf(cudaStream_t st, double* H, double* T, int64_t ld, int w0, int wk, int top, int jz, int stop,
+                int deflate, double* U, double* V) {
+  k_inf_win<<<1, kWinThreads, inf_smem_bytes(wk), st>>>(H, T, ld, w0, wk, top, jz, stop, deflate, U, V);
+}
+void launch_scan(cudaStream_t st, double* H, double* T, int64_t ld, int ifirst, int kbot, const Tol& tol, int* out) {
+  k_scan<<<1, 1024, 0, st>>>(H, T, ld, ifirst, kbot, tol, out);
+}
+void launch_inf_top(cudaStream_t st, double* H, double* T, double* Q, int64_t ld, int n, int f, int wantq) {
+  k_inf_top<<<1, 1024, 0, st>>>(H, T, Q, ld, n, f, wantq);
+}
+void launch_update(cudaStream_t st, const UpdBatch& B, int side) {
+  int tiles = 0;
+  for (int j = 0; j < B.njobs; ++j) tiles += B.job[j].tiles;
+  if (tiles == 0) return;
+  if (B.k > kUpdMaxK) {
+    if (side == 0) k_update_left_gen<<<tiles, 256, upd_smem(B.k, 0), st>>>(B);
+    else k_update_right_gen<<<tiles, 256, upd_smem(B.k, 1), st>>>(B);
+  } else {
+    if (side == 0) k_update_left<<<tiles, kUpdThreads, upd_smem(B.k, 0), st>>>(B);
+    else k_update_right<<<tiles, kUpdThreads, upd_smem(B.k, 1), st>>>(B);
+  }
+}
+int update_tile(int k) { return k > kUpdMaxK ? kUpdGenTile : kUpdTile; }
+void launch_finalize(cudaStream_t st, double* H, double* T, double* Z, int64_t ld, int n, int wantz, double* ar,
+                     double* ai, double* be) {
+  if (n <= 0) return;
+  k_signs<<<n, 256, 0, st>>>(H, T, Z, ld, n, wantz);
+  k_eigs<<<(n + 255) / 256, 256, 0, st>>>(H, T, ld, n, ar, ai, be);
+}
+void launch_identity(cudaStream_t st, double* Q, int64_t ld, int n) {
+  k_set_identity<<<592, 256, 0, st>>>(Q, ld, n);
+}
+void launch_sumsq(cudaStream_t st, const double* A, int64_t ld, int o, int n, double* out) {
+  k_sumsq<<<592, 256, 0, st>>>(A, ld, o, n, out);
+}
+
+}  // namespace qz

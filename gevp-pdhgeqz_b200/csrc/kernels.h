@@ -1,0 +1,40 @@
+// Launch interface of the sm_100a kernels (see kernels.cu).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "qz_chase.cuh"
+#include "update.cuh"
+
+namespace qz {
+
+constexpr int kWinThreads = 128;   // threads of the one-CTA window kernels
+constexpr int kWinSmemMax = 80;    // window size held entirely in shared memory (4 x 80^2 FP64 = 200 KB)
+constexpr int kMaxChain = 26;      // bulges per chain (3*26+2 rows fit a window of 80)
+
+// bulge descriptors travel as a kernel parameter (no host->device copy)
+struct BulgeArr {
+  Bulge b[kMaxChain];
+};
+
+size_t aed_smem_bytes(int nw);
+size_t chase_smem_bytes(int wk);
+size_t inf_smem_bytes(int wk);
+cudaError_t kernels_init();
+
+void launch_aed(cudaStream_t st, double* H, double* T, int64_t ld, int ktop, int kwtop, int nw, const Tol& tol,
+                double* Qw, double* Zw, double* shifts, int* info, double* gscratch);
+void launch_chase(cudaStream_t st, double* H, double* T, int64_t ld, int w0, int wk, int last, const Bulge* bl, int nb,
+                  int tmax, double* U, double* V);
+void launch_inf(cudaStream_t st, double* H, double* T, int64_t ld, int w0, int wk, int top, int jz, int stop,
+                int deflate, double* U, double* V);
+void launch_scan(cudaStream_t st, double* H, double* T, int64_t ld, int ifirst, int kbot, const Tol& tol, int* out);
+void launch_inf_top(cudaStream_t st, double* H, double* T, double* Q, int64_t ld, int n, int f, int wantq);
+void launch_update(cudaStream_t st, const UpdBatch& B, int side);
+int update_tile(int k);
+void launch_finalize(cudaStream_t st, double* H, double* T, double* Z, int64_t ld, int n, int wantz, double* ar,
+                     double* ai, double* be);
+void launch_identity(cudaStream_t st, double* Q, int64_t ld, int n);
+void launch_sumsq(cudaStream_t st, const double* A, int64_t ld, int o, int n, double* out);
+
+}  // namespace qz

@@ -1,0 +1,279 @@
+// CTA-level chase of a chain of 3x3 bulges through one diagonal window.
+//
+// Role in the reference: PDHGEQZA (bulge introduction, PDHGEQZA.f:325-420),
+// PDHGEQZB + DHGEQZ5 (chase inside a window, DHGEQZ5.f:128-250) and the
+// push-off at the bottom edge (PDHGEQZA.f:382-417), with the window's
+// orthogonal factors U (left) and V (right) accumulated for the
+// off-diagonal updates (PDHGEQZ6.f:276-380).
+//
+// B200 design: the whole chain advances in lockstep.  At chain step tau
+// every active bulge b does one step at window row j_b = base_b + tau:
+//   phase A  thread b computes the left reflector (from H(j:j+2, j-1), or
+//            from the shift polynomial when the bulge is introduced), the
+//            left-updated 3x3 block of T, the opposite (right) reflector
+//            that clears T(j+1:j+2, j), and the final 3x3 block of T;
+//   phase B  all threads apply every left reflector to its three rows of
+//            H and T and to three columns of U;
+//   phase C  all threads apply every right reflector to its three columns
+//            of H and T and to three columns of V; thread b stores its T
+//            block (the finished column j-1 of H is stored in phase B).
+// Bulges are packed 3 rows apart: the rows touched by different left
+// reflectors and the columns touched by different right reflectors are
+// disjoint, and phase A reads only entries no other bulge changes in the
+// same step, so the lockstep schedule equals the sequential
+// bottom-bulge-first chase.
+#pragma once
+#include "qz_cta.cuh"
+
+namespace qz {
+
+struct Bulge {
+  int base;   // window row of the bulge's step at tau = 0 (may be < 0)
+  int tlo;    // first active chain step
+  int thi;    // one past the last active chain step
+  int intro;  // 1: the step at tau = tlo introduces the bulge
+  double c2, c1, c0;  // shift polynomial c2 M^2 - c1 M + c0 I
+};
+
+// per-step record produced in phase A
+struct BulgeRec {
+  int kind;  // 0 inactive, 1: 3x3 step, 2: terminal 2x2 step
+  int j;
+  int writecol;  // 1: store H(j:j+2, j-1) in phase B
+  double tau, v1, v2;     // left reflector (kind 1) / rotation c,s in tau,v1 (kind 2)
+  double taur, u1, u2;    // right reflector (kind 1) / rotation c,s in taur,u1 (kind 2)
+  double beta;            // new H(j, j-1)
+  double tb[9];           // final T block
+};
+
+// Compute the step of one bulge at window row j.  last = last active row
+// of the window (rows > last are outside the active block).
+QZ_HD void bulge_step_compute(MatV H, MatV T, int j, int last, bool intro,
+                              double c2, double c1, double c0, BulgeRec& r) {
+  r.j = j;
+  if (j + 2 <= last) {
+    r.kind = 1;
+    double a0, a1, a2;
+    if (intro) {
+      shift_column(H(j, j), H(j + 1, j), H(j, j + 1), H(j + 1, j + 1), H(j + 2, j + 1),
+                   T(j, j), T(j, j + 1), T(j + 1, j + 1), c2, c1, c0, a0, a1, a2);
+      r.writecol = 0;
+    } else {
+      a0 = H(j, j - 1); a1 = H(j + 1, j - 1); a2 = H(j + 2, j - 1);
+      r.writecol = 1;
+    }
+    double tau, v1 = a1, v2 = a2, beta = a0;
+    larfg3(beta, v1, v2, tau);
+    double* tb = r.tb;
+    for (int cc = 0; cc < 3; ++cc)
+      for (int rr = 0; rr < 3; ++rr) tb[rr + 3 * cc] = T(j + rr, j + cc);
+    for (int cc = 0; cc < 3; ++cc) refl3(tau, v1, v2, tb[3 * cc], tb[3 * cc + 1], tb[3 * cc + 2]);
+    double taur, u1, u2;
+    opposite_reflector3(tb, taur, u1, u2);
+    for (int rr = 0; rr < 3; ++rr) refl3(taur, u1, u2, tb[rr], tb[rr + 3], tb[rr + 6]);
+    tb[1] = 0.0;
+    tb[2] = 0.0;
+    r.tau = tau; r.v1 = v1; r.v2 = v2; r.beta = beta;
+    r.taur = taur; r.u1 = u1; r.u2 = u2;
+  } else {
+    // terminal 2x2 step at rows j, j+1 = last
+    r.kind = 2;
+    r.writecol = 1;
+    double c, s, rr;
+    lartg(H(j, j - 1), H(j + 1, j - 1), c, s, rr);
+    double t00 = T(j, j), t01 = T(j, j + 1), t10 = T(j + 1, j), t11 = T(j + 1, j + 1);
+    rot2(c, s, t00, t10);
+    rot2(c, s, t01, t11);
+    double cr, sr;
+    opposite_rot2(t10, t11, cr, sr);
+    rot2(cr, sr, t00, t01);
+    rot2(cr, sr, t10, t11);
+    r.tau = c; r.v1 = s; r.beta = rr;
+    r.taur = cr; r.u1 = sr;
+    r.tb[0] = t00; r.tb[1] = 0.0; r.tb[3] = t01; r.tb[4] = t11;
+  }
+}
+
+// Chase a chain through a window of size wk held in H, T (wk x wk), while
+// accumulating U, V (wk x wk, identity on entry).  last = last row of the
+// active block inside the window (wk-1 if the block continues below).
+// bl[0..nb) describe the bulges, rec is shared scratch for nb records.
+template <class X>
+QZ_HD void cta_chase_window(X& x, int wk, int last, MatV H, MatV T, MatV U, MatV V,
+                            const Bulge* bl, int nb, int tmax, BulgeRec* rec) {
+  for (int tau = 0; tau < tmax; ++tau) {
+    // ---- phase A: per-bulge computations ----
+    for (int b = x.tid; b < nb; b += x.nt) {
+      const Bulge& g = bl[b];
+      if (tau >= g.tlo && tau < g.thi) {
+        bool intro = g.intro && tau == g.tlo;
+        bulge_step_compute(H, T, g.base + tau, last, intro, g.c2, g.c1, g.c0, rec[b]);
+      } else {
+        rec[b].kind = 0;
+      }
+    }
+    x.sync();
+    // ---- phase B: left transformations ----
+    // The finished column j-1 of H is stored here, before phase C: the
+    // right reflector of the bulge above (rows <= j, cols j-3..j-1) must
+    // see it, as in the sequential bottom-first order.
+    for (int b = x.tid; b < nb; b += x.nt) {
+      const BulgeRec& r = rec[b];
+      if (r.kind == 0 || !r.writecol) continue;
+      int j = r.j;
+      H(j, j - 1) = r.beta;
+      H(j + 1, j - 1) = 0.0;
+      if (r.kind == 1) H(j + 2, j - 1) = 0.0;
+    }
+    for (int b = 0; b < nb; ++b) {
+      const BulgeRec& r = rec[b];
+      if (r.kind == 0) continue;
+      int j = r.j;
+      if (r.kind == 1) {
+        int nh = wk - j, nt = wk - (j + 3);
+        int tot = nh + (nt > 0 ? nt : 0) + wk;
+        for (int i = x.tid; i < tot; i += x.nt) {
+          if (i < nh) {
+            int c = j + i;
+            double a0 = H(j, c), a1 = H(j + 1, c), a2 = H(j + 2, c);
+            refl3(r.tau, r.v1, r.v2, a0, a1, a2);
+            H(j, c) = a0; H(j + 1, c) = a1; H(j + 2, c) = a2;
+          } else if (i < nh + (nt > 0 ? nt : 0)) {
+            int c = j + 3 + (i - nh);
+            double a0 = T(j, c), a1 = T(j + 1, c), a2 = T(j + 2, c);
+            refl3(r.tau, r.v1, r.v2, a0, a1, a2);
+            T(j, c) = a0; T(j + 1, c) = a1; T(j + 2, c) = a2;
+          } else {
+            int rr = i - nh - (nt > 0 ? nt : 0);
+            double a0 = U(rr, j), a1 = U(rr, j + 1), a2 = U(rr, j + 2);
+            refl3(r.tau, r.v1, r.v2, a0, a1, a2);
+            U(rr, j) = a0; U(rr, j + 1) = a1; U(rr, j + 2) = a2;
+          }
+        }
+      } else {
+        double c = r.tau, s = r.v1;
+        int nh = wk - j, nt = wk - (j + 2);
+        int tot = nh + (nt > 0 ? nt : 0) + wk;
+        for (int i = x.tid; i < tot; i += x.nt) {
+          if (i < nh) {
+            int cc = j + i;
+            double a = H(j, cc), bb = H(j + 1, cc);
+            H(j, cc) = c * a + s * bb; H(j + 1, cc) = -s * a + c * bb;
+          } else if (i < nh + (nt > 0 ? nt : 0)) {
+            int cc = j + 2 + (i - nh);
+            double a = T(j, cc), bb = T(j + 1, cc);
+            T(j, cc) = c * a + s * bb; T(j + 1, cc) = -s * a + c * bb;
+          } else {
+            int rr = i - nh - (nt > 0 ? nt : 0);
+            double a = U(rr, j), bb = U(rr, j + 1);
+            U(rr, j) = c * a + s * bb; U(rr, j + 1) = -s * a + c * bb;
+          }
+        }
+      }
+    }
+    x.sync();
+    // ---- phase C: right transformations ----
+    for (int b = 0; b < nb; ++b) {
+      const BulgeRec& r = rec[b];
+      if (r.kind == 0) continue;
+      int j = r.j;
+      if (r.kind == 1) {
+        int hr = (j + 4 < last + 1) ? j + 4 : last + 1;
+        int tot = hr + j + wk;
+        for (int i = x.tid; i < tot; i += x.nt) {
+          if (i < hr) {
+            double a0 = H(i, j), a1 = H(i, j + 1), a2 = H(i, j + 2);
+            refl3(r.taur, r.u1, r.u2, a0, a1, a2);
+            H(i, j) = a0; H(i, j + 1) = a1; H(i, j + 2) = a2;
+          } else if (i < hr + j) {
+            int rr = i - hr;
+            double a0 = T(rr, j), a1 = T(rr, j + 1), a2 = T(rr, j + 2);
+            refl3(r.taur, r.u1, r.u2, a0, a1, a2);
+            T(rr, j) = a0; T(rr, j + 1) = a1; T(rr, j + 2) = a2;
+          } else {
+            int rr = i - hr - j;
+            double a0 = V(rr, j), a1 = V(rr, j + 1), a2 = V(rr, j + 2);
+            refl3(r.taur, r.u1, r.u2, a0, a1, a2);
+            V(rr, j) = a0; V(rr, j + 1) = a1; V(rr, j + 2) = a2;
+          }
+        }
+      } else {
+        double c = r.taur, s = r.u1;
+        int hr = last + 1;
+        int tot = hr + j + wk;
+        for (int i = x.tid; i < tot; i += x.nt) {
+          if (i < hr) {
+            double a = H(i, j), bb = H(i, j + 1);
+            H(i, j) = c * a + s * bb; H(i, j + 1) = -s * a + c * bb;
+          } else if (i < hr + j) {
+            int rr = i - hr;
+            double a = T(rr, j), bb = T(rr, j + 1);
+            T(rr, j) = c * a + s * bb; T(rr, j + 1) = -s * a + c * bb;
+          } else {
+            int rr = i - hr - j;
+            double a = V(rr, j), bb = V(rr, j + 1);
+            V(rr, j) = c * a + s * bb; V(rr, j + 1) = -s * a + c * bb;
+          }
+        }
+      }
+    }
+    // deferred stores owned by the bulge's thread
+    for (int b = x.tid; b < nb; b += x.nt) {
+      const BulgeRec& r = rec[b];
+      if (r.kind == 1) {
+        int j = r.j;
+        for (int cc = 0; cc < 3; ++cc)
+          for (int rr = 0; rr < 3; ++rr) T(j + rr, j + cc) = r.tb[rr + 3 * cc];
+      } else if (r.kind == 2) {
+        int j = r.j;
+        T(j, j) = r.tb[0]; T(j + 1, j) = 0.0; T(j, j + 1) = r.tb[3]; T(j + 1, j + 1) = r.tb[4];
+      }
+    }
+    x.sync();
+  }
+}
+
+// Chase a zero diagonal entry of T from window row jz down to window row
+// stop (<= last) inside a window, accumulating U and V.  If stop == last
+// and deflate is set, finish with the column rotation that zeros
+// H(last, last-1) (an infinite eigenvalue deflates at the bottom).
+// top = first row of the active block inside the window (-1 if the block
+// starts above the window).  The zero-chasing steps are those of the
+// Moler-Stewart QZ (cf. PDHGEQZ8/DHGEQZ7 for the windowed form).
+template <class X>
+QZ_HD void cta_inf_window(X& x, int wk, int top, int jz, int stop, bool deflate,
+                          MatV H, MatV T, MatV U, MatV V) {
+  for (int j = jz; j < stop; ++j) {
+    double c, s, r;
+    lartg(T(j, j + 1), T(j + 1, j + 1), c, s, r);
+    x.sync();
+    int hc0 = (j > top) ? j - 1 : j;
+    par_rot_rows(x, H, j, j + 1, c, s, hc0, wk);
+    par_rot_rows(x, T, j, j + 1, c, s, j + 2, wk);
+    par_rot_cols(x, U, j, j + 1, c, s, 0, wk);
+    if (x.tid == 0) { T(j, j + 1) = r; T(j + 1, j + 1) = 0.0; }
+    x.sync();
+    if (j > top) {
+      lartg(H(j + 1, j), H(j + 1, j - 1), c, s, r);
+      x.sync();
+      par_rot_cols(x, H, j, j - 1, c, s, 0, j + 1);
+      par_rot_cols(x, T, j, j - 1, c, s, 0, j);
+      par_rot_cols(x, V, j, j - 1, c, s, 0, wk);
+      if (x.tid == 0) { H(j + 1, j) = r; H(j + 1, j - 1) = 0.0; }
+      x.sync();
+    }
+  }
+  if (deflate) {
+    int l = stop;
+    double c, s, r;
+    lartg(H(l, l), H(l, l - 1), c, s, r);
+    x.sync();
+    par_rot_cols(x, H, l, l - 1, c, s, 0, l);
+    par_rot_cols(x, T, l, l - 1, c, s, 0, l);
+    par_rot_cols(x, V, l, l - 1, c, s, 0, wk);
+    if (x.tid == 0) { H(l, l) = r; H(l, l - 1) = 0.0; }
+    x.sync();
+  }
+}
+
+}  // namespace qz

@@ -1,0 +1,832 @@
+// CTA-level QZ algorithms on one square window (one thread block).
+//
+// Each routine is a template over an executor X that supplies
+//   int tid, nt;   thread index / count inside the block
+//   void sync();   block barrier
+//   int* si; double* sd;  small shared scratch (>= 64 ints, >= 256 doubles)
+// On the device X is a thin wrapper over threadIdx/__syncthreads and shared
+// memory.  Data-parallel loops are written "for (i = tid; i < n; i += nt)"
+// and every value that decides control flow is either computed redundantly
+// by all threads from data no thread writes in the same phase, or computed
+// by thread 0 and published through shared scratch across a barrier.
+//
+// Algorithms (all FP64, written from the published mathematics):
+//  * cta_small_qz: implicit double-shift QZ (Moler-Stewart) with zero-
+//    chasing for infinite eigenvalues and 2x2 standardisation; the role of
+//    the reference's serial small QZ kernels QZDACK/QZLAP
+//    (src/kkqz/qzdack.f, src/kkqz/qzlap.f) inside QZEARLY (qzearly.f:229-236)
+//    and of KKQZ in the endgame (PDHGEQZ4.f:329-372).
+//  * cta_swap / cta_move_block: reordering of 1x1/2x2 blocks of a
+//    generalized real Schur form by direct swapping (generalized Sylvester
+//    equation, Kagstrom-Poromaa), the role of DTGEXC/DTGEX2
+//    (src/reorder/dtgexc.f, dtgex2.f) called at qzearly.f:315.
+//  * cta_aed: aggressive early deflation on a window: Schur form, spike
+//    test, reordering, spike reflector, RQ-update of T and Givens
+//    Hessenberg-triangular re-reduction (qzearly.f:229-449).
+#pragma once
+#include "qz_prims.cuh"
+
+namespace qz {
+
+// ---------------------------------------------------------------------------
+// data-parallel helpers
+// ---------------------------------------------------------------------------
+template <class X>
+QZ_HD void par_rot_rows(X& x, MatV M, int r0, int r1, double c, double s, int c_lo, int c_hi) {
+  for (int j = c_lo + x.tid; j < c_hi; j += x.nt) {
+    double a = M(r0, j), b = M(r1, j);
+    M(r0, j) = c * a + s * b;
+    M(r1, j) = -s * a + c * b;
+  }
+}
+template <class X>
+QZ_HD void par_rot_cols(X& x, MatV M, int c0, int c1, double c, double s, int r_lo, int r_hi) {
+  for (int i = r_lo + x.tid; i < r_hi; i += x.nt) {
+    double a = M(i, c0), b = M(i, c1);
+    M(i, c0) = c * a + s * b;
+    M(i, c1) = -s * a + c * b;
+  }
+}
+template <class X>
+QZ_HD void par_refl_rows(X& x, MatV M, int r, double tau, double v1, double v2, int c_lo, int c_hi) {
+  for (int j = c_lo + x.tid; j < c_hi; j += x.nt) {
+    double a0 = M(r, j), a1 = M(r + 1, j), a2 = M(r + 2, j);
+    refl3(tau, v1, v2, a0, a1, a2);
+    M(r, j) = a0; M(r + 1, j) = a1; M(r + 2, j) = a2;
+  }
+}
+template <class X>
+QZ_HD void par_refl_cols(X& x, MatV M, int c, double tau, double v1, double v2, int r_lo, int r_hi) {
+  for (int i = r_lo + x.tid; i < r_hi; i += x.nt) {
+    double a0 = M(i, c), a1 = M(i, c + 1), a2 = M(i, c + 2);
+    refl3(tau, v1, v2, a0, a1, a2);
+    M(i, c) = a0; M(i, c + 1) = a1; M(i, c + 2) = a2;
+  }
+}
+template <class X>
+QZ_HD void par_neg_row(X& x, MatV M, int r, int c_lo, int c_hi) {
+  for (int j = c_lo + x.tid; j < c_hi; j += x.nt) M(r, j) = -M(r, j);
+}
+template <class X>
+QZ_HD void par_neg_col(X& x, MatV M, int c, int r_lo, int r_hi) {
+  for (int i = r_lo + x.tid; i < r_hi; i += x.nt) M(i, c) = -M(i, c);
+}
+template <class X>
+QZ_HD void par_set_identity(X& x, MatV M, int n) {
+  for (int k = x.tid; k < n * n; k += x.nt) {
+    int i = k % n, j = k / n;
+    M(i, j) = (i == j) ? 1.0 : 0.0;
+  }
+}
+
+// Window state shared by the routines below.  Q and Z accumulate the left
+// and right transformations of the window (H_in = Q H_out Z^T).
+struct WinState {
+  int n;
+  MatV H, T, Q, Z;
+  bool wantq, wantz;
+  Tol tol;
+};
+
+// ---------------------------------------------------------------------------
+// 2x2 standardisation of block (j, j+1) inside the window.
+// Applies rotations to rows/cols of the whole window (Schur mode).
+// ---------------------------------------------------------------------------
+template <class X>
+QZ_HD void cta_std2x2(X& x, WinState& w, int j) {
+  // every thread computes the same rotations from the same 8 values
+  double A[4] = {w.H(j, j), w.H(j + 1, j), w.H(j, j + 1), w.H(j + 1, j + 1)};
+  double B[4] = {w.T(j, j), w.T(j + 1, j), w.T(j, j + 1), w.T(j + 1, j + 1)};
+  Std2 o;
+  std2x2(A, B, o);
+  x.sync();  // all reads of the block done before anyone writes
+  int n = w.n;
+  // rows: columns j+2..n-1 (the block itself is written from o.a/o.b)
+  par_rot_rows(x, w.H, j, j + 1, o.csl, o.snl, j + 2, n);
+  par_rot_rows(x, w.T, j, j + 1, o.csl, o.snl, j + 2, n);
+  if (w.wantq) par_rot_cols(x, w.Q, j, j + 1, o.csl, o.snl, 0, n);
+  // cols: rows 0..j-1
+  par_rot_cols(x, w.H, j, j + 1, o.csr, o.snr, 0, j);
+  par_rot_cols(x, w.T, j, j + 1, o.csr, o.snr, 0, j);
+  if (w.wantz) par_rot_cols(x, w.Z, j, j + 1, o.csr, o.snr, 0, n);
+  x.sync();
+  if (o.negrow0) {
+    par_neg_row(x, w.H, j, j + 2, n);
+    par_neg_row(x, w.T, j, j + 2, n);
+    if (w.wantq) par_neg_col(x, w.Q, j, 0, n);
+  }
+  if (o.negrow1) {
+    par_neg_row(x, w.H, j + 1, j + 2, n);
+    par_neg_row(x, w.T, j + 1, j + 2, n);
+    if (w.wantq) par_neg_col(x, w.Q, j + 1, 0, n);
+  }
+  if (x.tid == 0) {
+    w.H(j, j) = o.a[0]; w.H(j + 1, j) = o.a[1]; w.H(j, j + 1) = o.a[2]; w.H(j + 1, j + 1) = o.a[3];
+    w.T(j, j) = o.b[0]; w.T(j + 1, j) = 0.0;    w.T(j, j + 1) = o.b[2]; w.T(j + 1, j + 1) = o.b[3];
+  }
+  x.sync();
+}
+
+// ---------------------------------------------------------------------------
+// Infinite eigenvalues: zero at T(jz,jz) in the active block [f, l].
+// ---------------------------------------------------------------------------
+// top of the block: row rotation zeroing H(f+1,f) splits off the 1x1 (inf)
+template <class X>
+QZ_HD void cta_inf_top(X& x, WinState& w, int f) {
+  double c, s, r;
+  lartg(w.H(f, f), w.H(f + 1, f), c, s, r);
+  x.sync();
+  par_rot_rows(x, w.H, f, f + 1, c, s, f + 1, w.n);
+  par_rot_rows(x, w.T, f, f + 1, c, s, f + 1, w.n);
+  if (w.wantq) par_rot_cols(x, w.Q, f, f + 1, c, s, 0, w.n);
+  if (x.tid == 0) { w.H(f, f) = r; w.H(f + 1, f) = 0.0; }
+  x.sync();
+}
+// bottom of the block: T(l,l)=0, column rotation zeroing H(l,l-1)
+template <class X>
+QZ_HD void cta_inf_bottom(X& x, WinState& w, int l) {
+  double c, s, r;
+  // pair (col l, col l-1): zero the second entry of row l
+  lartg(w.H(l, l), w.H(l, l - 1), c, s, r);
+  x.sync();
+  par_rot_cols(x, w.H, l, l - 1, c, s, 0, l);
+  par_rot_cols(x, w.T, l, l - 1, c, s, 0, l);
+  if (w.wantz) par_rot_cols(x, w.Z, l, l - 1, c, s, 0, w.n);
+  if (x.tid == 0) { w.H(l, l) = r; w.H(l, l - 1) = 0.0; }
+  x.sync();
+}
+// chase the zero at T(jz,jz) down to T(l,l) (Moler-Stewart zero chasing)
+template <class X>
+QZ_HD void cta_inf_chase_down(X& x, WinState& w, int f, int jz, int l) {
+  int n = w.n;
+  for (int j = jz; j < l; ++j) {
+    double c, s, r;
+    // (a) rows (j, j+1): zero T(j+1,j+1)
+    lartg(w.T(j, j + 1), w.T(j + 1, j + 1), c, s, r);
+    x.sync();
+    int hc0 = (j > f) ? j - 1 : j;
+    par_rot_rows(x, w.H, j, j + 1, c, s, hc0, n);
+    par_rot_rows(x, w.T, j, j + 1, c, s, j + 2, n);
+    if (w.wantq) par_rot_cols(x, w.Q, j, j + 1, c, s, 0, n);
+    if (x.tid == 0) { w.T(j, j + 1) = r; w.T(j + 1, j + 1) = 0.0; }
+    x.sync();
+    if (j > f) {
+      // (b) cols (j, j-1): zero H(j+1, j-1)
+      lartg(w.H(j + 1, j), w.H(j + 1, j - 1), c, s, r);
+      x.sync();
+      par_rot_cols(x, w.H, j, j - 1, c, s, 0, j + 1);
+      par_rot_cols(x, w.T, j, j - 1, c, s, 0, j);
+      if (w.wantz) par_rot_cols(x, w.Z, j, j - 1, c, s, 0, n);
+      if (x.tid == 0) { w.H(j + 1, j) = r; w.H(j + 1, j - 1) = 0.0; }
+      x.sync();
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// One implicit double-shift QZ sweep over the active block [f, l]
+// (l - f + 1 >= 3) with shift polynomial c2*M^2 - c1*M + c0.
+// ---------------------------------------------------------------------------
+template <class X>
+QZ_HD void cta_ds_sweep(X& x, WinState& w, int f, int l, double c2, double c1, double c0) {
+  int n = w.n;
+  for (int j = f; j < l; ++j) {
+    if (j < l - 1) {
+      // ---- 3x3 step at rows/cols j..j+2 ----
+      double a0, a1, a2;
+      if (j == f) {
+        shift_column(w.H(f, f), w.H(f + 1, f), w.H(f, f + 1), w.H(f + 1, f + 1), w.H(f + 2, f + 1),
+                     w.T(f, f), w.T(f, f + 1), w.T(f + 1, f + 1), c2, c1, c0, a0, a1, a2);
+      } else {
+        a0 = w.H(j, j - 1); a1 = w.H(j + 1, j - 1); a2 = w.H(j + 2, j - 1);
+      }
+      double tau, v1 = a1, v2 = a2, beta = a0;
+      larfg3(beta, v1, v2, tau);
+      double tb[9];
+      for (int cc = 0; cc < 3; ++cc)
+        for (int rr = 0; rr < 3; ++rr) tb[rr + 3 * cc] = w.T(j + rr, j + cc);
+      for (int cc = 0; cc < 3; ++cc) refl3(tau, v1, v2, tb[3 * cc], tb[3 * cc + 1], tb[3 * cc + 2]);
+      double taur, u1, u2;
+      opposite_reflector3(tb, taur, u1, u2);
+      for (int rr = 0; rr < 3; ++rr) refl3(taur, u1, u2, tb[rr], tb[rr + 3], tb[rr + 6]);
+      tb[1] = 0.0; tb[2] = 0.0;
+      x.sync();  // everyone has read H(.,j-1) and the T block
+      par_refl_rows(x, w.H, j, tau, v1, v2, j, n);
+      par_refl_rows(x, w.T, j, tau, v1, v2, j + 3, n);
+      if (w.wantq) par_refl_cols(x, w.Q, j, tau, v1, v2, 0, n);
+      x.sync();
+      int hr = (j + 4 < l + 1) ? j + 4 : l + 1;
+      par_refl_cols(x, w.H, j, taur, u1, u2, 0, hr);
+      par_refl_cols(x, w.T, j, taur, u1, u2, 0, j);
+      if (w.wantz) par_refl_cols(x, w.Z, j, taur, u1, u2, 0, n);
+      if (x.tid == 0) {
+        for (int cc = 0; cc < 3; ++cc)
+          for (int rr = 0; rr < 3; ++rr) w.T(j + rr, j + cc) = tb[rr + 3 * cc];
+        if (j > f) { w.H(j, j - 1) = beta; w.H(j + 1, j - 1) = 0.0; w.H(j + 2, j - 1) = 0.0; }
+      }
+      x.sync();
+    } else {
+      // ---- final 2x2 step at rows/cols l-1, l ----
+      double c, s, r;
+      lartg(w.H(j, j - 1), w.H(j + 1, j - 1), c, s, r);
+      double t00 = w.T(j, j), t01 = w.T(j, j + 1), t10 = w.T(j + 1, j), t11 = w.T(j + 1, j + 1);
+      rot2(c, s, t00, t10);
+      rot2(c, s, t01, t11);
+      double cr, sr;
+      opposite_rot2(t10, t11, cr, sr);
+      rot2(cr, sr, t00, t01);
+      rot2(cr, sr, t10, t11);
+      t10 = 0.0;
+      x.sync();
+      par_rot_rows(x, w.H, j, j + 1, c, s, j, n);
+      par_rot_rows(x, w.T, j, j + 1, c, s, j + 2, n);
+      if (w.wantq) par_rot_cols(x, w.Q, j, j + 1, c, s, 0, n);
+      x.sync();
+      par_rot_cols(x, w.H, j, j + 1, cr, sr, 0, l + 1);
+      par_rot_cols(x, w.T, j, j + 1, cr, sr, 0, j);
+      if (w.wantz) par_rot_cols(x, w.Z, j, j + 1, cr, sr, 0, n);
+      if (x.tid == 0) {
+        w.T(j, j) = t00; w.T(j + 1, j) = 0.0; w.T(j, j + 1) = t01; w.T(j + 1, j + 1) = t11;
+        w.H(j, j - 1) = r; w.H(j + 1, j - 1) = 0.0;
+      }
+      x.sync();
+    }
+  }
+}
+
+// negligible-subdiagonal test shared by all deflation scans
+QZ_HD bool negligible_sub(double hsub, double hkm1, double hkk, const Tol& t) {
+  double tst = fabs(hkm1) + fabs(hkk);
+  return fabs(hsub) <= dmax(t.smlnum, t.ulp * tst);
+}
+
+// ---------------------------------------------------------------------------
+// Small QZ: reduce the whole window (n x n) to generalized real Schur form.
+// Returns 0 on success, or ilast+1 (1-based index of the last unconverged
+// row) if maxit iterations did not suffice.
+// ---------------------------------------------------------------------------
+template <class X>
+QZ_HD int cta_small_qz(X& x, WinState& w, int maxit) {
+  int n = w.n;
+  int ilast = n - 1;
+  int iiter = 0, jiter = 0;
+  while (ilast >= 0) {
+    if (x.tid == 0) {
+      int ifirst = 0;
+      for (int j = ilast; j >= 1; --j) {
+        double tst = fabs(w.H(j - 1, j - 1)) + fabs(w.H(j, j));
+        if (tst == 0.0) tst = fabs(w.H(j - 1, j)) + fabs(w.H(j, j - 1));
+        if (fabs(w.H(j, j - 1)) <= dmax(w.tol.smlnum, w.tol.ulp * tst)) {
+          w.H(j, j - 1) = 0.0;
+          ifirst = j;
+          break;
+        }
+      }
+      int jz = -1;
+      for (int j = ilast; j >= ifirst; --j) {
+        if (fabs(w.T(j, j)) <= w.tol.ttol) { w.T(j, j) = 0.0; jz = j; break; }
+      }
+      x.si[0] = ifirst;
+      x.si[1] = jz;
+    }
+    x.sync();
+    int ifirst = x.si[0], jz = x.si[1];
+    x.sync();
+    if (ifirst == ilast) { ilast -= 1; iiter = 0; continue; }
+    if (jz >= 0) {
+      if (jz == ifirst) {
+        cta_inf_top(x, w, ifirst);
+      } else {
+        if (jz < ilast) cta_inf_chase_down(x, w, ifirst, jz, ilast);
+        cta_inf_bottom(x, w, ilast);
+        ilast -= 1;
+      }
+      iiter = 0;
+      continue;
+    }
+    if (ifirst + 1 == ilast) {
+      cta_std2x2(x, w, ifirst);
+      ilast -= 2;
+      iiter = 0;
+      continue;
+    }
+    ++iiter;
+    ++jiter;
+    if (jiter > maxit) return ilast + 1;
+    double c2, c1, c0;
+    int l = ilast;
+    if (iiter % 10 == 0) {
+      // exceptional shift from the bottom subdiagonals
+      double sc = fabs(w.H(l, l - 1) / w.T(l - 1, l - 1)) + fabs(w.H(l - 1, l - 2) / w.T(l - 2, l - 2));
+      double h11 = 0.75 * sc + w.H(l, l) / w.T(l, l);
+      c2 = 1.0;
+      c1 = 2.0 * h11;
+      c0 = h11 * h11 + 0.4375 * sc * sc;
+    } else {
+      pencil2_poly(w.H(l - 1, l - 1), w.H(l, l - 1), w.H(l - 1, l), w.H(l, l),
+                   w.T(l - 1, l - 1), w.T(l - 1, l), w.T(l, l), c2, c1, c0);
+    }
+    cta_ds_sweep(x, w, ifirst, ilast, c2, c1, c0);
+  }
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// Block swapping (reordering) of a generalized real Schur form.
+// ---------------------------------------------------------------------------
+// Small dense helpers on m x m (m <= 4) column-major arrays.
+QZ_HD void small_mm(int m, const double* A, const double* B, double* C, bool ta, bool tb) {
+  for (int i = 0; i < m; ++i)
+    for (int j = 0; j < m; ++j) {
+      double acc = 0.0;
+      for (int k = 0; k < m; ++k) {
+        double a = ta ? A[k + m * i] : A[i + m * k];
+        double b = tb ? B[j + m * k] : B[k + m * j];
+        acc += a * b;
+      }
+      C[i + m * j] = acc;
+    }
+}
+
+// Full orthogonal Q (m x m) from Householder QR of the m x k matrix X
+// (column-major, ld m); the first k columns of Q span range(X).
+QZ_HD void small_qr_q(int m, int k, double* X, double* Q) {
+  for (int i = 0; i < m * m; ++i) Q[i] = 0.0;
+  for (int i = 0; i < m; ++i) Q[i + m * i] = 1.0;
+  for (int c = 0; c < k; ++c) {
+    // reflector for X(c:m, c)
+    double nrm = 0.0, mx = 0.0;
+    for (int i = c; i < m; ++i) mx = dmax(mx, fabs(X[i + m * c]));
+    if (mx == 0.0) continue;
+    for (int i = c; i < m; ++i) { double t = X[i + m * c] / mx; nrm += t * t; }
+    nrm = sqrt(nrm) * mx;
+    double alpha = X[c + m * c];
+    double beta = -dsign(nrm, alpha);
+    double v[4];
+    v[0] = 1.0;
+    double sc = 1.0 / (alpha - beta);
+    for (int i = c + 1; i < m; ++i) v[i - c] = X[i + m * c] * sc;
+    double tau = (beta - alpha) / beta;
+    // apply to X(:, c:k) and accumulate Q = Q * P
+    for (int j = c; j < k; ++j) {
+      double t = 0.0;
+      for (int i = c; i < m; ++i) t += v[i - c] * X[i + m * j];
+      t *= tau;
+      for (int i = c; i < m; ++i) X[i + m * j] -= t * v[i - c];
+    }
+    for (int i = 0; i < m; ++i) {
+      double t = 0.0;
+      for (int r = c; r < m; ++r) t += Q[i + m * r] * v[r - c];
+      t *= tau;
+      for (int r = c; r < m; ++r) Q[i + m * r] -= t * v[r - c];
+    }
+  }
+}
+
+// Gaussian elimination with complete pivoting on an s x s system (s <= 8).
+// Tiny pivots are replaced by smin (the DGETC2 device); returns false if
+// that happened (swap then needs the stability test to decide).
+QZ_HD bool small_solve_cp(int s, double* M, double* rhs, double smin) {
+  int perm_r[8], perm_c[8];
+  bool exact = true;
+  for (int i = 0; i < s; ++i) { perm_r[i] = i; perm_c[i] = i; }
+  for (int k = 0; k < s; ++k) {
+    int pi = k, pj = k;
+    double best = -1.0;
+    for (int i = k; i < s; ++i)
+      for (int j = k; j < s; ++j) {
+        double v = fabs(M[i + 8 * j]);
+        if (v > best) { best = v; pi = i; pj = j; }
+      }
+    if (pi != k) {
+      for (int j = 0; j < s; ++j) { double t = M[k + 8 * j]; M[k + 8 * j] = M[pi + 8 * j]; M[pi + 8 * j] = t; }
+      double t = rhs[k]; rhs[k] = rhs[pi]; rhs[pi] = t;
+    }
+    if (pj != k) {
+      for (int i = 0; i < s; ++i) { double t = M[i + 8 * k]; M[i + 8 * k] = M[i + 8 * pj]; M[i + 8 * pj] = t; }
+      int t = perm_c[k]; perm_c[k] = perm_c[pj]; perm_c[pj] = t;
+    }
+    if (fabs(M[k + 8 * k]) < smin) { M[k + 8 * k] = smin; exact = false; }
+    double piv = M[k + 8 * k];
+    for (int i = k + 1; i < s; ++i) {
+      double f = M[i + 8 * k] / piv;
+      if (f == 0.0) continue;
+      for (int j = k + 1; j < s; ++j) M[i + 8 * j] -= f * M[k + 8 * j];
+      rhs[i] -= f * rhs[k];
+      M[i + 8 * k] = 0.0;
+    }
+  }
+  double y[8];
+  for (int k = s - 1; k >= 0; --k) {
+    double acc = rhs[k];
+    for (int j = k + 1; j < s; ++j) acc -= M[k + 8 * j] * y[j];
+    y[k] = acc / M[k + 8 * k];
+  }
+  for (int k = 0; k < s; ++k) rhs[perm_c[k]] = y[k];
+  (void)perm_r;
+  return exact;
+}
+
+// Compute the orthogonal Qs, Zs (m x m, m = n1+n2) that swap the diagonal
+// blocks of the m x m pencil (S, T) (upper block triangular, column-major
+// ld m).  On success S, T are overwritten by Qs^T S Zs, Qs^T T Zs with the
+// lower-left n1 x n2 ... n2-row block exactly zero.  Returns false if the
+// swap fails the weak stability test (then nothing should be applied).
+QZ_HD bool swap_compute(int n1, int n2, double* S, double* T, double* Qs, double* Zs, double ulp, double smlnum) {
+  int m = n1 + n2;
+  // ||(S,T)||_F
+  double fn = 0.0;
+  for (int i = 0; i < m * m; ++i) fn += S[i] * S[i] + T[i] * T[i];
+  fn = sqrt(fn);
+  double thresh = dmax(20.0 * ulp * fn, smlnum);
+  // generalized Sylvester system in unknowns vec(R) (n1*n2), vec(L) (n1*n2)
+  //   A11 R - L A22 = -A12,  B11 R - L B22 = -B12
+  int q = n1 * n2;
+  int s = 2 * q;
+  double M[64];
+  double rhs[8];
+  for (int i = 0; i < 64; ++i) M[i] = 0.0;
+  for (int j = 0; j < n2; ++j)
+    for (int i = 0; i < n1; ++i) {
+      int row = i + n1 * j;  // equation index for entry (i,j)
+      // A11 R : sum_k A11(i,k) R(k,j)
+      for (int k = 0; k < n1; ++k) {
+        M[row + 8 * (k + n1 * j)] += S[i + m * k];
+        M[(row + q) + 8 * (k + n1 * j)] += T[i + m * k];
+      }
+      // - L A22 : - sum_k L(i,k) A22(k,j)
+      for (int k = 0; k < n2; ++k) {
+        M[row + 8 * (q + i + n1 * k)] -= S[(n1 + k) + m * (n1 + j)];
+        M[(row + q) + 8 * (q + i + n1 * k)] -= T[(n1 + k) + m * (n1 + j)];
+      }
+      rhs[row] = -S[i + m * (n1 + j)];
+      rhs[row + q] = -T[i + m * (n1 + j)];
+    }
+  double smin = dmax(ulp * fn * 1e-3, smlnum);
+  small_solve_cp(s, M, rhs, smin);
+  for (int i = 0; i < s; ++i)
+    if (!isfinite(rhs[i])) return false;
+  // [R; I] and [L; I] (m x n2)
+  double XR[16], XL[16];
+  for (int j = 0; j < n2; ++j) {
+    for (int i = 0; i < n1; ++i) {
+      XR[i + m * j] = rhs[i + n1 * j];
+      XL[i + m * j] = rhs[q + i + n1 * j];
+    }
+    for (int i = 0; i < n2; ++i) {
+      XR[n1 + i + m * j] = (i == j) ? 1.0 : 0.0;
+      XL[n1 + i + m * j] = (i == j) ? 1.0 : 0.0;
+    }
+  }
+  small_qr_q(m, n2, XR, Zs);
+  small_qr_q(m, n2, XL, Qs);
+  double tmp[16], S2[16], T2[16];
+  small_mm(m, S, Zs, tmp, false, false);
+  small_mm(m, Qs, tmp, S2, true, false);
+  small_mm(m, T, Zs, tmp, false, false);
+  small_mm(m, Qs, tmp, T2, true, false);
+  double ll = 0.0;
+  for (int j = 0; j < n2; ++j)
+    for (int i = n2; i < m; ++i) ll += S2[i + m * j] * S2[i + m * j] + T2[i + m * j] * T2[i + m * j];
+  if (!(sqrt(ll) <= thresh)) return false;
+  for (int j = 0; j < n2; ++j)
+    for (int i = n2; i < m; ++i) { S2[i + m * j] = 0.0; T2[i + m * j] = 0.0; }
+  // 1x1 diagonal blocks of T: nothing below the diagonal
+  if (n2 == 1) {}
+  if (n1 == 1) {}
+  for (int i = 0; i < m * m; ++i) { S[i] = S2[i]; T[i] = T2[i]; }
+  return true;
+}
+
+// Swap the blocks at j1 (size n1) and j1+n1 (size n2) of the window.
+// Thread 0 computes, everyone applies.  Returns false (nothing changed)
+// if the swap was rejected.
+template <class X>
+QZ_HD bool cta_swap(X& x, WinState& w, int j1, int n1, int n2) {
+  int m = n1 + n2;
+  double* sQ = x.sd;       // 16
+  double* sZ = x.sd + 16;  // 16
+  double* sS = x.sd + 32;  // 16
+  double* sT = x.sd + 48;  // 16
+  if (x.tid == 0) {
+    for (int c = 0; c < m; ++c)
+      for (int r = 0; r < m; ++r) {
+        sS[r + m * c] = w.H(j1 + r, j1 + c);
+        sT[r + m * c] = w.T(j1 + r, j1 + c);
+      }
+    bool ok = swap_compute(n1, n2, sS, sT, sQ, sZ, w.tol.ulp, w.tol.smlnum);
+    x.si[2] = ok ? 1 : 0;
+  }
+  x.sync();
+  bool ok = x.si[2] != 0;
+  if (!ok) { x.sync(); return false; }
+  int n = w.n;
+  // rows j1..j1+m-1, cols j1+m..n-1 : Qs^T * rows
+  for (int j = j1 + m + x.tid; j < n; j += x.nt) {
+    double hv[4], tv[4];
+    for (int r = 0; r < m; ++r) { hv[r] = w.H(j1 + r, j); tv[r] = w.T(j1 + r, j); }
+    for (int r = 0; r < m; ++r) {
+      double ah = 0.0, at = 0.0;
+      for (int k = 0; k < m; ++k) { ah += sQ[k + m * r] * hv[k]; at += sQ[k + m * r] * tv[k]; }
+      w.H(j1 + r, j) = ah; w.T(j1 + r, j) = at;
+    }
+  }
+  // cols j1..j1+m-1, rows 0..j1-1 : cols * Zs
+  for (int i = x.tid; i < j1; i += x.nt) {
+    double hv[4], tv[4];
+    for (int c = 0; c < m; ++c) { hv[c] = w.H(i, j1 + c); tv[c] = w.T(i, j1 + c); }
+    for (int c = 0; c < m; ++c) {
+      double ah = 0.0, at = 0.0;
+      for (int k = 0; k < m; ++k) { ah += hv[k] * sZ[k + m * c]; at += tv[k] * sZ[k + m * c]; }
+      w.H(i, j1 + c) = ah; w.T(i, j1 + c) = at;
+    }
+  }
+  if (w.wantq)
+    for (int i = x.tid; i < n; i += x.nt) {
+      double v[4];
+      for (int c = 0; c < m; ++c) v[c] = w.Q(i, j1 + c);
+      for (int c = 0; c < m; ++c) {
+        double a = 0.0;
+        for (int k = 0; k < m; ++k) a += v[k] * sQ[k + m * c];
+        w.Q(i, j1 + c) = a;
+      }
+    }
+  if (w.wantz)
+    for (int i = x.tid; i < n; i += x.nt) {
+      double v[4];
+      for (int c = 0; c < m; ++c) v[c] = w.Z(i, j1 + c);
+      for (int c = 0; c < m; ++c) {
+        double a = 0.0;
+        for (int k = 0; k < m; ++k) a += v[k] * sZ[k + m * c];
+        w.Z(i, j1 + c) = a;
+      }
+    }
+  if (x.tid == 0) {
+    for (int c = 0; c < m; ++c)
+      for (int r = 0; r < m; ++r) {
+        w.H(j1 + r, j1 + c) = sS[r + m * c];
+        w.T(j1 + r, j1 + c) = sT[r + m * c];
+      }
+  }
+  x.sync();
+  // re-standardise the new diagonal blocks (moved block first, size n2)
+  if (n2 == 2) cta_std2x2(x, w, j1);
+  if (n1 == 2) cta_std2x2(x, w, j1 + n2);
+  return true;
+}
+
+// Move the block starting at ifst (size nb) up to position ilst
+// (DTGEXC semantics for ifst > ilst).  Returns false on a rejected swap.
+template <class X>
+QZ_HD bool cta_move_block(X& x, WinState& w, int ifst, int nb, int ilst) {
+  int here = ifst;
+  while (here > ilst) {
+    int nbn = 1;
+    if (here - 2 >= ilst && w.H(here - 1, here - 2) != 0.0) nbn = 2;
+    x.sync();
+    if (!cta_swap(x, w, here - nbn, nbn, nb)) return false;
+    here -= nbn;
+    // the moved block must keep its size (a complex pair stays 2x2)
+    int nbnow = (nb == 2 && w.H(here + 1, here) != 0.0) ? 2 : 1;
+    x.sync();
+    if (nbnow != nb) return false;
+  }
+  return true;
+}
+
+// ---------------------------------------------------------------------------
+// Aggressive early deflation on a window (already copied into w, with
+// w.Q = w.Z = I).  s is the spike H(kwtop, kwtop-1) (0 at the top of the
+// active block).  On return:
+//   si[8]  = number of undeflated eigenvalues m (positions 0..m-1)
+//   si[9]  = status (0 ok, >0 small QZ failed)
+//   si[10] = 1 if the window was transformed (nd > 0 or full solve)
+//   sd[128..] unused
+// shifts (alphar, alphai, beta) of the undeflated eigenvalues are written
+// to sr/si_/sb (length >= m) by thread 0 before the spike reflector is
+// applied.  When nothing deflates the window is left in Schur form but the
+// caller discards it (the pencil is unchanged).
+// ---------------------------------------------------------------------------
+template <class X>
+QZ_HD void cta_aed(X& x, WinState& w, double s, double* sr, double* si_, double* sb, int maxit) {
+  int n = w.n;
+  int info = cta_small_qz(x, w, maxit);
+  if (info != 0) {
+    if (x.tid == 0) { x.si[8] = n; x.si[9] = info; x.si[10] = 0; }
+    x.sync();
+    return;
+  }
+  // ---- spike test with reordering (qzearly.f:253-365) ----
+  int kb = n - 1, ilst = 0;
+  bool failed = false;
+  while (kb >= ilst) {
+    bool bulge = (kb > ilst) && (w.H(kb, kb - 1) != 0.0);
+    bool dfl;
+    if (!bulge) {
+      double temp = fabs(s) + fabs(w.H(kb, kb));
+      dfl = fabs(s * w.Q(0, kb)) <= dmax(w.tol.ulp * temp, w.tol.smlnum);
+    } else {
+      double h11 = w.H(kb - 1, kb - 1), h21 = w.H(kb, kb - 1), h12 = w.H(kb - 1, kb), h22 = w.H(kb, kb);
+      double rtdet;
+      if (h11 == 0.0 && h21 == 0.0) rtdet = 0.0;
+      else if (fabs(h11) >= fabs(h21)) rtdet = sqrt(fabs(h11)) * sqrt(fabs(h22 - (h21 / h11) * h12));
+      else rtdet = sqrt(fabs(h21)) * sqrt(fabs(h12 - (h11 / h21) * h22));
+      double temp = fabs(s) + rtdet;
+      dfl = dmax(fabs(s * w.Q(0, kb)), fabs(s * w.Q(0, kb - 1))) <= dmax(w.tol.ulp * temp, w.tol.smlnum);
+    }
+    x.sync();
+    int nb = bulge ? 2 : 1;
+    if (dfl) {
+      kb -= nb;
+    } else {
+      if (!cta_move_block(x, w, kb - nb + 1, nb, ilst)) { failed = true; break; }
+      ilst += nb;
+    }
+  }
+  (void)failed;
+  int m = kb + 1;  // undeflated eigenvalues at 0..m-1
+  // ---- shifts: eigenvalues of the undeflated Schur blocks ----
+  if (x.tid == 0) {
+    int j = 0;
+    while (j < m) {
+      if (j + 1 < m && w.H(j + 1, j) != 0.0) {
+        double c2, c1, c0;
+        pencil2_poly(w.H(j, j), w.H(j + 1, j), w.H(j, j + 1), w.H(j + 1, j + 1),
+                     w.T(j, j), w.T(j, j + 1), w.T(j + 1, j + 1), c2, c1, c0);
+        // complex pair (or real pair if rounding says so): store as
+        // lambda = (c1 +- sqrt(disc)) / (2 c2)
+        double disc = c1 * c1 - 4.0 * c2 * c0;
+        if (disc < 0.0) {
+          sr[j] = c1; si_[j] = sqrt(-disc); sb[j] = 2.0 * c2;
+          sr[j + 1] = c1; si_[j + 1] = -sqrt(-disc); sb[j + 1] = 2.0 * c2;
+        } else {
+          double sq = sqrt(disc);
+          sr[j] = c1 + sq; si_[j] = 0.0; sb[j] = 2.0 * c2;
+          sr[j + 1] = c1 - sq; si_[j + 1] = 0.0; sb[j + 1] = 2.0 * c2;
+        }
+        j += 2;
+      } else {
+        sr[j] = w.H(j, j); si_[j] = 0.0; sb[j] = w.T(j, j);
+        j += 1;
+      }
+    }
+    x.si[8] = m;
+    x.si[9] = 0;
+    x.si[10] = (m < n) ? 1 : 0;
+  }
+  x.sync();
+  if (m == n || m <= 1 || s == 0.0) {
+    // nothing deflated (caller discards), or nothing left to re-reduce
+    x.sync();
+    return;
+  }
+  // ---- spike reflector from Q(0, 0:m-1) (qzearly.f:371-381) ----
+  double* v = x.sd + 64;  // length m (<= n); caller guarantees room
+  if (x.tid == 0) {
+    double alpha = w.Q(0, 0);
+    double mx = 0.0;
+    for (int i = 1; i < m; ++i) mx = dmax(mx, fabs(w.Q(0, i)));
+    double tau = 0.0;
+    v[0] = 1.0;
+    if (mx > 0.0) {
+      double ma = dmax(mx, fabs(alpha));
+      double nrm = 0.0;
+      nrm += (alpha / ma) * (alpha / ma);
+      for (int i = 1; i < m; ++i) { double t = w.Q(0, i) / ma; nrm += t * t; }
+      nrm = sqrt(nrm) * ma;
+      double beta = -dsign(nrm, alpha);
+      tau = (beta - alpha) / beta;
+      double sc = 1.0 / (alpha - beta);
+      for (int i = 1; i < m; ++i) v[i] = w.Q(0, i) * sc;
+    } else {
+      for (int i = 1; i < m; ++i) v[i] = 0.0;
+    }
+    x.sd[63] = tau;
+  }
+  x.sync();
+  double tau = x.sd[63];
+  if (tau != 0.0) {
+    // H(0:m, :) <- P H ; T(0:m, m:n) <- P T ; Q(:, 0:m) <- Q P
+    for (int j = x.tid; j < n; j += x.nt) {
+      double t = 0.0;
+      for (int i = 0; i < m; ++i) t += v[i] * w.H(i, j);
+      t *= tau;
+      for (int i = 0; i < m; ++i) w.H(i, j) -= t * v[i];
+      if (j >= m) {
+        double u = 0.0;
+        for (int i = 0; i < m; ++i) u += v[i] * w.T(i, j);
+        u *= tau;
+        for (int i = 0; i < m; ++i) w.T(i, j) -= u * v[i];
+      }
+    }
+    if (w.wantq)
+      for (int r = x.tid; r < n; r += x.nt) {
+        double t = 0.0;
+        for (int i = 0; i < m; ++i) t += w.Q(r, i) * v[i];
+        t *= tau;
+        for (int i = 0; i < m; ++i) w.Q(r, i) -= t * v[i];
+      }
+    // RQ update of the leading m x m block of T:  T' = T + v*wv^T with
+    // wv = -tau T^T v  (qzearly.f:396-446)
+    double* wv = x.sd + 64 + n;  // length m
+    for (int j = x.tid; j < m; j += x.nt) {
+      double t = 0.0;
+      for (int i = 0; i <= j; ++i) t += w.T(i, j) * v[i];
+      wv[j] = -tau * t;
+    }
+    x.sync();
+    // pass 1 rotations (depend on wv only): zero wv(i) into wv(i+1)
+    double* rc = x.sd + 64 + 2 * n;      // length m
+    double* rs = x.sd + 64 + 3 * n;      // length m
+    if (x.tid == 0) {
+      double wl = wv[0];
+      for (int i = 0; i < m - 1; ++i) {
+        double c, sn, r;
+        lartg(wv[i + 1], wl, c, sn, r);
+        // column op on (col i, col i+1): col_i' = c col_i - sn col_{i+1}
+        //                                col_{i+1}' = sn col_i + c col_{i+1}
+        rc[i] = c; rs[i] = sn;
+        wl = r;
+      }
+      x.sd[62] = wl;  // final wv(m-1)
+    }
+    x.sync();
+    // apply pass 1 row by row to T (rows 0..m-1), H (rows 0..m-1), Z (all rows)
+    for (int r = x.tid; r < n; r += x.nt) {
+      if (r < m) {
+        for (int i = (r > 0 ? r - 1 : 0); i < m - 1; ++i) {
+          double a = w.T(r, i), b = w.T(r, i + 1);
+          w.T(r, i) = rc[i] * a - rs[i] * b;
+          w.T(r, i + 1) = rs[i] * a + rc[i] * b;
+        }
+        for (int i = 0; i < m - 1; ++i) {
+          double a = w.H(r, i), b = w.H(r, i + 1);
+          w.H(r, i) = rc[i] * a - rs[i] * b;
+          w.H(r, i + 1) = rs[i] * a + rc[i] * b;
+        }
+      }
+      if (w.wantz)
+        for (int i = 0; i < m - 1; ++i) {
+          double a = w.Z(r, i), b = w.Z(r, i + 1);
+          w.Z(r, i) = rc[i] * a - rs[i] * b;
+          w.Z(r, i + 1) = rs[i] * a + rc[i] * b;
+        }
+    }
+    x.sync();
+    double wl = x.sd[62];
+    for (int i = x.tid; i < m; i += x.nt) w.T(i, m - 1) += wl * v[i];
+    x.sync();
+    // pass 2: zero the subdiagonal of T from the bottom
+    for (int i = m - 2; i >= 0; --i) {
+      double c, sn, r;
+      lartg(w.T(i + 1, i + 1), w.T(i + 1, i), c, sn, r);
+      x.sync();
+      for (int rr = x.tid; rr <= i; rr += x.nt) {
+        double a = w.T(rr, i), b = w.T(rr, i + 1);
+        w.T(rr, i) = c * a - sn * b;
+        w.T(rr, i + 1) = sn * a + c * b;
+      }
+      if (x.tid == 0) { w.T(i + 1, i + 1) = r; w.T(i + 1, i) = 0.0; rc[i] = c; rs[i] = sn; }
+      x.sync();
+    }
+    for (int r = x.tid; r < n; r += x.nt) {
+      if (r < m)
+        for (int i = m - 2; i >= 0; --i) {
+          double a = w.H(r, i), b = w.H(r, i + 1);
+          w.H(r, i) = rc[i] * a - rs[i] * b;
+          w.H(r, i + 1) = rs[i] * a + rc[i] * b;
+        }
+      if (w.wantz)
+        for (int i = m - 2; i >= 0; --i) {
+          double a = w.Z(r, i), b = w.Z(r, i + 1);
+          w.Z(r, i) = rc[i] * a - rs[i] * b;
+          w.Z(r, i + 1) = rs[i] * a + rc[i] * b;
+        }
+    }
+    x.sync();
+  }
+  // ---- Hessenberg-triangular re-reduction of the leading m x m block
+  //      by Givens rotations (the job of DGGHRD at qzearly.f:449) ----
+  for (int jc = 0; jc < m - 2; ++jc) {
+    for (int jr = m - 1; jr >= jc + 2; --jr) {
+      double c, sn, r;
+      lartg(w.H(jr - 1, jc), w.H(jr, jc), c, sn, r);
+      x.sync();
+      par_rot_rows(x, w.H, jr - 1, jr, c, sn, jc + 1, n);
+      par_rot_rows(x, w.T, jr - 1, jr, c, sn, jr - 1, n);
+      if (w.wantq) par_rot_cols(x, w.Q, jr - 1, jr, c, sn, 0, n);
+      if (x.tid == 0) { w.H(jr - 1, jc) = r; w.H(jr, jc) = 0.0; }
+      x.sync();
+      // pair (col jr, col jr-1): zero T(jr, jr-1)
+      lartg(w.T(jr, jr), w.T(jr, jr - 1), c, sn, r);
+      x.sync();
+      par_rot_cols(x, w.H, jr, jr - 1, c, sn, 0, m);
+      par_rot_cols(x, w.T, jr, jr - 1, c, sn, 0, jr);
+      if (w.wantz) par_rot_cols(x, w.Z, jr, jr - 1, c, sn, 0, n);
+      if (x.tid == 0) { w.T(jr, jr) = r; w.T(jr, jr - 1) = 0.0; }
+      x.sync();
+    }
+  }
+}
+
+}  // namespace qz

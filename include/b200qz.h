@@ -1,0 +1,125 @@
+/*
+ * b200qz: B200-native multishift QZ (generalized real Schur form of a
+ * Hessenberg-triangular pencil) behind the PDHGEQZ calling convention.
+ *
+ * Plain C ABI: pointers, sizes and characters only.  Every entry point is
+ * exported from libb200qz.so (gevp-pdhgeqz_b200/libb200qz.so).
+ *
+ * Matrices are FP64 column-major.  Conventions follow the reference
+ * routine PDHGEQZ (src/pdhgeqz/PDHGEQZ.f:35-214): on exit
+ *   Q_in * H_in * Z_in^T = Q_out * S * Z_out^T,  the same for T and P,
+ * S quasi upper triangular with standardised 2x2 blocks, P upper
+ * triangular with non-negative diagonal (2x2 blocks: diagonal, positive),
+ * and lambda_j = (ALPHAR(j) + i*ALPHAI(j)) / BETA(j).
+ */
+#ifndef B200QZ_H
+#define B200QZ_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct b200qz_ctx b200qz_ctx;
+
+/* ------------------------------------------------------------------ */
+/* Drop-in for the reference's Fortran entry point.                     */
+/* ------------------------------------------------------------------ */
+
+/* Replaces SUBROUTINE PDHGEQZ( JOB, COMPQ, COMPZ, N, ILO, IHI, H, DESCH,
+ * T, DESCT, ALPHAR, ALPHAI, BETA, Q, DESCQ, Z, DESCZ, DWORK, LDWORK,
+ * IWORK, LIWORK, INFO ) of src/pdhgeqz/PDHGEQZ.f:15-31, with the gfortran
+ * by-reference convention and hidden CHARACTER lengths.  Only the 1x1
+ * process grid is supported: H, T, Q, Z are full N x N local arrays with
+ * leading dimension DESC(9).  DESC(5) = DESC(6) = NB >= 5 is required
+ * (PDHGEQZ.f:396-399).  Workspace query: LDWORK = -1 or LIWORK = -1
+ * returns the sizes in DWORK(1), IWORK(1) (PDHGEQZ.f:409-430).
+ * INFO: -1 JOB, -2 COMPQ, -3 COMPZ, -4 N, -5 ILO, -6 IHI, -7 NB < 5,
+ * -8 NB /= MB, -9 LDWORK, -10 LIWORK (PDHGEQZ.f:383-444), -(i*1000+9)
+ * for a bad leading dimension of argument i; > 0 the index of the first
+ * unconverged row (PDHGEQZ0.f:1207); 10001 a CUDA error. */
+void pdhgeqz_(const char* job, const char* compq, const char* compz, const int* n, const int* ilo,
+              const int* ihi, double* h, const int* desch, double* t, const int* desct, double* alphar,
+              double* alphai, double* beta, double* q, const int* descq, double* z, const int* descz,
+              double* dwork, const int* ldwork, int* iwork, const int* liwork, int* info,
+              size_t len_job, size_t len_compq, size_t len_compz);
+
+/* Replaces SUBROUTINE KKQZCONF( EPS ) (src/kkqz/kkqzconf.f:45-170), which
+ * every reference caller invokes first (testing/EXRAND1.f:96-98) to fill
+ * the COMMON parameter blocks.  Here the parameters live in a per-call
+ * context, so this is an accepted no-op. */
+void kkqzconf_(const double* eps);
+
+/* ------------------------------------------------------------------ */
+/* Native C entry points.                                                */
+/* ------------------------------------------------------------------ */
+
+/* Create / destroy a solver context on a CUDA device.  A context owns its
+ * stream and device workspace; distinct contexts may be used from
+ * different host threads concurrently. Returns 0 or a CUDA error code. */
+int b200qz_create(b200qz_ctx** ctx, int device);
+void b200qz_destroy(b200qz_ctx* ctx);
+
+/* Solve with all arrays already resident on the device (one leading
+ * dimension ld >= n for H, T, Q, Z).  job/compq/compz and ilo/ihi
+ * (1-based) as in PDHGEQZ.  alphar/alphai/beta are device arrays of
+ * length n.  Returns INFO (0 ok, > 0 unconverged row, < 0 bad argument,
+ * 10001 CUDA error). */
+int b200qz_solve_dev(b200qz_ctx* ctx, char job, char compq, char compz, int n, int ilo, int ihi,
+                     double* h, double* t, double* q, double* z, int ld,
+                     double* alphar, double* alphai, double* beta);
+
+/* Solve with host arrays (each with its own leading dimension); copies to
+ * the device, solves, copies back. */
+int b200qz_solve_host(b200qz_ctx* ctx, char job, char compq, char compz, int n, int ilo, int ihi,
+                      double* h, int ldh, double* t, int ldt, double* q, int ldq, double* z, int ldz,
+                      double* alphar, double* alphai, double* beta);
+
+/* Statistics of the last solve, written into out[0..nout):
+ * 0 seconds (device time), 1 iterations, 2 AEDs, 3 AED deflations,
+ * 4 sweeps, 5 chains, 6 windows, 7 endgames, 8 infinite-eigenvalue
+ * steps, 9 shifts used, 10 update flops (FP64-equivalent), 11 window
+ * kernel bytes.  Returns the number of values written. */
+int b200qz_get_stats(const b200qz_ctx* ctx, double* out, int nout);
+
+/* Tunables: nw_max (AED window), w_chase (chase window), nmin (blocks
+ * solved by one CTA), nibble (percent), ns_max (shift cap), maxit factor.
+ * A value < 0 keeps the current setting. Returns 0 or -i for argument i. */
+int b200qz_set_params(b200qz_ctx* ctx, int nw_max, int w_chase, int nmin, int nibble, int ns_max,
+                      int maxit_factor);
+
+/* ------------------------------------------------------------------ */
+/* Kernel-level entry points (device pointers), for parity tests.       */
+/* ------------------------------------------------------------------ */
+
+/* AED on the window H(kwtop:kbot, kwtop:kbot) (0-based, inclusive) of the
+ * active block starting at ktop; the role of PDHGEQZ2 + QZEARLY
+ * (PDHGEQZ2.f:315-389, qzearly.f:229-449) without the off-diagonal
+ * updates.  qw, zw: nw x nw outputs (ld nw); shifts: 3*nw outputs
+ * (alphar, alphai, beta of the undeflated part, each at stride nw);
+ * info3 (host): {undeflated m, status, transformed}.  When ktop == kwtop
+ * the whole window is reduced to Schur form (the PDHGEQZ4/KKQZ role). */
+int b200qz_aed_window(b200qz_ctx* ctx, double* h, double* t, int ld, int ktop, int kwtop, int kbot,
+                      double* qw, double* zw, double* shifts, int* info3);
+
+/* Chase one chain of bulges through the window H(w:w+wk, w:w+wk); the
+ * role of PDHGEQZB + DHGEQZ5 (PDHGEQZB.f:356-408, DHGEQZ5.f:128-250)
+ * and, for bulges with intro = 1, PDHGEQZA's introduction.  bulges is a
+ * host array of nb records {base, tlo, thi, intro} (int[4]) and coef a
+ * host array of nb x {c2, c1, c0}.  last = last active row inside the
+ * window (window coordinates).  u, v: wk x wk outputs (ld wk). */
+int b200qz_chase_window(b200qz_ctx* ctx, double* h, double* t, int ld, int w, int wk, int last,
+                        const int* bulges, const double* coef, int nb, int tmax, double* u, double* v);
+
+/* In-place update of a slab with a k x k factor (the role of PDHGEQZ6,
+ * PDHGEQZ6.f:276-380): side 'L': M(r0:r0+k, c0:c0+len) <- W^T M(...);
+ * side 'R': M(r0:r0+len, c0:c0+k) <- M(...) W. */
+int b200qz_update(b200qz_ctx* ctx, char side, double* m, int ldm, int r0, int c0, int len,
+                  const double* w, int ldw, int k);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* B200QZ_H */

@@ -1,0 +1,57 @@
+"""The C-ABI library loads on a machine without a GPU and exports every
+entry point include/b200qz.h declares (no compute calls here)."""
+import ctypes
+import os
+import re
+
+from conftest import ROOT
+
+
+def declared_symbols():
+    src = open(os.path.join(ROOT, "include", "b200qz.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b([a-z0-9_]+)\s*\(", src)) - {"if", "sizeof"})
+
+
+def test_header_declares_entry_points():
+    syms = declared_symbols()
+    for s in ("pdhgeqz_", "kkqzconf_", "b200qz_create", "b200qz_solve_dev", "b200qz_solve_host"):
+        assert s in syms
+
+
+def test_library_exports_all_declared(pkg):
+    lib = pkg.lib()
+    for s in declared_symbols():
+        assert hasattr(lib, s), s
+    assert set(pkg.EXPORTS) <= set(declared_symbols())
+
+
+def test_kkqzconf_noop(pkg):
+    pkg.kkqzconf(2.2e-16)
+
+
+def test_pdhgeqz_argument_errors_need_no_gpu(pkg):
+    import numpy as np
+    n = 8
+    H, T = pkg.pencils.random_ht(n, 0)
+    Q = np.eye(n, order="F")
+    Z = np.eye(n, order="F")
+    # argument checks run before any device work (PDHGEQZ.f:383-405)
+    assert pkg.pdhgeqz("X", "I", "I", H, T, Q, Z)[3] == -1
+    assert pkg.pdhgeqz("S", "X", "I", H, T, Q, Z)[3] == -2
+    assert pkg.pdhgeqz("S", "I", "X", H, T, Q, Z)[3] == -3
+    assert pkg.pdhgeqz("S", "I", "I", H, T, Q, Z, ilo=0)[3] == -5
+    assert pkg.pdhgeqz("S", "I", "I", H, T, Q, Z, ihi=n + 1)[3] == -6
+    assert pkg.pdhgeqz("S", "I", "I", H, T, Q, Z, nb=4)[3] == -7
+    d = [pkg.descriptor(n, 16, n) for _ in range(4)]
+    d[0][4] = 8  # MB != NB
+    assert pkg.pdhgeqz("S", "I", "I", H, T, Q, Z, descs=d)[3] == -8
+    # workspace query (PDHGEQZ.f:409-430)
+    dw, iw, _, info = pkg.pdhgeqz("S", "I", "I", H, T, Q, Z, nb=16, ldwork=-1)
+    assert info == 0 and dw == n * 16 and iw == 2 * n
+    assert pkg.pdhgeqz("S", "I", "I", H, T, Q, Z, nb=16, ldwork=5)[3] == -9
+    assert pkg.pdhgeqz("S", "I", "I", H, T, Q, Z, nb=16, liwork=3)[3] == -10
+    # quick return: nothing touched
+    H0 = H.copy()
+    assert pkg.pdhgeqz("S", "I", "I", H, T, Q, Z, ilo=5, ihi=4)[3] == 0
+    assert np.array_equal(H, H0)
