@@ -1,0 +1,371 @@
+"""Benchmark: time-to-Schur of the multishift QZ path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--n 10000] [--workload c3]
+
+One step = one complete reduction of a Hessenberg-triangular pencil to
+generalized real Schur form with Q and Z (JOB='S', COMPQ=COMPZ='I').
+Default workload: the graded n=10000 pencil from seed 2 (H = D1 X_H D2,
+T = D1 X_T D2, diag(D1), diag(D2) = 10^U(-3,3)); inputs are 4 x 800 MB,
+larger than L2, so no flush is needed between steps.
+
+value      mean device seconds per solve (CUDA events on the solver stream),
+           inputs restored from a device-resident copy before each step
+           outside the timed events
+e2e        the same solve through the public C-ABI entry b200qz_solve_host
+           with pinned host buffers: H, T copied in, S, P, Q, Z and the
+           eigenvalues copied out inside the timed region
+roofline   the kernel with the largest device-time share in a profiled solve
+cpu_baseline / --impl reference
+           the oracle's C restatement of the reference path (oracle/qzref.c,
+           OpenBLAS with all host threads) on a bounded sample: a smaller
+           pencil of the same distribution; seconds scaled by (n/n_s)^3
+
+Multi-GPU (torchrun): a single pencil does not shard; every rank solves its
+own replica, value = max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib.util
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+
+def load_pkg():
+    name = "gevp_pdhgeqz_b200"
+    if name in sys.modules:
+        return sys.modules[name]
+    spec = importlib.util.spec_from_file_location(name, os.path.join(ROOT, "gevp-pdhgeqz_b200", "__init__.py"))
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+METRIC = "time-to-Schur (s) at n=10k, backward err<=50*n*eps; split+learned vs plain FP64 GPU"
+EPS = np.finfo(np.float64).eps
+
+
+def make_pencil(pkg, workload, n):
+    P = pkg.pencils
+    if workload == "c3":
+        return P.graded_ht(n, 2), "graded (D1 X D2, 10^U(-3,3)) seed 2"
+    if workload == "c2":
+        return P.random_ht(n, 1, 0.05), "N(0,1) seed 1, 5% zero T diagonal"
+    if workload == "c1":
+        return P.random_ht(n, 0), "N(0,1) seed 0"
+    if workload == "c4":
+        return P.random_ht(n, 3), "N(0,1) seed 3"
+    raise ValueError(workload)
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev), "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def read_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d, "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def read_ncu_traffic(kernel):
+    """Per-launch DRAM bytes of a kernel from the committed ncu summary
+    (profiles/ncu_<kernel>.md, line 'traffic_bytes_per_launch: X')."""
+    p = os.path.join(ROOT, "profiles", "ncu_%s.md" % kernel)
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.startswith("traffic_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1].strip().split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+def cpu_reference_seconds(n_target, n_sample, workload, pkg, steps=1, warmup=0):
+    """The oracle port on a bounded sample; returns (scaled seconds list, sample seconds)."""
+    from oracle import lapack as L
+    from oracle import qzref as R
+    threads = os.cpu_count() or 1
+    L.set_threads(threads)
+    (H, T), desc = make_pencil(pkg, workload, n_sample)
+    R.lib()
+    for _ in range(warmup):
+        R.pdhgeqz(H, T, nb=60 if n_sample <= 2000 else 130)
+    samples = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        out = R.pdhgeqz(H, T, nb=60 if n_sample <= 2000 else 130)
+        samples.append(time.perf_counter() - t0)
+        if out[7] != 0:
+            raise RuntimeError("oracle port did not converge (info=%d)" % out[7])
+    scale = (n_target / n_sample) ** 3
+    return [s * scale for s in samples], samples, threads, desc
+
+
+def run_reference(args, pkg, rank):
+    if rank != 0:
+        return
+    n_s = args.cpu_sample_n
+    scaled, raw, threads, desc = cpu_reference_seconds(args.n, n_s, args.workload, pkg, steps=args.steps,
+                                                       warmup=args.warmup)
+    v = float(np.mean(scaled))
+    sample = ("oracle/qzref.c (C restatement of PDHGEQZ on a 1x1 grid, OpenBLAS %d threads), "
+              "full solve of a %s pencil at n=%d, %.2f s measured, scaled by (n/%d)^3" % (threads, desc, n_s,
+                                                                                          np.mean(raw), n_s))
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": v * 1e3, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "%s n=%d" % (args.workload, args.n), "n": args.n, "job": "S", "compq": "I",
+                       "compz": "I", "cpu_sample_n": n_s},
+            "cpu_baseline": {"value": v, "unit": "s", "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=10000)
+    ap.add_argument("--workload", default="c3")
+    ap.add_argument("--cpu-sample-n", type=int, default=2000)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--param", action="append", default=[], help="solver tunable name=value")
+    args = ap.parse_args()
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pkg = load_pkg()
+
+    if args.impl == "reference":
+        run_reference(args, pkg, rank)
+        return
+
+    import torch
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.cuda.current_device()
+    n = args.n
+    (H, T), desc = make_pencil(pkg, args.workload, n)
+    ld = n
+    # device-resident pristine copies (column-major storage = transposed torch tensors)
+    dH0 = torch.from_numpy(np.ascontiguousarray(H.T)).to(dev)
+    dT0 = torch.from_numpy(np.ascontiguousarray(T.T)).to(dev)
+    dH = torch.empty_like(dH0)
+    dT = torch.empty_like(dT0)
+    dQ = torch.empty_like(dH0)
+    dZ = torch.empty_like(dH0)
+    de = torch.empty(3 * n, dtype=torch.float64, device=dev)
+    solver = pkg.Solver(dev)
+    for kv in args.param:
+        k, v = kv.split("=")
+        solver.set_param(k, float(v))
+
+    def one_solve():
+        dH.copy_(dH0)
+        dT.copy_(dT0)
+        torch.cuda.synchronize()
+        info = solver.solve_device(dH.data_ptr(), dT.data_ptr(), dQ.data_ptr(), dZ.data_ptr(), ld, n,
+                                   de.data_ptr(), de.data_ptr() + 8 * n, de.data_ptr() + 16 * n)
+        if info != 0:
+            raise RuntimeError("solver returned INFO=%d" % info)
+        st = solver.stats()
+        return st["seconds"], st
+
+    for _ in range(args.warmup):
+        one_solve()
+    clocks = ClockSampler(dev)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    times, launches = [], 0
+    last_stats = None
+    for _ in range(args.steps):
+        t, st = one_solve()
+        times.append(t)
+        launches += int(st.get("launches", 0))
+        last_stats = st
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    if dist is not None:
+        dist.barrier()
+    t_mean = float(np.mean(times))
+    if dist is not None:
+        tt = torch.tensor([t_mean], dtype=torch.float64, device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_mean = float(tt.item())
+
+    # ---- backward errors of the last timed solve (FP64 on the GPU) ----
+    Ht = dH0.t()
+    Tt = dT0.t()
+    S = dH.t()
+    P = dT.t()
+    Q = dQ.t()
+    Z = dZ.t()
+    nrm_h = torch.linalg.norm(Ht).item()
+    nrm_t = torch.linalg.norm(Tt).item()
+    res_h = (torch.linalg.norm(Q.T @ Ht @ Z - S).item() / nrm_h) / (n * EPS)
+    res_t = (torch.linalg.norm(Q.T @ Tt @ Z - P).item() / nrm_t) / (n * EPS)
+    I = torch.eye(n, dtype=torch.float64, device=dev)
+    orth_q = torch.linalg.norm(Q.T @ Q - I).item() / (n * EPS)
+    orth_z = torch.linalg.norm(Z.T @ Z - I).item() / (n * EPS)
+    del I
+
+    # ---- profiled solve (untimed) for the phase breakdown / roofline ----
+    os.environ["B200QZ_PROFILE"] = "1"
+    _, pst = one_solve()
+    os.environ.pop("B200QZ_PROFILE", None)
+    peaks, peak_kind = read_peaks()
+    phases = {k[3:]: v for k, v in pst.items() if k.startswith("ms_") and not k.startswith("ms_aed_")}
+    dom = max(phases, key=phases.get)
+    kernel_of = {"aed": "k_aed_win", "chase": "k_chase_win", "aed_update": "k_update_left/right",
+                 "chase_update": "k_update_left/right", "scan": "k_scan", "inf": "k_inf_win", "final": "k_eigs"}
+    nw = 80
+    if dom in ("aed_update", "chase_update"):
+        upd_ms = phases["aed_update"] + phases["chase_update"]
+        ach = pst["update_flops"] / (upd_ms * 1e-3) / 1e12
+        fp64_peak = 37.0
+        roof = {"kernel": "k_update_left/right (DMMA FP64)", "bound": "tensor", "achieved": ach,
+                "peak": fp64_peak, "unit": "TFLOP/s", "frac": ach / fp64_peak, "traffic": None,
+                "peak_source": "datasheet FP64 tensor (no FP64 peak in MEASURED_PEAKS.json)"}
+    else:
+        launches_dom = {"aed": pst["aeds"] + pst["endgames"], "chase": pst["windows"]}.get(dom, 1)
+        bytes_per = 6.0 * 8.0 * nw * nw  # window in + out, both factors out
+        dur = phases[dom] * 1e-3 / max(1.0, launches_dom)
+        ach = bytes_per / dur / 1e9
+        kname = kernel_of.get(dom, dom)
+        roof = {"kernel": kname, "bound": "hbm", "achieved": ach, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                "frac": ach / peaks["hbm_gbs"], "traffic": read_ncu_traffic(kname),
+                "avg_launch_ms": dur * 1e3, "bytes_per_launch": bytes_per,
+                "peak_source": "%s HBM copy bandwidth" % ("measured" if peak_kind == "measured" else "fallback")}
+    share = {k: round(v / max(1e-9, sum(phases.values())), 4) for k, v in phases.items()}
+
+    # ---- end to end through the C-ABI with pinned host buffers ----
+    e2e_times = []
+    pin = lambda a: torch.empty(a.shape[::-1], dtype=torch.float64, pin_memory=True).numpy().T
+    Hp, Tp, Qp, Zp = pin(H), pin(T), pin(H), pin(H)
+    for _ in range(max(1, args.steps)):
+        np.copyto(Hp, H)
+        np.copyto(Tp, T)
+        t0 = time.perf_counter()
+        ar, ai, be, info = solver.solve_host(Hp, Tp, Qp, Zp)
+        e2e_times.append(time.perf_counter() - t0)
+        if info != 0:
+            raise RuntimeError("e2e solve INFO=%d" % info)
+    e2e = float(np.mean(e2e_times))
+    if dist is not None:
+        tt = torch.tensor([e2e], dtype=torch.float64, device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e = float(tt.item())
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        scaled, raw, threads, cdesc = cpu_reference_seconds(n, args.cpu_sample_n, args.workload, pkg)
+        cpu = {"value": float(scaled[0]), "unit": "s", "cores": threads, "kind": "port",
+               "sample": "oracle/qzref.c on a %s pencil at n=%d: %.2f s measured, scaled by (%d/%d)^3"
+                         % (cdesc, args.cpu_sample_n, raw[0], n, args.cpu_sample_n)}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": t_mean, "unit": "s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_mean * 1e3, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "%s: %s n=%d" % (args.workload, desc, n), "n": n, "job": "S", "compq": "I",
+                       "compz": "I", "parallelism": "replicas" if world > 1 else "single-gpu",
+                       "l2": "inputs 4 x %.0f MB > L2; restored from device copy outside timed events"
+                             % (8 * n * n / 1e6),
+                       "params": args.param,
+                       "backward_error_neps": {"h": res_h, "t": res_t},
+                       "orthogonality_neps": {"q": orth_q, "z": orth_z},
+                       "stats": {k: v for k, v in last_stats.items() if not k.startswith("ms_")}},
+            "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": 2 * 8 * n * n,
+                    "d2h_bytes_per_step": 4 * 8 * n * n + 3 * 8 * n},
+            "gpu_launches": launches,
+            "clocks": clk,
+            "roofline": roof,
+            "phase_share": share,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    solver.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -55,11 +55,13 @@ _c = ctypes.c_char
 EXPORTS = (
     "pdhgeqz_", "kkqzconf_", "b200qz_create", "b200qz_destroy", "b200qz_solve_dev",
     "b200qz_solve_host", "b200qz_get_stats", "b200qz_set_params", "b200qz_aed_window",
-    "b200qz_chase_window", "b200qz_update",
+    "b200qz_chase_window", "b200qz_update", "b200qz_set_param",
 )
 
 STAT_NAMES = ("seconds", "iters", "aeds", "aed_deflations", "sweeps", "chains", "windows",
-              "endgames", "inf_steps", "shifts", "update_flops", "window_bytes")
+              "endgames", "inf_steps", "shifts", "update_flops", "window_bytes",
+              "ms_scan", "ms_aed", "ms_aed_update", "ms_chase", "ms_chase_update", "ms_inf", "ms_final",
+              "ms_aed_smallqz", "ms_aed_reorder", "ms_aed_spike", "ms_aed_hessred", "launches")
 
 
 def lib() -> ctypes.CDLL:
@@ -95,6 +97,8 @@ def lib() -> ctypes.CDLL:
     L.b200qz_aed_window.argtypes = [_vp, _vp, _vp, _i, _i, _i, _i, _vp, _vp, _vp, _pi]
     L.b200qz_chase_window.restype = _i
     L.b200qz_chase_window.argtypes = [_vp, _vp, _vp, _i, _i, _i, _i, _pi, _pd, _i, _i, _vp, _vp]
+    L.b200qz_set_param.restype = _i
+    L.b200qz_set_param.argtypes = [_vp, ctypes.c_char_p, _d]
     L.b200qz_update.restype = _i
     L.b200qz_update.argtypes = [_vp, _c, _vp, _i, _i, _i, _i, _vp, _i, _i]
     _lib = L
@@ -190,6 +194,11 @@ class Solver:
         rc = lib().b200qz_set_params(self._h, nw_max, w_chase, nmin, nibble, ns_max, maxit_factor)
         if rc != 0:
             raise ValueError("b200qz_set_params: bad argument %d" % -rc)
+
+    def set_param(self, name: str, value) -> None:
+        rc = lib().b200qz_set_param(self._h, name.encode(), float(value))
+        if rc != 0:
+            raise ValueError("b200qz_set_param(%s=%r) failed: %d" % (name, value, rc))
 
     def stats(self) -> dict:
         out = np.zeros(len(STAT_NAMES))

@@ -10,6 +10,8 @@
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
+#include <string>
+#include <vector>
 
 #include "../../include/b200qz.h"
 #include "kernels.h"
@@ -20,6 +22,51 @@ using namespace qz;
 namespace {
 constexpr int kAedMax = 512;  // largest AED / small-solve window supported
 }
+
+// Phase timer: CUDA event pairs recorded around each group of launches on
+// the solver stream, resolved once at the end of a solve (B200QZ_PROFILE=1).
+enum Phase { kPhScan, kPhAed, kPhAedUpd, kPhChase, kPhChaseUpd, kPhInf, kPhFinal, kPhN };
+
+struct PhaseTimer {
+  bool on = false;
+  std::vector<cudaEvent_t> pool;
+  size_t used = 0;
+  std::vector<std::pair<int, size_t>> marks;  // (phase, index of start event)
+  double ms[kPhN] = {0};
+  cudaEvent_t next() {
+    if (used == pool.size()) {
+      cudaEvent_t e;
+      cudaEventCreate(&e);
+      pool.push_back(e);
+    }
+    return pool[used++];
+  }
+  void begin(int ph, cudaStream_t st) {
+    if (!on) return;
+    marks.push_back({ph, used});
+    cudaEventRecord(next(), st);
+  }
+  void end(cudaStream_t st) {
+    if (!on) return;
+    cudaEventRecord(next(), st);
+  }
+  void reset() {
+    used = 0;
+    marks.clear();
+    for (double& v : ms) v = 0.0;
+  }
+  void resolve() {
+    if (!on) return;
+    for (auto& m : marks) {
+      float t = 0.f;
+      if (m.second + 1 < used && cudaEventElapsedTime(&t, pool[m.second], pool[m.second + 1]) == cudaSuccess)
+        ms[m.first] += t;
+    }
+  }
+  ~PhaseTimer() {
+    for (cudaEvent_t e : pool) cudaEventDestroy(e);
+  }
+};
 
 struct b200qz_ctx {
   int device = 0;
@@ -42,6 +89,12 @@ struct b200qz_ctx {
   int ka = 0;  // size of the AED factors in Ua/Va
   int kc = 0;  // size of the chase factors in Uc/Vc
   cudaError_t err = cudaSuccess;
+  PhaseTimer timer;
+  unsigned long long* dts = nullptr;  // AED phase timestamps (device)
+  double* dbuf = nullptr;             // cached device copy of H, T, Q, Z, eigenvalues (host entry)
+  size_t dbuf_bytes = 0;
+  unsigned long long* hts = nullptr;  // pinned mirror
+  double aed_ms[4] = {0, 0, 0, 0};   // small QZ, reorder, spike+RQ, HT re-reduction
 };
 
 namespace {
@@ -64,7 +117,10 @@ struct GpuBackend {
   Tol tol;
 
   void scan(int ifirst, int kbot, int* out) {
+    c->timer.begin(kPhScan, c->stream);
     launch_scan(c->stream, H, T, ld, ifirst, kbot, tol, c->dinfo);
+    c->stats.launches += 1;
+    c->timer.end(c->stream);
     QZ_CK(cudaMemcpyAsync(c->hinfo, c->dinfo, 4 * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     QZ_CK(cudaStreamSynchronize(c->stream));
     if (c->err != cudaSuccess) { out[0] = ifirst; out[1] = 0; out[2] = -1; out[3] = -1; return; }
@@ -72,11 +128,29 @@ struct GpuBackend {
   }
   void aed(int ktop, int kwtop, int kbot, int* info3, double* sh) {
     int nw = kbot - kwtop + 1;
-    launch_aed(c->stream, H, T, ld, ktop, kwtop, nw, tol, c->Ua, c->Va, c->shifts, c->dinfo + 4, c->gscratch);
+    c->timer.begin(kPhAed, c->stream);
+    launch_aed(c->stream, H, T, ld, ktop, kwtop, nw, tol, c->Ua, c->Va, c->shifts, c->dinfo + 4, c->gscratch,
+               c->timer.on ? c->dts : nullptr, (kwtop > ktop) ? c->params.aed_nskip : 0);
+    c->stats.launches += 1;
+    c->timer.end(c->stream);
     QZ_CK(cudaMemcpyAsync(c->hinfo + 4, c->dinfo + 4, 3 * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     QZ_CK(cudaMemcpyAsync(c->hshifts, c->shifts, 3 * nw * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    if (c->timer.on)
+      QZ_CK(cudaMemcpyAsync(c->hts, c->dts, 8 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream));
     QZ_CK(cudaStreamSynchronize(c->stream));
     c->ka = nw;
+    if (c->timer.on) {
+      // stamps 0..4: start, after small QZ, after reordering, after spike+RQ, end
+      unsigned long long* t = c->hts;
+      if (t[1] >= t[0]) c->aed_ms[0] += (t[1] - t[0]) * 1e-6;
+      if (c->hinfo[5] == 0 && t[2] >= t[1]) c->aed_ms[1] += (t[2] - t[1]) * 1e-6;
+      if (c->hinfo[5] == 0 && t[3] >= t[2] && t[4] >= t[3]) {
+        c->aed_ms[2] += (t[3] - t[2]) * 1e-6;
+        c->aed_ms[3] += (t[4] - t[3]) * 1e-6;
+      }
+      for (int i = 0; i < 8; ++i) t[i] = 0;
+      QZ_CK(cudaMemsetAsync(c->dts, 0, 8 * sizeof(unsigned long long), c->stream));
+    }
     if (c->err != cudaSuccess) { info3[0] = nw; info3[1] = 1; info3[2] = 0; return; }
     info3[0] = c->hinfo[4];
     info3[1] = c->hinfo[5];
@@ -90,16 +164,27 @@ struct GpuBackend {
     c->stats.win_bytes += 2.0 * 2.0 * 8.0 * nw * nw + 2.0 * 8.0 * nw * nw;
   }
   void chase(int w, int wk, int last, const Bulge* bl, int nb, int tmax) {
+    c->timer.begin(kPhChase, c->stream);
     launch_chase(c->stream, H, T, ld, w, wk, last, bl, nb, tmax, c->Uc, c->Vc);
+    c->stats.launches += 1;
+    c->timer.end(c->stream);
     c->kc = wk;
     c->stats.win_bytes += 2.0 * 2.0 * 8.0 * wk * wk + 2.0 * 8.0 * wk * wk;
   }
   void inf_window(int w, int wk, int top, int jz, int stop, bool deflate) {
+    c->timer.begin(kPhInf, c->stream);
     launch_inf(c->stream, H, T, ld, w, wk, top, jz, stop, deflate ? 1 : 0, c->Uc, c->Vc);
+    c->stats.launches += 1;
+    c->timer.end(c->stream);
     c->kc = wk;
     c->stats.win_bytes += 2.0 * 2.0 * 8.0 * wk * wk + 2.0 * 8.0 * wk * wk;
   }
-  void inf_top(int f) { launch_inf_top(c->stream, H, T, Q, ld, n, f, wantq ? 1 : 0); }
+  void inf_top(int f) {
+    c->timer.begin(kPhInf, c->stream);
+    launch_inf_top(c->stream, H, T, Q, ld, n, f, wantq ? 1 : 0);
+    c->stats.launches += 1;
+    c->timer.end(c->stream);
+  }
   // off-diagonal updates with the factors of the last window kernel
   void update(int w, int wk, int which) {
     const double* U = which == 0 ? c->Ua : c->Uc;
@@ -140,8 +225,10 @@ struct GpuBackend {
       j.tiles = (n + tile - 1) / tile;
       c->stats.upd_flops += 2.0 * wk * wk * n;
     }
-    if (L.njobs) launch_update(c->stream, L, 0);
-    if (R.njobs) launch_update(c->stream, R, 1);
+    c->timer.begin(which == 0 ? kPhAedUpd : kPhChaseUpd, c->stream);
+    if (L.njobs) { launch_update(c->stream, L, 0); c->stats.launches += 1; }
+    if (R.njobs) { launch_update(c->stream, R, 1); c->stats.launches += 1; }
+    c->timer.end(c->stream);
   }
 };
 
@@ -165,17 +252,22 @@ int solve_dev_impl(b200qz_ctx* c, char job, char compq, char compz, int n, int i
   {
     const char* v = std::getenv("B200QZ_VERBOSE");
     c->params.verbose = (v && *v && *v != '0') ? 1 : 0;
+    const char* p = std::getenv("B200QZ_PROFILE");
+    c->timer.on = (p && *p && *p != '0');
+    c->timer.reset();
+    for (double& a : c->aed_ms) a = 0.0;
   }
   QZ_CK(cudaSetDevice(c->device));
   bool wantq = !is(compq, 'N'), wantz = !is(compz, 'N');
-  if (is(compq, 'I')) launch_identity(c->stream, q, ld, n);
-  if (is(compz, 'I')) launch_identity(c->stream, z, ld, n);
+  if (is(compq, 'I')) { launch_identity(c->stream, q, ld, n); c->stats.launches += 1; }
+  if (is(compz, 'I')) { launch_identity(c->stream, z, ld, n); c->stats.launches += 1; }
   QZ_CK(cudaEventRecord(c->ev0, c->stream));
   int nh = ihi - ilo + 1;
   // /PREC/ constants (PDHGEQZ.f:449-458): ulp, smlnum, Frobenius norms
   QZ_CK(cudaMemsetAsync(c->norms, 0, 2 * sizeof(double), c->stream));
   launch_sumsq(c->stream, h, ld, ilo - 1, nh, c->norms);
   launch_sumsq(c->stream, t, ld, ilo - 1, nh, c->norms + 1);
+  c->stats.launches += 2;
   QZ_CK(cudaMemcpyAsync(c->hnorms, c->norms, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   QZ_CK(cudaStreamSynchronize(c->stream));
   if (c->err != cudaSuccess) return 10001;
@@ -194,10 +286,14 @@ int solve_dev_impl(b200qz_ctx* c, char job, char compq, char compz, int n, int i
   tol.ttol = std::max(DBL_MIN, DBL_EPSILON * std::sqrt(c->hnorms[1]));
   int info = 0;
   if (nh > 0) info = qz_iterate(bk, n, ilo - 1, ihi - 1, c->params, c->stats);
+  c->timer.begin(kPhFinal, c->stream);
   launch_finalize(c->stream, h, t, z, ld, n, wantz ? 1 : 0, ar, ai, be);
+  c->stats.launches += 2;
+  c->timer.end(c->stream);
   QZ_CK(cudaGetLastError());
   QZ_CK(cudaEventRecord(c->ev1, c->stream));
   QZ_CK(cudaEventSynchronize(c->ev1));
+  c->timer.resolve();
   float ms = 0.f;
   QZ_CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
   c->seconds = ms * 1e-3;
@@ -231,6 +327,9 @@ int b200qz_create(b200qz_ctx** out, int device) {
   if (e == cudaSuccess) e = cudaMallocHost(&c->hinfo, 8 * sizeof(int));
   if (e == cudaSuccess) e = cudaMallocHost(&c->hshifts, 3 * kAedMax * sizeof(double));
   if (e == cudaSuccess) e = cudaMallocHost(&c->hnorms, 2 * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc(&c->dts, 8 * sizeof(unsigned long long));
+  if (e == cudaSuccess) e = cudaMemset(c->dts, 0, 8 * sizeof(unsigned long long));
+  if (e == cudaSuccess) e = cudaMallocHost(&c->hts, 8 * sizeof(unsigned long long));
   if (e == cudaSuccess) e = cudaEventCreate(&c->ev0);
   if (e == cudaSuccess) e = cudaEventCreate(&c->ev1);
   if (e != cudaSuccess) {
@@ -250,6 +349,9 @@ void b200qz_destroy(b200qz_ctx* c) {
   if (c->hinfo) cudaFreeHost(c->hinfo);
   if (c->hshifts) cudaFreeHost(c->hshifts);
   if (c->hnorms) cudaFreeHost(c->hnorms);
+  cudaFree(c->dts);
+  if (c->hts) cudaFreeHost(c->hts);
+  if (c->dbuf) cudaFree(c->dbuf);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -269,6 +371,24 @@ int b200qz_set_params(b200qz_ctx* c, int nw_max, int w_chase, int nmin, int nibb
   if (ns_max >= 0) c->params.ns_max = ns_max;
   if (maxit_factor >= 0) c->params.maxit_factor = std::max(1, maxit_factor);
   c->params.chain_max = std::min(kMaxChain, std::max(1, (c->params.w_chase - 4) / 6));
+  return 0;
+}
+
+int b200qz_set_param(b200qz_ctx* c, const char* name, double value) {
+  if (!c || !name) return -1;
+  std::string k(name);
+  int v = (int)value;
+  SolveParams& P = c->params;
+  if (k == "nw_max") { if (v < 4 || v > kWinSmemMax) return -3; P.nw_max = v; }
+  else if (k == "w_chase") { if (v < 12 || v > kWinSmemMax) return -3; P.w_chase = v;
+    P.chain_max = std::min(kMaxChain, std::max(1, (v - 4) / 6)); }
+  else if (k == "nmin") { if (v < 4 || v > kAedMax) return -3; P.nmin = v; }
+  else if (k == "nibble") { if (v < 0 || v > 100) return -3; P.nibble = v; }
+  else if (k == "ns_max") { if (v < 0) return -3; P.ns_max = v; }
+  else if (k == "maxit_factor") { if (v < 1) return -3; P.maxit_factor = v; }
+  else if (k == "chain_max") { if (v < 1 || v > kMaxChain) return -3; P.chain_max = v; }
+  else if (k == "aed_nskip") { if (v < 0) return -3; P.aed_nskip = v; }
+  else return -2;
   return 0;
 }
 
@@ -298,12 +418,19 @@ int b200qz_solve_host(b200qz_ctx* c, char job, char compq, char compz, int n, in
   QZ_CK(cudaSetDevice(c->device));
   int ldd = (n + 31) & ~31;
   size_t bytes = (size_t)ldd * n * sizeof(double);
-  double *dh = nullptr, *dt = nullptr, *dq = nullptr, *dz = nullptr, *de = nullptr;
-  QZ_CK(cudaMalloc(&dh, bytes));
-  QZ_CK(cudaMalloc(&dt, bytes));
-  QZ_CK(cudaMalloc(&dq, bytes));
-  QZ_CK(cudaMalloc(&dz, bytes));
-  QZ_CK(cudaMalloc(&de, 3 * (size_t)n * sizeof(double)));
+  size_t need = 4 * bytes + 3 * (size_t)n * sizeof(double);
+  if (c->dbuf_bytes < need) {
+    if (c->dbuf) cudaFree(c->dbuf);
+    c->dbuf = nullptr;
+    c->dbuf_bytes = 0;
+    QZ_CK(cudaMalloc(&c->dbuf, need));
+    if (c->err == cudaSuccess) c->dbuf_bytes = need;
+  }
+  double* dh = c->dbuf;
+  double* dt = dh + bytes / sizeof(double);
+  double* dq = dt + bytes / sizeof(double);
+  double* dz = dq + bytes / sizeof(double);
+  double* de = dz + bytes / sizeof(double);
   int info = 10001;
   if (c->err == cudaSuccess) {
     size_t w = (size_t)n * sizeof(double);
@@ -327,7 +454,6 @@ int b200qz_solve_host(b200qz_ctx* c, char job, char compq, char compz, int n, in
       QZ_CK(cudaStreamSynchronize(c->stream));
     }
   }
-  cudaFree(dh); cudaFree(dt); cudaFree(dq); cudaFree(dz); cudaFree(de);
   if (c->err != cudaSuccess) return 10001;
   return info;
 }
@@ -335,10 +461,13 @@ int b200qz_solve_host(b200qz_ctx* c, char job, char compq, char compz, int n, in
 int b200qz_get_stats(const b200qz_ctx* c, double* out, int nout) {
   if (!c || !out) return 0;
   const SolveStats& s = c->stats;
-  double v[12] = {c->seconds, (double)s.iters, (double)s.aeds, (double)s.aed_defl, (double)s.sweeps,
+  const double* ph = c->timer.ms;
+  double v[24] = {c->seconds, (double)s.iters, (double)s.aeds, (double)s.aed_defl, (double)s.sweeps,
                   (double)s.chains, (double)s.windows, (double)s.endgames, (double)s.infs, (double)s.shifts,
-                  s.upd_flops, s.win_bytes};
-  int k = std::min(nout, 12);
+                  s.upd_flops, s.win_bytes,
+                  ph[kPhScan], ph[kPhAed], ph[kPhAedUpd], ph[kPhChase], ph[kPhChaseUpd], ph[kPhInf], ph[kPhFinal],
+                  c->aed_ms[0], c->aed_ms[1], c->aed_ms[2], c->aed_ms[3], (double)s.launches};
+  int k = std::min(nout, 24);
   for (int i = 0; i < k; ++i) out[i] = v[i];
   return k;
 }

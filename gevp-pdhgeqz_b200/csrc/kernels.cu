@@ -25,7 +25,15 @@ struct DevExec {
   int tid, nt;
   int* si;
   double* sd;
+  unsigned long long* ts = nullptr;  // phase timestamps (ns), thread 0 writes
   __device__ void sync() { __syncthreads(); }
+  __device__ void stamp(int k) {
+    if (ts && tid == 0) {
+      unsigned long long t;
+      asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+      ts[k] = t;
+    }
+  }
 };
 
 // shared-memory scratch carved at the end of the dynamic smem block
@@ -38,20 +46,24 @@ __device__ __forceinline__ double& G(double* p, int64_t ld, int i, int j) { retu
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(kWinThreads) k_aed_win(double* H, double* T, int64_t ld, int ktop, int kwtop,
                                                          int nw, Tol tol, double* Qw, double* Zw, double* shifts,
-                                                         int* info, double* gscratch, int maxit) {
+                                                         int* info, double* gscratch, int maxit,
+                                                         unsigned long long* ts, int nskip) {
   extern __shared__ double smem[];
   const int n = nw;
+  const bool in_smem = n <= kWinSmemMax;
+  // odd leading dimension in shared memory: row accesses hit distinct banks
+  const int lw = in_smem ? smem_ld(n) : n;
   double* Hs;
   double* Ts;
   double* Qs;
   double* Zs;
   double* sd;
-  if (n <= kWinSmemMax) {
+  if (in_smem) {
     Hs = smem;
-    Ts = Hs + n * n;
-    Qs = Ts + n * n;
-    Zs = Qs + n * n;
-    sd = Zs + n * n;
+    Ts = Hs + n * lw;
+    Qs = Ts + n * lw;
+    Zs = Qs + n * lw;
+    sd = Zs + n * lw;
   } else {
     Hs = gscratch;
     Ts = gscratch + (int64_t)n * n;
@@ -60,36 +72,36 @@ __global__ void __launch_bounds__(kWinThreads) k_aed_win(double* H, double* T, i
     sd = smem;
   }
   int* si = (int*)(sd + 64 + 4 * n);
-  DevExec x{(int)threadIdx.x, (int)blockDim.x, si, sd};
+  DevExec x{(int)threadIdx.x, (int)blockDim.x, si, sd, ts};
   for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
     int i = idx % n, j = idx / n;
-    Hs[idx] = G(H, ld, kwtop + i, kwtop + j);
-    Ts[idx] = G(T, ld, kwtop + i, kwtop + j);
-    Qs[idx] = (i == j) ? 1.0 : 0.0;
-    Zs[idx] = (i == j) ? 1.0 : 0.0;
+    Hs[i + j * lw] = G(H, ld, kwtop + i, kwtop + j);
+    Ts[i + j * lw] = G(T, ld, kwtop + i, kwtop + j);
+    Qs[i + j * lw] = (i == j) ? 1.0 : 0.0;
+    Zs[i + j * lw] = (i == j) ? 1.0 : 0.0;
   }
   double s = (kwtop > ktop) ? G(H, ld, kwtop, kwtop - 1) : 0.0;
   __syncthreads();
   WinState w;
   w.n = n;
-  w.H = MatV{Hs, n};
-  w.T = MatV{Ts, n};
-  w.Q = MatV{Qs, n};
-  w.Z = MatV{Zs, n};
+  w.H = MatV{Hs, lw};
+  w.T = MatV{Ts, lw};
+  w.Q = MatV{Qs, lw};
+  w.Z = MatV{Zs, lw};
   w.wantq = true;
   w.wantz = true;
   w.tol = tol;
-  cta_aed(x, w, s, shifts, shifts + n, shifts + 2 * n, maxit);
+  cta_aed(x, w, s, shifts, shifts + n, shifts + 2 * n, maxit, nskip);
   __syncthreads();
   const int m = si[8], st = si[9], tr = si[10];
   if (st == 0 && tr) {
     for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
       int i = idx % n, j = idx / n;
-      G(H, ld, kwtop + i, kwtop + j) = Hs[idx];
-      G(T, ld, kwtop + i, kwtop + j) = Ts[idx];
-      if (n <= kWinSmemMax) {
-        Qw[idx] = Qs[idx];
-        Zw[idx] = Zs[idx];
+      G(H, ld, kwtop + i, kwtop + j) = Hs[i + j * lw];
+      G(T, ld, kwtop + i, kwtop + j) = Ts[i + j * lw];
+      if (in_smem) {
+        Qw[idx] = Qs[i + j * lw];
+        Zw[idx] = Zs[i + j * lw];
       }
     }
     if (threadIdx.x == 0 && kwtop > ktop) G(H, ld, kwtop, kwtop - 1) = s * Qs[0];
@@ -104,34 +116,36 @@ __global__ void __launch_bounds__(kWinThreads) k_aed_win(double* H, double* T, i
 // ---------------------------------------------------------------------------
 // chase kernel
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kWinThreads) k_chase_win(double* H, double* T, int64_t ld, int w0, int wk, int last,
-                                                           const BulgeArr bl_g, int nb, int tmax, double* U, double* V) {
+__global__ void __launch_bounds__(kChaseThreads) k_chase_win(double* H, double* T, int64_t ld, int w0, int wk,
+                                                             int last, const BulgeArr bl_g, int nb, int tmax,
+                                                             double* U, double* V) {
   extern __shared__ double smem[];
+  const int lw = smem_ld(wk);
   double* Hs = smem;
-  double* Ts = Hs + wk * wk;
-  double* Us = Ts + wk * wk;
-  double* Vs = Us + wk * wk;
-  Bulge* bl = (Bulge*)(Vs + wk * wk);
+  double* Ts = Hs + wk * lw;
+  double* Us = Ts + wk * lw;
+  double* Vs = Us + wk * lw;
+  Bulge* bl = (Bulge*)(Vs + wk * lw);
   BulgeRec* rec = (BulgeRec*)(bl + kMaxChain);
   int* si = (int*)(rec + kMaxChain);
   DevExec x{(int)threadIdx.x, (int)blockDim.x, si, nullptr};
   for (int idx = threadIdx.x; idx < wk * wk; idx += blockDim.x) {
     int i = idx % wk, j = idx / wk;
-    Hs[idx] = G(H, ld, w0 + i, w0 + j);
-    Ts[idx] = G(T, ld, w0 + i, w0 + j);
-    Us[idx] = (i == j) ? 1.0 : 0.0;
-    Vs[idx] = (i == j) ? 1.0 : 0.0;
+    Hs[i + j * lw] = G(H, ld, w0 + i, w0 + j);
+    Ts[i + j * lw] = G(T, ld, w0 + i, w0 + j);
+    Us[i + j * lw] = (i == j) ? 1.0 : 0.0;
+    Vs[i + j * lw] = (i == j) ? 1.0 : 0.0;
   }
   for (int b = threadIdx.x; b < nb; b += blockDim.x) bl[b] = bl_g.b[b];
   __syncthreads();
-  cta_chase_window(x, wk, last, MatV{Hs, wk}, MatV{Ts, wk}, MatV{Us, wk}, MatV{Vs, wk}, bl, nb, tmax, rec);
+  cta_chase_window(x, wk, last, MatV{Hs, lw}, MatV{Ts, lw}, MatV{Us, lw}, MatV{Vs, lw}, bl, nb, tmax, rec);
   __syncthreads();
   for (int idx = threadIdx.x; idx < wk * wk; idx += blockDim.x) {
     int i = idx % wk, j = idx / wk;
-    G(H, ld, w0 + i, w0 + j) = Hs[idx];
-    G(T, ld, w0 + i, w0 + j) = Ts[idx];
-    U[idx] = Us[idx];
-    V[idx] = Vs[idx];
+    G(H, ld, w0 + i, w0 + j) = Hs[i + j * lw];
+    G(T, ld, w0 + i, w0 + j) = Ts[i + j * lw];
+    U[idx] = Us[i + j * lw];
+    V[idx] = Vs[i + j * lw];
   }
 }
 
@@ -141,28 +155,29 @@ __global__ void __launch_bounds__(kWinThreads) k_chase_win(double* H, double* T,
 __global__ void __launch_bounds__(kWinThreads) k_inf_win(double* H, double* T, int64_t ld, int w0, int wk, int top,
                                                          int jz, int stop, int deflate, double* U, double* V) {
   extern __shared__ double smem[];
+  const int lw = smem_ld(wk);
   double* Hs = smem;
-  double* Ts = Hs + wk * wk;
-  double* Us = Ts + wk * wk;
-  double* Vs = Us + wk * wk;
-  int* si = (int*)(Vs + wk * wk);
+  double* Ts = Hs + wk * lw;
+  double* Us = Ts + wk * lw;
+  double* Vs = Us + wk * lw;
+  int* si = (int*)(Vs + wk * lw);
   DevExec x{(int)threadIdx.x, (int)blockDim.x, si, nullptr};
   for (int idx = threadIdx.x; idx < wk * wk; idx += blockDim.x) {
     int i = idx % wk, j = idx / wk;
-    Hs[idx] = G(H, ld, w0 + i, w0 + j);
-    Ts[idx] = G(T, ld, w0 + i, w0 + j);
-    Us[idx] = (i == j) ? 1.0 : 0.0;
-    Vs[idx] = (i == j) ? 1.0 : 0.0;
+    Hs[i + j * lw] = G(H, ld, w0 + i, w0 + j);
+    Ts[i + j * lw] = G(T, ld, w0 + i, w0 + j);
+    Us[i + j * lw] = (i == j) ? 1.0 : 0.0;
+    Vs[i + j * lw] = (i == j) ? 1.0 : 0.0;
   }
   __syncthreads();
-  cta_inf_window(x, wk, top, jz, stop, deflate != 0, MatV{Hs, wk}, MatV{Ts, wk}, MatV{Us, wk}, MatV{Vs, wk});
+  cta_inf_window(x, wk, top, jz, stop, deflate != 0, MatV{Hs, lw}, MatV{Ts, lw}, MatV{Us, lw}, MatV{Vs, lw});
   __syncthreads();
   for (int idx = threadIdx.x; idx < wk * wk; idx += blockDim.x) {
     int i = idx % wk, j = idx / wk;
-    G(H, ld, w0 + i, w0 + j) = Hs[idx];
-    G(T, ld, w0 + i, w0 + j) = Ts[idx];
-    U[idx] = Us[idx];
-    V[idx] = Vs[idx];
+    G(H, ld, w0 + i, w0 + j) = Hs[i + j * lw];
+    G(T, ld, w0 + i, w0 + j) = Ts[i + j * lw];
+    U[idx] = Us[i + j * lw];
+    V[idx] = Vs[i + j * lw];
   }
 }
 
@@ -303,14 +318,15 @@ __global__ void k_sumsq(const double* A, int64_t ld, int o, int n, double* out) 
 // launchers
 // ---------------------------------------------------------------------------
 size_t aed_smem_bytes(int nw) {
-  size_t d = (nw <= kWinSmemMax) ? (size_t)4 * nw * nw : 0;
+  size_t d = (nw <= kWinSmemMax) ? (size_t)4 * nw * smem_ld(nw) : 0;
   d += 64 + 4 * (size_t)nw;
   return d * sizeof(double) + kSi * sizeof(int);
 }
 size_t chase_smem_bytes(int wk) {
-  return (size_t)4 * wk * wk * sizeof(double) + kMaxChain * (sizeof(Bulge) + sizeof(BulgeRec)) + kSi * sizeof(int);
+  return (size_t)4 * wk * smem_ld(wk) * sizeof(double) + kMaxChain * (sizeof(Bulge) + sizeof(BulgeRec)) +
+         kSi * sizeof(int);
 }
-size_t inf_smem_bytes(int wk) { return (size_t)4 * wk * wk * sizeof(double) + kSi * sizeof(int); }
+size_t inf_smem_bytes(int wk) { return (size_t)4 * wk * smem_ld(wk) * sizeof(double) + kSi * sizeof(int); }
 
 static size_t upd_smem(int k, int side) {
   int kp = (k + 15) & ~15;
@@ -338,15 +354,15 @@ cudaError_t kernels_init() {
 }
 
 void launch_aed(cudaStream_t st, double* H, double* T, int64_t ld, int ktop, int kwtop, int nw, const Tol& tol,
-                double* Qw, double* Zw, double* shifts, int* info, double* gscratch) {
+                double* Qw, double* Zw, double* shifts, int* info, double* gscratch, unsigned long long* ts, int nskip) {
   k_aed_win<<<1, kWinThreads, aed_smem_bytes(nw), st>>>(H, T, ld, ktop, kwtop, nw, tol, Qw, Zw, shifts, info, gscratch,
-                                                       30 * nw);
+                                                       30 * nw, ts, nskip);
 }
 void launch_chase(cudaStream_t st, double* H, double* T, int64_t ld, int w0, int wk, int last, const Bulge* bl, int nb,
                   int tmax, double* U, double* V) {
   BulgeArr arr;
   for (int b = 0; b < nb && b < kMaxChain; ++b) arr.b[b] = bl[b];
-  k_chase_win<<<1, kWinThreads, chase_smem_bytes(wk), st>>>(H, T, ld, w0, wk, last, arr, nb, tmax, U, V);
+  k_chase_win<<<1, kChaseThreads, chase_smem_bytes(wk), st>>>(H, T, ld, w0, wk, last, arr, nb, tmax, U, V);
 }
 void launch_inf(cudaStream_t st, double* H, double* T, int64_t ld, int w0, int wk, int top, int jz, int stop,
                 int deflate, double* U, double* V) {

@@ -8,9 +8,15 @@
 
 namespace qz {
 
-constexpr int kWinThreads = 128;   // threads of the one-CTA window kernels
+constexpr int kWinThreads = 128;   // threads of the one-CTA AED / zero-chase kernels
+constexpr int kChaseThreads = 256; // threads of the chase kernel
 constexpr int kWinSmemMax = 80;    // window size held entirely in shared memory (4 x 80^2 FP64 = 200 KB)
 constexpr int kMaxChain = 26;      // bulges per chain (3*26+2 rows fit a window of 80)
+
+// odd leading dimension of a shared-memory window: consecutive elements of
+// a row then fall into distinct banks (an even one puts a whole row of an
+// 80-wide window into the same bank)
+__host__ __device__ constexpr int smem_ld(int n) { return (n % 2 == 0) ? n + 1 : n; }
 
 // bulge descriptors travel as a kernel parameter (no host->device copy)
 struct BulgeArr {
@@ -23,7 +29,8 @@ size_t inf_smem_bytes(int wk);
 cudaError_t kernels_init();
 
 void launch_aed(cudaStream_t st, double* H, double* T, int64_t ld, int ktop, int kwtop, int nw, const Tol& tol,
-                double* Qw, double* Zw, double* shifts, int* info, double* gscratch);
+                double* Qw, double* Zw, double* shifts, int* info, double* gscratch,
+                unsigned long long* ts = nullptr, int nskip = 0);
 void launch_chase(cudaStream_t st, double* H, double* T, int64_t ld, int w0, int wk, int last, const Bulge* bl, int nb,
                   int tmax, double* U, double* V);
 void launch_inf(cudaStream_t st, double* H, double* T, int64_t ld, int w0, int wk, int top, int jz, int stop,

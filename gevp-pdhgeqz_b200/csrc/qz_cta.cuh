@@ -3,6 +3,7 @@
 // Each routine is a template over an executor X that supplies
 //   int tid, nt;   thread index / count inside the block
 //   void sync();   block barrier
+//   void stamp(int k);  optional phase timestamp k (profiling)
 //   int* si; double* sd;  small shared scratch (>= 64 ints, >= 256 doubles)
 // On the device X is a thin wrapper over threadIdx/__syncthreads and shared
 // memory.  Data-parallel loops are written "for (i = tid; i < n; i += nt)"
@@ -608,9 +609,11 @@ QZ_HD bool cta_move_block(X& x, WinState& w, int ifst, int nb, int ilst) {
 // caller discards it (the pencil is unchanged).
 // ---------------------------------------------------------------------------
 template <class X>
-QZ_HD void cta_aed(X& x, WinState& w, double s, double* sr, double* si_, double* sb, int maxit) {
+QZ_HD void cta_aed(X& x, WinState& w, double s, double* sr, double* si_, double* sb, int maxit, int nskip = 0) {
   int n = w.n;
+  x.stamp(0);
   int info = cta_small_qz(x, w, maxit);
+  x.stamp(1);
   if (info != 0) {
     if (x.tid == 0) { x.si[8] = n; x.si[9] = info; x.si[10] = 0; }
     x.sync();
@@ -619,7 +622,11 @@ QZ_HD void cta_aed(X& x, WinState& w, double s, double* sr, double* si_, double*
   // ---- spike test with reordering (qzearly.f:253-365) ----
   int kb = n - 1, ilst = 0;
   bool failed = false;
+  int fails = 0;  // consecutive undeflatable blocks
   while (kb >= ilst) {
+    // optional early stop: after nskip consecutive undeflatable blocks the
+    // rest of the window is left undeflated (bounds the O(n^2) swaps)
+    if (nskip > 0 && fails >= nskip) break;
     bool bulge = (kb > ilst) && (w.H(kb, kb - 1) != 0.0);
     bool dfl;
     if (!bulge) {
@@ -638,12 +645,15 @@ QZ_HD void cta_aed(X& x, WinState& w, double s, double* sr, double* si_, double*
     int nb = bulge ? 2 : 1;
     if (dfl) {
       kb -= nb;
+      fails = 0;
     } else {
       if (!cta_move_block(x, w, kb - nb + 1, nb, ilst)) { failed = true; break; }
       ilst += nb;
+      ++fails;
     }
   }
   (void)failed;
+  x.stamp(2);
   int m = kb + 1;  // undeflated eigenvalues at 0..m-1
   // ---- shifts: eigenvalues of the undeflated Schur blocks ----
   if (x.tid == 0) {
@@ -805,6 +815,7 @@ QZ_HD void cta_aed(X& x, WinState& w, double s, double* sr, double* si_, double*
     }
     x.sync();
   }
+  x.stamp(3);
   // ---- Hessenberg-triangular re-reduction of the leading m x m block
   //      by Givens rotations (the job of DGGHRD at qzearly.f:449) ----
   for (int jc = 0; jc < m - 2; ++jc) {
@@ -827,6 +838,7 @@ QZ_HD void cta_aed(X& x, WinState& w, double s, double* sr, double* si_, double*
       x.sync();
     }
   }
+  x.stamp(4);
 }
 
 }  // namespace qz

@@ -41,6 +41,9 @@ QZ_HD double dmin(double a, double b) { return a < b ? a : b; }
 QZ_HD double dsign(double a, double b) { return b >= 0.0 ? fabs(a) : -fabs(a); }
 
 // Givens rotation: c*f + s*g = r, -s*f + c*g = 0, c >= 0 when f != 0.
+// In the range where squares cannot over/underflow the rotation costs one
+// square root and one division; outside it the operands are rescaled.
+constexpr double kSafeLo = 1e-140, kSafeHi = 1e140;
 QZ_HD void lartg(double f, double g, double& c, double& s, double& r) {
   if (g == 0.0) {
     c = 1.0; s = 0.0; r = f;
@@ -49,11 +52,20 @@ QZ_HD void lartg(double f, double g, double& c, double& s, double& r) {
   } else {
     double af = fabs(f), ag = fabs(g);
     double m = af > ag ? af : ag;
-    double fs = f / m, gs = g / m;
-    double d = sqrt(fs * fs + gs * gs);
-    c = fabs(fs) / d;
-    r = dsign(d * m, f);
-    s = gs / d;
+    double d;
+    if (m > kSafeLo && m < kSafeHi) {
+      d = sqrt(f * f + g * g);
+      double inv = 1.0 / d;
+      c = af * inv;
+      s = g * inv;
+    } else {
+      double fs = f / m, gs = g / m;
+      double dd = sqrt(fs * fs + gs * gs);
+      c = fabs(fs) / dd;
+      s = gs / dd;
+      d = dd * m;
+    }
+    r = dsign(d, f);
     if (f < 0.0) s = -s;
   }
 }
@@ -63,6 +75,9 @@ QZ_HD void lartg(double f, double g, double& c, double& s, double& r) {
 QZ_HD void larfg3(double& alpha, double& x1, double& x2, double& tau) {
   double m = dmax(fabs(x1), fabs(x2));
   if (m == 0.0) { tau = 0.0; x1 = 0.0; x2 = 0.0; return; }
+  // norm with the entries divided by the largest one (one of them is then
+  // exactly 1): keeps the reflector orthogonal to a few ulp; an unscaled sum
+  // of squares or a multiplication by a rounded reciprocal measurably does not
   double ma = dmax(m, fabs(alpha));
   double a = alpha / ma, b1 = x1 / ma, b2 = x2 / ma;
   double nrm = sqrt(a * a + b1 * b1 + b2 * b2) * ma;

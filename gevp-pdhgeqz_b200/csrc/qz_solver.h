@@ -30,6 +30,8 @@ struct SolveParams {
   int maxit_factor = 30; // MAXIT = 30*NH
   int chain_max = -1;    // bulges per chain, -1: from w_chase
   int verbose = 0;       // progress lines on stderr (B200QZ_VERBOSE=1)
+  int aed_nskip = 0;     // AED spike test stops after this many consecutive
+                         // undeflatable blocks (0: test the whole window)
 };
 
 struct SolveStats {
@@ -37,6 +39,7 @@ struct SolveStats {
   int64_t endgames = 0, infs = 0, shifts = 0;
   double upd_flops = 0.0;  // FP64-equivalent flops of the off-diagonal updates
   double win_bytes = 0.0;  // algorithmic bytes of window kernels (load+store)
+  int64_t launches = 0;    // kernel launches issued by the solve
 };
 
 // reference shift-count table (piparmq.f:504-533)

@@ -71,7 +71,8 @@ int b200qz_solve_dev(b200qz_ctx* ctx, char job, char compq, char compz, int n, i
                      double* alphar, double* alphai, double* beta);
 
 /* Solve with host arrays (each with its own leading dimension); copies to
- * the device, solves, copies back. */
+ * the device (buffers cached in the context and grown on demand), solves,
+ * copies back.  Pinned host memory gives the fastest copies. */
 int b200qz_solve_host(b200qz_ctx* ctx, char job, char compq, char compz, int n, int ilo, int ihi,
                       double* h, int ldh, double* t, int ldt, double* q, int ldq, double* z, int ldz,
                       double* alphar, double* alphai, double* beta);
@@ -80,7 +81,13 @@ int b200qz_solve_host(b200qz_ctx* ctx, char job, char compq, char compz, int n, 
  * 0 seconds (device time), 1 iterations, 2 AEDs, 3 AED deflations,
  * 4 sweeps, 5 chains, 6 windows, 7 endgames, 8 infinite-eigenvalue
  * steps, 9 shifts used, 10 update flops (FP64-equivalent), 11 window
- * kernel bytes.  Returns the number of values written. */
+ * kernel bytes; with B200QZ_PROFILE=1 set during the solve also device
+ * milliseconds per phase: 12 scan, 13 AED, 14 AED updates, 15 chase,
+ * 16 chase updates, 17 infinite-eigenvalue deflation, 18 finalisation,
+ * and inside the AED kernel 19 small QZ, 20 reordering, 21 spike
+ * reflector + RQ update, 22 Hessenberg-triangular re-reduction;
+ * 23 kernel launches issued by the solve.
+ * Returns the number of values written. */
 int b200qz_get_stats(const b200qz_ctx* ctx, double* out, int nout);
 
 /* Tunables: nw_max (AED window), w_chase (chase window), nmin (blocks
@@ -88,6 +95,13 @@ int b200qz_get_stats(const b200qz_ctx* ctx, double* out, int nout);
  * A value < 0 keeps the current setting. Returns 0 or -i for argument i. */
 int b200qz_set_params(b200qz_ctx* ctx, int nw_max, int w_chase, int nmin, int nibble, int ns_max,
                       int maxit_factor);
+
+/* Set one tunable by name: "nw_max", "w_chase", "nmin", "nibble",
+ * "ns_max", "maxit_factor", "chain_max" (bulges per chain), "aed_nskip"
+ * (AED spike test stops after this many consecutive undeflatable blocks,
+ * 0 = whole window).  Returns 0, -2 for an unknown name, -3 for a value
+ * out of range. */
+int b200qz_set_param(b200qz_ctx* ctx, const char* name, double value);
 
 /* ------------------------------------------------------------------ */
 /* Kernel-level entry points (device pointers), for parity tests.       */

@@ -117,3 +117,87 @@ def test_aed_window(pkg, lapack, solver, n, nw, seed):
     assert np.all(W1[m:, :m] == 0)
     # nothing outside the window changed
     assert np.array_equal(Hn[:kwtop, :], H[:kwtop, :]) and np.array_equal(Hn[:, :kwtop - 1], H[:, :kwtop - 1])
+
+
+def _shift_set(rng, nb, cplx):
+    """nb shift pairs as (sr, si, sb) lists and polynomial coefficients."""
+    sr, si, sb, coef = [], [], [], []
+    for b in range(nb):
+        if cplx and b % 2 == 0:
+            ar, ai = rng.standard_normal(), abs(rng.standard_normal()) + 0.1
+            sr += [ar, ar]; si += [ai, -ai]; sb += [1.0, 1.0]
+            coef += [1.0, 2 * ar, ar * ar + ai * ai]
+        else:
+            a1, a2 = rng.standard_normal(2)
+            sr += [a1, a2]; si += [0.0, 0.0]; sb += [1.0, 1.0]
+            coef += [1.0, a1 + a2, a1 * a2]
+    return np.array(sr), np.array(si), np.array(sb), np.array(coef)
+
+
+@pytest.mark.parametrize("n,nb,cplx", [(12, 1, False), (30, 3, False), (50, 5, True), (60, 6, True), (80, 12, True)])
+def test_chase_window_matches_restatement(pkg, solver, n, nb, cplx):
+    """Chase of an introduced chain through one window (lockstep, GPU)
+    against the oracle's bulge-by-bulge PDHGEQZB/DHGEQZ5 restatement from
+    the same state (the oracle's PDHGEQZA introduction).  Both apply the
+    same reflectors in exact arithmetic, so H, T, U (=Q), V (=Z) agree to
+    rounding: 1e-9 relative.  (Whole sweeps are not compared element-wise:
+    the two codes form the shift polynomial's first column with different
+    roundings, and a long chase amplifies that difference.)"""
+    from oracle import qzref as R
+    H, T = pkg.pencils.random_ht(n, 20 + n)
+    rng = np.random.default_rng(n)
+    sr, si, sb, coef = _shift_set(rng, nb, cplx)
+    H1, T1, _, _ = R.sweep(H, T, sr, si, sb, phase=1)
+    S_ref, P_ref, Q_ref, Z_ref = R.sweep(H1, T1, sr, si, sb, phase=2)
+    bul, tmax = [], 0
+    for k in range(nb):
+        base = 3 * (nb - 1 - k) + 1   # next step row of bulge k (0 = deepest)
+        thi = (n - 1) - base           # chase to the bottom and push off
+        bul += [base, 0, thi, 0]
+        tmax = max(tmax, thi)
+    bul = (ctypes.c_int * len(bul))(*bul)
+    cf = (ctypes.c_double * len(coef))(*coef.tolist())
+    dH, dT = colmajor_cuda(H1), colmajor_cuda(T1)
+    dU = torch.zeros(n * n, dtype=torch.float64, device="cuda")
+    dV = torch.zeros_like(dU)
+    rc = pkg.lib().b200qz_chase_window(solver.handle, dH.data_ptr(), dT.data_ptr(), n, 0, n, n - 1, bul, cf, nb,
+                                       tmax, dU.data_ptr(), dV.data_ptr())
+    assert rc == 0
+    S, P = to_np(dH, n, n), to_np(dT, n, n)
+    U = dU.cpu().numpy().reshape(n, n).T
+    V = dV.cpu().numpy().reshape(n, n).T
+    assert np.linalg.norm(U @ S @ V.T - H1) <= 50 * n * EPS * np.linalg.norm(H1)
+    assert np.linalg.norm(U @ P @ V.T - T1) <= 50 * n * EPS * np.linalg.norm(T1)
+    assert np.all(np.tril(S, -2) == 0) and np.all(np.tril(P, -1) == 0)
+    for a, b in ((S, S_ref), (P, P_ref), (U, Q_ref), (V, Z_ref)):
+        assert np.linalg.norm(a - b) <= 1e-9 * max(1.0, np.linalg.norm(b)), np.linalg.norm(a - b)
+
+
+@pytest.mark.parametrize("n,nb,cplx", [(40, 4, True), (80, 12, False)])
+def test_chase_window_full_sweep_backward_stable(pkg, solver, n, nb, cplx):
+    """Introduction + chase + push-off in one window: an orthogonal
+    equivalence to 50*n*eps that returns a Hessenberg-triangular pencil."""
+    H, T = pkg.pencils.random_ht(n, 40 + n)
+    rng = np.random.default_rng(n + 1)
+    sr, si, sb, coef = _shift_set(rng, nb, cplx)
+    bul, tmax = [], 0
+    for k in range(nb):
+        base, tlo = -3 * k, 3 * k
+        thi = (n - 1) - base
+        bul += [base, tlo, thi, 1]
+        tmax = max(tmax, thi)
+    bul = (ctypes.c_int * len(bul))(*bul)
+    cf = (ctypes.c_double * len(coef))(*coef.tolist())
+    dH, dT = colmajor_cuda(H), colmajor_cuda(T)
+    dU = torch.zeros(n * n, dtype=torch.float64, device="cuda")
+    dV = torch.zeros_like(dU)
+    rc = pkg.lib().b200qz_chase_window(solver.handle, dH.data_ptr(), dT.data_ptr(), n, 0, n, n - 1, bul, cf, nb,
+                                       tmax, dU.data_ptr(), dV.data_ptr())
+    assert rc == 0
+    S, P = to_np(dH, n, n), to_np(dT, n, n)
+    U = dU.cpu().numpy().reshape(n, n).T
+    V = dV.cpu().numpy().reshape(n, n).T
+    assert np.linalg.norm(U @ S @ V.T - H) <= 50 * n * EPS * np.linalg.norm(H)
+    assert np.linalg.norm(U @ P @ V.T - T) <= 50 * n * EPS * np.linalg.norm(T)
+    assert np.linalg.norm(U.T @ U - np.eye(n)) <= 50 * n * EPS
+    assert np.all(np.tril(S, -2) == 0) and np.all(np.tril(P, -1) == 0)
