@@ -61,7 +61,8 @@ EXPORTS = (
 STAT_NAMES = ("seconds", "iters", "aeds", "aed_deflations", "sweeps", "chains", "windows",
               "endgames", "inf_steps", "shifts", "update_flops", "window_bytes",
               "ms_scan", "ms_aed", "ms_aed_update", "ms_chase", "ms_chase_update", "ms_inf", "ms_final",
-              "ms_aed_smallqz", "ms_aed_reorder", "ms_aed_spike", "ms_aed_hessred", "launches")
+              "ms_aed_smallqz", "ms_aed_reorder", "ms_aed_spike", "ms_aed_hessred", "launches",
+              "aed_failures")
 
 
 def lib() -> ctypes.CDLL:

@@ -21,6 +21,7 @@ using namespace qz;
 
 namespace {
 constexpr int kAedMax = 512;  // largest AED / small-solve window supported
+constexpr int64_t kUslot = (int64_t)kWinSmemMax * kWinSmemMax;  // one window's factor in Uc/Vc
 }
 
 // Phase timer: CUDA event pairs recorded around each group of launches on
@@ -155,6 +156,7 @@ struct GpuBackend {
     info3[0] = c->hinfo[4];
     info3[1] = c->hinfo[5];
     info3[2] = c->hinfo[6];
+    if (info3[1] != 0) dump_window(ktop, kwtop, nw);
     int m = std::min(info3[0], nw);
     for (int i = 0; i < m; ++i) {
       sh[i] = c->hshifts[i];
@@ -163,13 +165,53 @@ struct GpuBackend {
     }
     c->stats.win_bytes += 2.0 * 2.0 * 8.0 * nw * nw + 2.0 * 8.0 * nw * nw;
   }
-  void chase(int w, int wk, int last, const Bulge* bl, int nb, int tmax) {
+  // With B200QZ_DUMP_DIR set, a window whose small QZ did not converge is
+  // written to <dir>/aed_fail_<kwtop>.bin (int32 nw, double spike, then the
+  // nw x nw windows of H and T, column-major) for offline study.  The
+  // kernel leaves a failed window untouched, so it is read back as it was.
+  void dump_window(int ktop, int kwtop, int nw) {
+    const char* dir = std::getenv("B200QZ_DUMP_DIR");
+    if (!dir || !*dir) return;
+    std::vector<double> hw((size_t)nw * nw), tw((size_t)nw * nw);
+    double sp = 0.0;
+    for (int j = 0; j < nw; ++j) {
+      QZ_CK(cudaMemcpy(hw.data() + (size_t)j * nw, H + kwtop + (kwtop + j) * ld, nw * sizeof(double),
+                       cudaMemcpyDeviceToHost));
+      QZ_CK(cudaMemcpy(tw.data() + (size_t)j * nw, T + kwtop + (kwtop + j) * ld, nw * sizeof(double),
+                       cudaMemcpyDeviceToHost));
+    }
+    if (kwtop > ktop) QZ_CK(cudaMemcpy(&sp, H + kwtop + (kwtop - 1) * ld, sizeof(double), cudaMemcpyDeviceToHost));
+    std::string path = std::string(dir) + "/aed_fail_" + std::to_string(kwtop) + ".bin";
+    FILE* f = std::fopen(path.c_str(), "wb");
+    if (!f) return;
+    int32_t n32 = nw;
+    std::fwrite(&n32, sizeof(n32), 1, f);
+    std::fwrite(&sp, sizeof(sp), 1, f);
+    std::fwrite(hw.data(), sizeof(double), hw.size(), f);
+    std::fwrite(tw.data(), sizeof(double), tw.size(), f);
+    std::fclose(f);
+  }
+
+  // one CTA per window of the wave; window i's factors go to slot i
+  void chase_wave(const WinPlan* const* wins, int nw) {
+    ChaseWave wave;
+    for (int i = 0; i < nw; ++i) {
+      const WinPlan& p = *wins[i];
+      ChaseJob& J = wave.job[i];
+      J.w0 = p.w; J.wk = p.wk; J.last = p.last; J.nb = p.nb; J.tmax = p.tmax;
+      for (int b = 0; b < p.nb; ++b) J.bl[b] = p.bl[b];
+      c->stats.win_bytes += 2.0 * 2.0 * 8.0 * p.wk * p.wk + 2.0 * 8.0 * p.wk * p.wk;
+    }
     c->timer.begin(kPhChase, c->stream);
-    launch_chase(c->stream, H, T, ld, w, wk, last, bl, nb, tmax, c->Uc, c->Vc);
-    c->stats.launches += 1;
+    launch_chase_wave(c->stream, H, T, ld, wave, nw, c->Uc, c->Vc, kUslot);
     c->timer.end(c->stream);
-    c->kc = wk;
-    c->stats.win_bytes += 2.0 * 2.0 * 8.0 * wk * wk + 2.0 * 8.0 * wk * wk;
+    c->stats.launches += 1;
+    c->kc = kWinSmemMax;
+  }
+  void update_wave(const WinPlan* const* wins, int nw) {
+    std::vector<int> w(nw), wk(nw);
+    for (int i = 0; i < nw; ++i) { w[i] = wins[i]->w; wk[i] = wins[i]->wk; }
+    update_list(w.data(), wk.data(), nw, c->Uc, c->Vc, kUslot, kPhChaseUpd);
   }
   void inf_window(int w, int wk, int top, int jz, int stop, bool deflate) {
     c->timer.begin(kPhInf, c->stream);
@@ -185,47 +227,57 @@ struct GpuBackend {
     c->stats.launches += 1;
     c->timer.end(c->stream);
   }
-  // off-diagonal updates with the factors of the last window kernel
+  // off-diagonal updates with the factors of the last AED (which 0) or
+  // zero-chase (which 1) window kernel
   void update(int w, int wk, int which) {
-    const double* U = which == 0 ? c->Ua : c->Uc;
-    const double* V = which == 0 ? c->Va : c->Vc;
-    int tile = update_tile(wk);
-    UpdBatch L;
-    L.k = wk;
+    if (which == 0) update_list(&w, &wk, 1, c->Ua, c->Va, 0, kPhAedUpd);
+    else update_list(&w, &wk, 1, c->Uc, c->Vc, kUslot, kPhChaseUpd);
+  }
+  // Far updates of a list of disjoint windows (window i's factors at
+  // U + i*ustride, V + i*ustride): one batched launch for every left
+  // update (rows of a window, columns to its right), then one for every
+  // right update (rows above a window, its columns; Q and Z columns).
+  void update_list(const int* w, const int* wk, int nwin, const double* Ub, const double* Vb, int64_t ustride,
+                   int phase) {
+    UpdBatch L, R;
     L.njobs = 0;
-    int right_len = n - (w + wk);
-    if (right_len > 0) {
-      for (double* M : {H, T}) {
-        UpdJob& j = L.job[L.njobs++];
-        j.M = M; j.ld = ld; j.r0 = w; j.c0 = w + wk; j.len = right_len; j.W = U; j.ldw = wk;
-        j.tiles = (right_len + tile - 1) / tile;
-      }
-      c->stats.upd_flops += 2.0 * 2.0 * wk * wk * right_len;
-    }
-    UpdBatch R;
-    R.k = wk;
     R.njobs = 0;
-    if (w > 0) {
-      for (double* M : {H, T}) {
-        UpdJob& j = R.job[R.njobs++];
-        j.M = M; j.ld = ld; j.r0 = 0; j.c0 = w; j.len = w; j.W = V; j.ldw = wk;
-        j.tiles = (w + tile - 1) / tile;
+    for (int i = 0; i < nwin; ++i) {
+      const double* U = Ub + i * ustride;
+      const double* V = Vb + i * ustride;
+      int k = wk[i], w0 = w[i];
+      int tile = update_tile(k);
+      int right_len = n - (w0 + k);
+      if (right_len > 0) {
+        for (double* M : {H, T}) {
+          UpdJob& j = L.job[L.njobs++];
+          j.M = M; j.ld = ld; j.r0 = w0; j.c0 = w0 + k; j.len = right_len; j.W = U; j.ldw = k; j.k = k;
+          j.tiles = (right_len + tile - 1) / tile;
+        }
+        c->stats.upd_flops += 2.0 * 2.0 * k * k * right_len;
       }
-      c->stats.upd_flops += 2.0 * 2.0 * wk * wk * w;
+      if (w0 > 0) {
+        for (double* M : {H, T}) {
+          UpdJob& j = R.job[R.njobs++];
+          j.M = M; j.ld = ld; j.r0 = 0; j.c0 = w0; j.len = w0; j.W = V; j.ldw = k; j.k = k;
+          j.tiles = (w0 + tile - 1) / tile;
+        }
+        c->stats.upd_flops += 2.0 * 2.0 * k * k * w0;
+      }
+      if (wantq) {
+        UpdJob& j = R.job[R.njobs++];
+        j.M = Q; j.ld = ld; j.r0 = 0; j.c0 = w0; j.len = n; j.W = U; j.ldw = k; j.k = k;
+        j.tiles = (n + tile - 1) / tile;
+        c->stats.upd_flops += 2.0 * k * k * n;
+      }
+      if (wantz) {
+        UpdJob& j = R.job[R.njobs++];
+        j.M = Z; j.ld = ld; j.r0 = 0; j.c0 = w0; j.len = n; j.W = V; j.ldw = k; j.k = k;
+        j.tiles = (n + tile - 1) / tile;
+        c->stats.upd_flops += 2.0 * k * k * n;
+      }
     }
-    if (wantq) {
-      UpdJob& j = R.job[R.njobs++];
-      j.M = Q; j.ld = ld; j.r0 = 0; j.c0 = w; j.len = n; j.W = U; j.ldw = wk;
-      j.tiles = (n + tile - 1) / tile;
-      c->stats.upd_flops += 2.0 * wk * wk * n;
-    }
-    if (wantz) {
-      UpdJob& j = R.job[R.njobs++];
-      j.M = Z; j.ld = ld; j.r0 = 0; j.c0 = w; j.len = n; j.W = V; j.ldw = wk;
-      j.tiles = (n + tile - 1) / tile;
-      c->stats.upd_flops += 2.0 * wk * wk * n;
-    }
-    c->timer.begin(which == 0 ? kPhAedUpd : kPhChaseUpd, c->stream);
+    c->timer.begin(phase, c->stream);
     if (L.njobs) { launch_update(c->stream, L, 0); c->stats.launches += 1; }
     if (R.njobs) { launch_update(c->stream, R, 1); c->stats.launches += 1; }
     c->timer.end(c->stream);
@@ -315,7 +367,7 @@ int b200qz_create(b200qz_ctx** out, int device) {
   if (e == cudaSuccess) e = kernels_init();
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
   size_t a2 = (size_t)kAedMax * kAedMax * sizeof(double);
-  size_t w2 = (size_t)kWinSmemMax * kWinSmemMax * sizeof(double);
+  size_t w2 = (size_t)kMaxWave * kUslot * sizeof(double);
   if (e == cudaSuccess) e = cudaMalloc(&c->Ua, a2);
   if (e == cudaSuccess) e = cudaMalloc(&c->Va, a2);
   if (e == cudaSuccess) e = cudaMalloc(&c->Uc, w2);
@@ -388,6 +440,7 @@ int b200qz_set_param(b200qz_ctx* c, const char* name, double value) {
   else if (k == "maxit_factor") { if (v < 1) return -3; P.maxit_factor = v; }
   else if (k == "chain_max") { if (v < 1 || v > kMaxChain) return -3; P.chain_max = v; }
   else if (k == "aed_nskip") { if (v < 0) return -3; P.aed_nskip = v; }
+  else if (k == "max_wave") { if (v < 1 || v > kMaxWave) return -3; P.max_wave = v; }
   else return -2;
   return 0;
 }
@@ -462,12 +515,13 @@ int b200qz_get_stats(const b200qz_ctx* c, double* out, int nout) {
   if (!c || !out) return 0;
   const SolveStats& s = c->stats;
   const double* ph = c->timer.ms;
-  double v[24] = {c->seconds, (double)s.iters, (double)s.aeds, (double)s.aed_defl, (double)s.sweeps,
+  double v[25] = {c->seconds, (double)s.iters, (double)s.aeds, (double)s.aed_defl, (double)s.sweeps,
                   (double)s.chains, (double)s.windows, (double)s.endgames, (double)s.infs, (double)s.shifts,
                   s.upd_flops, s.win_bytes,
                   ph[kPhScan], ph[kPhAed], ph[kPhAedUpd], ph[kPhChase], ph[kPhChaseUpd], ph[kPhInf], ph[kPhFinal],
-                  c->aed_ms[0], c->aed_ms[1], c->aed_ms[2], c->aed_ms[3], (double)s.launches};
-  int k = std::min(nout, 24);
+                  c->aed_ms[0], c->aed_ms[1], c->aed_ms[2], c->aed_ms[3], (double)s.launches,
+                  (double)s.aed_fail};
+  int k = std::min(nout, 25);
   for (int i = 0; i < k; ++i) out[i] = v[i];
   return k;
 }
@@ -507,17 +561,19 @@ int b200qz_chase_window(b200qz_ctx* c, double* h, double* t, int ld, int w, int 
   if (wk < 4 || wk > kWinSmemMax || nb < 1 || nb > kMaxChain || last >= wk) return -1;
   c->err = cudaSuccess;
   QZ_CK(cudaSetDevice(c->device));
-  Bulge bl[kMaxChain];
+  ChaseWave wave;
+  ChaseJob& J = wave.job[0];
+  J.w0 = w; J.wk = wk; J.last = last; J.nb = nb; J.tmax = tmax;
   for (int b = 0; b < nb; ++b) {
-    bl[b].base = bulges[4 * b];
-    bl[b].tlo = bulges[4 * b + 1];
-    bl[b].thi = bulges[4 * b + 2];
-    bl[b].intro = bulges[4 * b + 3];
-    bl[b].c2 = coef[3 * b];
-    bl[b].c1 = coef[3 * b + 1];
-    bl[b].c0 = coef[3 * b + 2];
+    J.bl[b].base = bulges[4 * b];
+    J.bl[b].tlo = bulges[4 * b + 1];
+    J.bl[b].thi = bulges[4 * b + 2];
+    J.bl[b].intro = bulges[4 * b + 3];
+    J.bl[b].c2 = coef[3 * b];
+    J.bl[b].c1 = coef[3 * b + 1];
+    J.bl[b].c0 = coef[3 * b + 2];
   }
-  launch_chase(c->stream, h, t, ld, w, wk, last, bl, nb, tmax, u, v);
+  launch_chase_wave(c->stream, h, t, ld, wave, 1, u, v, 0);
   QZ_CK(cudaGetLastError());
   QZ_CK(cudaStreamSynchronize(c->stream));
   return c->err == cudaSuccess ? 0 : 10001;
@@ -533,7 +589,7 @@ int b200qz_update(b200qz_ctx* c, char side, double* m, int ldm, int r0, int c0, 
   B.k = k;
   B.njobs = 1;
   UpdJob& j = B.job[0];
-  j.M = m; j.ld = ldm; j.r0 = r0; j.c0 = c0; j.len = len; j.W = w; j.ldw = ldw;
+  j.M = m; j.ld = ldm; j.r0 = r0; j.c0 = c0; j.len = len; j.W = w; j.ldw = ldw; j.k = k;
   int tile = update_tile(k);
   j.tiles = (len + tile - 1) / tile;
   if (is(side, 'L')) launch_update(c->stream, B, 0);

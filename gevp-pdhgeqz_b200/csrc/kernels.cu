@@ -116,10 +116,13 @@ __global__ void __launch_bounds__(kWinThreads) k_aed_win(double* H, double* T, i
 // ---------------------------------------------------------------------------
 // chase kernel
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kChaseThreads) k_chase_win(double* H, double* T, int64_t ld, int w0, int wk,
-                                                             int last, const BulgeArr bl_g, int nb, int tmax,
-                                                             double* U, double* V) {
+__global__ void __launch_bounds__(kChaseThreads) k_chase_win(double* H, double* T, int64_t ld, const ChaseWave wave,
+                                                             double* Ug, double* Vg, int64_t ustride) {
   extern __shared__ double smem[];
+  const ChaseJob& J = wave.job[blockIdx.x];
+  const int w0 = J.w0, wk = J.wk, last = J.last, nb = J.nb, tmax = J.tmax;
+  double* U = Ug + blockIdx.x * ustride;
+  double* V = Vg + blockIdx.x * ustride;
   const int lw = smem_ld(wk);
   double* Hs = smem;
   double* Ts = Hs + wk * lw;
@@ -136,7 +139,7 @@ __global__ void __launch_bounds__(kChaseThreads) k_chase_win(double* H, double* 
     Us[i + j * lw] = (i == j) ? 1.0 : 0.0;
     Vs[i + j * lw] = (i == j) ? 1.0 : 0.0;
   }
-  for (int b = threadIdx.x; b < nb; b += blockDim.x) bl[b] = bl_g.b[b];
+  for (int b = threadIdx.x; b < nb; b += blockDim.x) bl[b] = J.bl[b];
   __syncthreads();
   cta_chase_window(x, wk, last, MatV{Hs, lw}, MatV{Ts, lw}, MatV{Us, lw}, MatV{Vs, lw}, bl, nb, tmax, rec);
   __syncthreads();
@@ -358,11 +361,12 @@ void launch_aed(cudaStream_t st, double* H, double* T, int64_t ld, int ktop, int
   k_aed_win<<<1, kWinThreads, aed_smem_bytes(nw), st>>>(H, T, ld, ktop, kwtop, nw, tol, Qw, Zw, shifts, info, gscratch,
                                                        30 * nw, ts, nskip);
 }
-void launch_chase(cudaStream_t st, double* H, double* T, int64_t ld, int w0, int wk, int last, const Bulge* bl, int nb,
-                  int tmax, double* U, double* V) {
-  BulgeArr arr;
-  for (int b = 0; b < nb && b < kMaxChain; ++b) arr.b[b] = bl[b];
-  k_chase_win<<<1, kChaseThreads, chase_smem_bytes(wk), st>>>(H, T, ld, w0, wk, last, arr, nb, tmax, U, V);
+void launch_chase_wave(cudaStream_t st, double* H, double* T, int64_t ld, const ChaseWave& wave, int njob, double* U,
+                       double* V, int64_t ustride) {
+  if (njob <= 0) return;
+  int wmax = 0;
+  for (int i = 0; i < njob; ++i) wmax = wave.job[i].wk > wmax ? wave.job[i].wk : wmax;
+  k_chase_win<<<njob, kChaseThreads, chase_smem_bytes(wmax), st>>>(H, T, ld, wave, U, V, ustride);
 }
 void launch_inf(cudaStream_t st, double* H, double* T, int64_t ld, int w0, int wk, int top, int jz, int stop,
                 int deflate, double* U, double* V) {
@@ -374,9 +378,14 @@ void launch_scan(cudaStream_t st, double* H, double* T, int64_t ld, int ifirst, 
 void launch_inf_top(cudaStream_t st, double* H, double* T, double* Q, int64_t ld, int n, int f, int wantq) {
   k_inf_top<<<1, 1024, 0, st>>>(H, T, Q, ld, n, f, wantq);
 }
-void launch_update(cudaStream_t st, const UpdBatch& B, int side) {
+void launch_update(cudaStream_t st, const UpdBatch& B_in, int side) {
+  UpdBatch B = B_in;
   int tiles = 0;
-  for (int j = 0; j < B.njobs; ++j) tiles += B.job[j].tiles;
+  B.k = 0;
+  for (int j = 0; j < B.njobs; ++j) {
+    tiles += B.job[j].tiles;
+    if (B.job[j].k > B.k) B.k = B.job[j].k;
+  }
   if (tiles == 0) return;
   if (B.k > kUpdMaxK) {
     if (side == 0) k_update_left_gen<<<tiles, 256, upd_smem(B.k, 0), st>>>(B);

@@ -18,9 +18,16 @@ constexpr int kMaxChain = 26;      // bulges per chain (3*26+2 rows fit a window
 // 80-wide window into the same bank)
 __host__ __device__ constexpr int smem_ld(int n) { return (n % 2 == 0) ? n + 1 : n; }
 
-// bulge descriptors travel as a kernel parameter (no host->device copy)
-struct BulgeArr {
-  Bulge b[kMaxChain];
+// chains chased concurrently (one CTA each) by one wave launch
+constexpr int kMaxWave = 8;
+
+// window jobs travel as a kernel parameter (no host->device copy)
+struct ChaseJob {
+  int w0, wk, last, nb, tmax;
+  Bulge bl[kMaxChain];
+};
+struct ChaseWave {
+  ChaseJob job[kMaxWave];
 };
 
 size_t aed_smem_bytes(int nw);
@@ -31,8 +38,9 @@ cudaError_t kernels_init();
 void launch_aed(cudaStream_t st, double* H, double* T, int64_t ld, int ktop, int kwtop, int nw, const Tol& tol,
                 double* Qw, double* Zw, double* shifts, int* info, double* gscratch,
                 unsigned long long* ts = nullptr, int nskip = 0);
-void launch_chase(cudaStream_t st, double* H, double* T, int64_t ld, int w0, int wk, int last, const Bulge* bl, int nb,
-                  int tmax, double* U, double* V);
+// one CTA per job; job i writes its factors to U + i*ustride, V + i*ustride
+void launch_chase_wave(cudaStream_t st, double* H, double* T, int64_t ld, const ChaseWave& wave, int njob, double* U,
+                       double* V, int64_t ustride);
 void launch_inf(cudaStream_t st, double* H, double* T, int64_t ld, int w0, int wk, int top, int jz, int stop,
                 int deflate, double* U, double* V);
 void launch_scan(cudaStream_t st, double* H, double* T, int64_t ld, int ifirst, int kbot, const Tol& tol, int* out);

@@ -40,10 +40,10 @@ struct BulgeRec {
   int kind;  // 0 inactive, 1: 3x3 step, 2: terminal 2x2 step
   int j;
   int writecol;  // 1: store H(j:j+2, j-1) in phase B
-  double tau, v1, v2;     // left reflector (kind 1) / rotation c,s in tau,v1 (kind 2)
-  double taur, u1, u2;    // right reflector (kind 1) / rotation c,s in taur,u1 (kind 2)
-  double beta;            // new H(j, j-1)
-  double tb[9];           // final T block
+  House3 L;      // left reflector (kind 1); kind 2: rotation c, s in L.s, L.u0
+  House3 R;      // right reflector (kind 1); kind 2: rotation c, s in R.s, R.u0
+  double beta;   // new H(j, j-1)
+  double tb[9];  // final T block
 };
 
 // Compute the step of one bulge at window row j.  last = last active row
@@ -62,19 +62,15 @@ QZ_HD void bulge_step_compute(MatV H, MatV T, int j, int last, bool intro,
       a0 = H(j, j - 1); a1 = H(j + 1, j - 1); a2 = H(j + 2, j - 1);
       r.writecol = 1;
     }
-    double tau, v1 = a1, v2 = a2, beta = a0;
-    larfg3(beta, v1, v2, tau);
+    house3(a0, a1, a2, r.L, r.beta);
     double* tb = r.tb;
     for (int cc = 0; cc < 3; ++cc)
       for (int rr = 0; rr < 3; ++rr) tb[rr + 3 * cc] = T(j + rr, j + cc);
-    for (int cc = 0; cc < 3; ++cc) refl3(tau, v1, v2, tb[3 * cc], tb[3 * cc + 1], tb[3 * cc + 2]);
-    double taur, u1, u2;
-    opposite_reflector3(tb, taur, u1, u2);
-    for (int rr = 0; rr < 3; ++rr) refl3(taur, u1, u2, tb[rr], tb[rr + 3], tb[rr + 6]);
+    for (int cc = 0; cc < 3; ++cc) house3_apply(r.L, tb[3 * cc], tb[3 * cc + 1], tb[3 * cc + 2]);
+    opposite_house3(tb, r.R);
+    for (int rr = 0; rr < 3; ++rr) house3_apply(r.R, tb[rr], tb[rr + 3], tb[rr + 6]);
     tb[1] = 0.0;
     tb[2] = 0.0;
-    r.tau = tau; r.v1 = v1; r.v2 = v2; r.beta = beta;
-    r.taur = taur; r.u1 = u1; r.u2 = u2;
   } else {
     // terminal 2x2 step at rows j, j+1 = last
     r.kind = 2;
@@ -88,8 +84,8 @@ QZ_HD void bulge_step_compute(MatV H, MatV T, int j, int last, bool intro,
     opposite_rot2(t10, t11, cr, sr);
     rot2(cr, sr, t00, t01);
     rot2(cr, sr, t10, t11);
-    r.tau = c; r.v1 = s; r.beta = rr;
-    r.taur = cr; r.u1 = sr;
+    r.L.s = c; r.L.u0 = s; r.beta = rr;
+    r.R.s = cr; r.R.u0 = sr;
     r.tb[0] = t00; r.tb[1] = 0.0; r.tb[3] = t01; r.tb[4] = t11;
   }
 }
@@ -136,22 +132,22 @@ QZ_HD void cta_chase_window(X& x, int wk, int last, MatV H, MatV T, MatV U, MatV
           if (i < nh) {
             int c = j + i;
             double a0 = H(j, c), a1 = H(j + 1, c), a2 = H(j + 2, c);
-            refl3(r.tau, r.v1, r.v2, a0, a1, a2);
+            house3_apply(r.L, a0, a1, a2);
             H(j, c) = a0; H(j + 1, c) = a1; H(j + 2, c) = a2;
           } else if (i < nh + (nt > 0 ? nt : 0)) {
             int c = j + 3 + (i - nh);
             double a0 = T(j, c), a1 = T(j + 1, c), a2 = T(j + 2, c);
-            refl3(r.tau, r.v1, r.v2, a0, a1, a2);
+            house3_apply(r.L, a0, a1, a2);
             T(j, c) = a0; T(j + 1, c) = a1; T(j + 2, c) = a2;
           } else {
             int rr = i - nh - (nt > 0 ? nt : 0);
             double a0 = U(rr, j), a1 = U(rr, j + 1), a2 = U(rr, j + 2);
-            refl3(r.tau, r.v1, r.v2, a0, a1, a2);
+            house3_apply(r.L, a0, a1, a2);
             U(rr, j) = a0; U(rr, j + 1) = a1; U(rr, j + 2) = a2;
           }
         }
       } else {
-        double c = r.tau, s = r.v1;
+        double c = r.L.s, s = r.L.u0;
         int nh = wk - j, nt = wk - (j + 2);
         int tot = nh + (nt > 0 ? nt : 0) + wk;
         for (int i = x.tid; i < tot; i += x.nt) {
@@ -183,22 +179,22 @@ QZ_HD void cta_chase_window(X& x, int wk, int last, MatV H, MatV T, MatV U, MatV
         for (int i = x.tid; i < tot; i += x.nt) {
           if (i < hr) {
             double a0 = H(i, j), a1 = H(i, j + 1), a2 = H(i, j + 2);
-            refl3(r.taur, r.u1, r.u2, a0, a1, a2);
+            house3_apply(r.R, a0, a1, a2);
             H(i, j) = a0; H(i, j + 1) = a1; H(i, j + 2) = a2;
           } else if (i < hr + j) {
             int rr = i - hr;
             double a0 = T(rr, j), a1 = T(rr, j + 1), a2 = T(rr, j + 2);
-            refl3(r.taur, r.u1, r.u2, a0, a1, a2);
+            house3_apply(r.R, a0, a1, a2);
             T(rr, j) = a0; T(rr, j + 1) = a1; T(rr, j + 2) = a2;
           } else {
             int rr = i - hr - j;
             double a0 = V(rr, j), a1 = V(rr, j + 1), a2 = V(rr, j + 2);
-            refl3(r.taur, r.u1, r.u2, a0, a1, a2);
+            house3_apply(r.R, a0, a1, a2);
             V(rr, j) = a0; V(rr, j + 1) = a1; V(rr, j + 2) = a2;
           }
         }
       } else {
-        double c = r.taur, s = r.u1;
+        double c = r.R.s, s = r.R.u0;
         int hr = last + 1;
         int tot = hr + j + wk;
         for (int i = x.tid; i < tot; i += x.nt) {

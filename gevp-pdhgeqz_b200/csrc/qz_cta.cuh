@@ -65,6 +65,22 @@ QZ_HD void par_refl_cols(X& x, MatV M, int c, double tau, double v1, double v2, 
   }
 }
 template <class X>
+QZ_HD void par_house_rows(X& x, MatV M, int r, const House3& h, int c_lo, int c_hi) {
+  for (int j = c_lo + x.tid; j < c_hi; j += x.nt) {
+    double a0 = M(r, j), a1 = M(r + 1, j), a2 = M(r + 2, j);
+    house3_apply(h, a0, a1, a2);
+    M(r, j) = a0; M(r + 1, j) = a1; M(r + 2, j) = a2;
+  }
+}
+template <class X>
+QZ_HD void par_house_cols(X& x, MatV M, int c, const House3& h, int r_lo, int r_hi) {
+  for (int i = r_lo + x.tid; i < r_hi; i += x.nt) {
+    double a0 = M(i, c), a1 = M(i, c + 1), a2 = M(i, c + 2);
+    house3_apply(h, a0, a1, a2);
+    M(i, c) = a0; M(i, c + 1) = a1; M(i, c + 2) = a2;
+  }
+}
+template <class X>
 QZ_HD void par_neg_row(X& x, MatV M, int r, int c_lo, int c_hi) {
   for (int j = c_lo + x.tid; j < c_hi; j += x.nt) M(r, j) = -M(r, j);
 }
@@ -201,25 +217,25 @@ QZ_HD void cta_ds_sweep(X& x, WinState& w, int f, int l, double c2, double c1, d
       } else {
         a0 = w.H(j, j - 1); a1 = w.H(j + 1, j - 1); a2 = w.H(j + 2, j - 1);
       }
-      double tau, v1 = a1, v2 = a2, beta = a0;
-      larfg3(beta, v1, v2, tau);
+      House3 PL, PR;
+      double beta;
+      house3(a0, a1, a2, PL, beta);
       double tb[9];
       for (int cc = 0; cc < 3; ++cc)
         for (int rr = 0; rr < 3; ++rr) tb[rr + 3 * cc] = w.T(j + rr, j + cc);
-      for (int cc = 0; cc < 3; ++cc) refl3(tau, v1, v2, tb[3 * cc], tb[3 * cc + 1], tb[3 * cc + 2]);
-      double taur, u1, u2;
-      opposite_reflector3(tb, taur, u1, u2);
-      for (int rr = 0; rr < 3; ++rr) refl3(taur, u1, u2, tb[rr], tb[rr + 3], tb[rr + 6]);
+      for (int cc = 0; cc < 3; ++cc) house3_apply(PL, tb[3 * cc], tb[3 * cc + 1], tb[3 * cc + 2]);
+      opposite_house3(tb, PR);
+      for (int rr = 0; rr < 3; ++rr) house3_apply(PR, tb[rr], tb[rr + 3], tb[rr + 6]);
       tb[1] = 0.0; tb[2] = 0.0;
       x.sync();  // everyone has read H(.,j-1) and the T block
-      par_refl_rows(x, w.H, j, tau, v1, v2, j, n);
-      par_refl_rows(x, w.T, j, tau, v1, v2, j + 3, n);
-      if (w.wantq) par_refl_cols(x, w.Q, j, tau, v1, v2, 0, n);
+      par_house_rows(x, w.H, j, PL, j, n);
+      par_house_rows(x, w.T, j, PL, j + 3, n);
+      if (w.wantq) par_house_cols(x, w.Q, j, PL, 0, n);
       x.sync();
       int hr = (j + 4 < l + 1) ? j + 4 : l + 1;
-      par_refl_cols(x, w.H, j, taur, u1, u2, 0, hr);
-      par_refl_cols(x, w.T, j, taur, u1, u2, 0, j);
-      if (w.wantz) par_refl_cols(x, w.Z, j, taur, u1, u2, 0, n);
+      par_house_cols(x, w.H, j, PR, 0, hr);
+      par_house_cols(x, w.T, j, PR, 0, j);
+      if (w.wantz) par_house_cols(x, w.Z, j, PR, 0, n);
       if (x.tid == 0) {
         for (int cc = 0; cc < 3; ++cc)
           for (int rr = 0; rr < 3; ++rr) w.T(j + rr, j + cc) = tb[rr + 3 * cc];
@@ -615,7 +631,13 @@ QZ_HD void cta_aed(X& x, WinState& w, double s, double* sr, double* si_, double*
   int info = cta_small_qz(x, w, maxit);
   x.stamp(1);
   if (info != 0) {
-    if (x.tid == 0) { x.si[8] = n; x.si[9] = info; x.si[10] = 0; }
+    // window QZ did not converge: deflate nothing, hand the diagonal
+    // ratios of the (equivalent) partly reduced window over as shifts
+    // (qzearly.f:237-248); the caller discards the window itself
+    if (x.tid == 0) {
+      for (int i = 0; i < n; ++i) { sr[i] = w.H(i, i); si_[i] = 0.0; sb[i] = w.T(i, i); }
+      x.si[8] = n; x.si[9] = info; x.si[10] = 0;
+    }
     x.sync();
     return;
   }

@@ -141,6 +141,67 @@ QZ_HD void opposite_reflector3(const double* m_in, double& tau, double& v1, doub
   larfg3(a, v1, v2, tau);
 }
 
+// Householder reflector in unnormalised form, P = I - s*u*u^T with
+// P*x = beta*e1: u = x - beta*e1, s = 2/(u^T u).  P is orthogonal to
+// rounding whatever the accuracy of beta, because s is formed from the
+// stored u.  One square root and one division.
+struct House3 {
+  double s, u0, u1, u2;
+};
+QZ_HD void house3(double x0, double x1, double x2, House3& h, double& beta) {
+  if (x1 == 0.0 && x2 == 0.0) {
+    h.s = 0.0; h.u0 = 1.0; h.u1 = 0.0; h.u2 = 0.0;
+    beta = x0;
+    return;
+  }
+  double m = dmax(fabs(x0), dmax(fabs(x1), fabs(x2)));
+  double nrm;
+  if (m > kSafeLo && m < kSafeHi) {
+    nrm = sqrt(x0 * x0 + x1 * x1 + x2 * x2);
+  } else {
+    double a = x0 / m, b = x1 / m, c = x2 / m;
+    nrm = sqrt(a * a + b * b + c * c) * m;
+  }
+  beta = -dsign(nrm, x0);
+  h.u0 = x0 - beta;
+  h.u1 = x1;
+  h.u2 = x2;
+  double uu = h.u0 * h.u0 + x1 * x1 + x2 * x2;
+  h.s = 2.0 / uu;
+}
+QZ_HD void house3_apply(const House3& h, double& a0, double& a1, double& a2) {
+  double t = h.s * (h.u0 * a0 + h.u1 * a1 + h.u2 * a2);
+  a0 -= t * h.u0;
+  a1 -= t * h.u1;
+  a2 -= t * h.u2;
+}
+
+// Opposite reflector in unnormalised form: (M*P) e1 = gamma*e1.  The
+// direction P e1 spans the null space of rows 1 and 2 of M, i.e. their
+// cross product, which costs no square root or division.  Its rounding
+// error grows like 1/sin(angle between the rows); when sin < 0.1 the
+// direction comes from the RQ factorisation by Givens rotations instead
+// (opposite_reflector3), which is backward stable for any block.
+QZ_HD void opposite_house3(const double* m, House3& h) {
+  double r10 = m[1], r11 = m[4], r12 = m[7];
+  double r20 = m[2], r21 = m[5], r22 = m[8];
+  double w0 = r11 * r22 - r12 * r21;
+  double w1 = r12 * r20 - r10 * r22;
+  double w2 = r10 * r21 - r11 * r20;
+  double ww = w0 * w0 + w1 * w1 + w2 * w2;
+  double n1 = r10 * r10 + r11 * r11 + r12 * r12;
+  double n2 = r20 * r20 + r21 * r21 + r22 * r22;
+  double beta;
+  if (ww >= 0.01 * n1 * n2 && ww > 0.0 && isfinite(ww) && n1 * n2 < 1e280 && n1 * n2 > 1e-280) {
+    house3(w0, w1, w2, h, beta);
+  } else {
+    double tau, v1, v2;
+    opposite_reflector3(m, tau, v1, v2);
+    // I - tau*v*v^T with v = [1, v1, v2] is I - s*u*u^T with u = v, s = tau
+    h.s = tau; h.u0 = 1.0; h.u1 = v1; h.u2 = v2;
+  }
+}
+
 // Opposite rotation for a 2x2 block: a column rotation (c, s) on columns
 // (0,1) that zeros m(1,0): new col0 = c*col0 + s*col1 ... expressed in the
 // global convention (x, y) -> (c*x + s*y, -s*x + c*y) on (col0, col1).
@@ -164,20 +225,16 @@ QZ_HD void shift_column(double h11, double h21, double h12, double h22, double h
                         double t11, double t12, double t22,
                         double c2, double c1, double c0,
                         double& v0, double& v1, double& v2) {
-  // y = M e1 = H T^{-1} e1 = (h11, h21) / t11
-  double y0 = h11 / t11, y1 = h21 / t11;
-  // z = T^{-1} y (2x2 upper triangular)
-  double z1 = y1 / t22;
-  double z0 = (y0 - t12 * z1) / t11;
-  // M^2 e1 = H z
-  double w0 = h11 * z0 + h12 * z1;
-  double w1 = h21 * z0 + h22 * z1;
-  double w2 = h32 * z1;
-  v0 = c2 * w0 - c1 * y0 + c0;
-  v1 = c2 * w1 - c1 * y1;
-  v2 = c2 * w2;
+  // p(M) e1 multiplied by t11^2 * t22 (M = H T^{-1}): no division, so a
+  // tiny T diagonal entry (a nearly infinite eigenvalue) cannot overflow
+  double g = h11 * t22 - t12 * h21;
+  v0 = c2 * (h11 * g + h12 * h21 * t11) - c1 * h11 * t11 * t22 + c0 * t11 * t11 * t22;
+  v1 = c2 * (h21 * g + h22 * h21 * t11) - c1 * h21 * t11 * t22;
+  v2 = c2 * h32 * h21 * t11;
   double m = dmax(fabs(v0), dmax(fabs(v1), fabs(v2)));
   if (m > 0.0 && isfinite(m)) { v0 /= m; v1 /= m; v2 /= m; }
+  // the scaling by t11^2*t22 may flip the sign of the vector; the
+  // reflector built from it is the same
 }
 
 // Eigenvalues of a 2x2 pencil (A, B), B upper triangular (b10 = 0), as

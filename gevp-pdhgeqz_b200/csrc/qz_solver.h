@@ -32,6 +32,7 @@ struct SolveParams {
   int verbose = 0;       // progress lines on stderr (B200QZ_VERBOSE=1)
   int aed_nskip = 0;     // AED spike test stops after this many consecutive
                          // undeflatable blocks (0: test the whole window)
+  int max_wave = 8;      // chains chased concurrently (one CTA each)
 };
 
 struct SolveStats {
@@ -40,6 +41,7 @@ struct SolveStats {
   double upd_flops = 0.0;  // FP64-equivalent flops of the off-diagonal updates
   double win_bytes = 0.0;  // algorithmic bytes of window kernels (load+store)
   int64_t launches = 0;    // kernel launches issued by the solve
+  int64_t aed_fail = 0;    // AED windows whose small QZ did not converge
 };
 
 // reference shift-count table (piparmq.f:504-533)
@@ -103,11 +105,69 @@ inline void pair_shifts(const double* sr, const double* si, const double* sb, in
   }
 }
 
+// One chase window of one chain.
+struct WinPlan {
+  int w, wk, last, tmax, nb;
+  std::vector<Bulge> bl;
+};
+struct ChainPlan {
+  std::vector<WinPlan> wins;
+};
+
+// Window sequence of one chain of nb bulges over the active block
+// [ktop, kbot] (the PDHGEQZ5 schedule with windows of size W): the first
+// window introduces the bulges at ktop, the following ones start one row
+// above the topmost bulge, the last one pushes every bulge off at kbot.
+// Every window advances the chain by exactly adv rows (adv must not exceed
+// W - 4 - 3*(nb-1), the most a chain of nb bulges can move), so chains of
+// different lengths launched with the same lag never catch up.
+inline void plan_chain(int ktop, int kbot, int W, int nb, const ShiftPair* sp, int adv, ChainPlan& cp) {
+  std::vector<int> pos(nb);
+  bool first = true;
+  while (true) {
+    WinPlan wp;
+    wp.w = first ? ktop : pos[nb - 1] - 1;
+    wp.wk = std::min(W, kbot - wp.w + 1);
+    bool fin = (wp.w + wp.wk - 1 >= kbot);
+    wp.last = fin ? (kbot - wp.w) : (wp.wk - 1);
+    wp.nb = nb;
+    wp.bl.resize(nb);
+    wp.tmax = 0;
+    for (int k = 0; k < nb; ++k) {
+      Bulge& g = wp.bl[k];
+      g.c2 = sp[k].c2; g.c1 = sp[k].c1; g.c0 = sp[k].c0;
+      if (first) {
+        g.base = -3 * k;
+        g.tlo = 3 * k;
+        g.intro = 1;
+      } else {
+        g.base = pos[k] - wp.w;
+        g.tlo = 0;
+        g.intro = 0;
+      }
+      if (fin) {
+        // push-off: each bulge ends with its 2x2 step at row kbot-1
+        g.thi = (kbot - wp.w) - g.base;
+      } else {
+        // lockstep: every bulge moves adv rows; in the first window bulge
+        // k starts at step 3k, so the topmost one also advances adv
+        g.thi = first ? (adv + 3 * nb - 2) : adv;
+      }
+      wp.tmax = std::max(wp.tmax, g.thi);
+    }
+    for (int k = 0; k < nb; ++k) pos[k] = wp.w + wp.bl[k].base + wp.bl[k].thi;
+    cp.wins.push_back(std::move(wp));
+    if (fin) break;
+    first = false;
+  }
+}
+
 // Backend interface (implemented by the GPU backend):
 //   void scan(int ifirst, int kbot, int* out4)          // ktop, ninf, jmax, jmin
 //   void aed(int ktop, int kwtop, int kbot, int* info3, double* shifts) // m, status, transformed
-//   void update(int w, int wk, int which)               // which 0: AED factors, 1: chase U,V
-//   void chase(int w, int wk, int last, const Bulge* bl, int nb, int tmax)
+//   void update(int w, int wk, int which)               // which 0: AED factors, 1: zero-chase U,V
+//   void chase_wave(const WinPlan* const* wins, int n)  // one CTA per window
+//   void update_wave(const WinPlan* const* wins, int n) // far updates of those windows
 //   void inf_window(int w, int wk, int top, int jz, int stop, bool deflate)
 //   void inf_top(int ktop)
 template <class BK>
@@ -117,7 +177,7 @@ int qz_iterate(BK& bk, int n, int ilo, int ihi, const SolveParams& P, SolveStats
   int64_t maxit = (int64_t)P.maxit_factor * std::max(1, nh0);
   std::vector<double> sh(3 * std::max(P.nw_max, P.nmin) + 8);
   std::vector<ShiftPair> pairs;
-  std::vector<Bulge> bl;
+  std::vector<const WinPlan*> wave;
   int scan_out[4];
   int info3[3];
   for (int64_t it = 0; it < maxit; ++it) {
@@ -180,12 +240,15 @@ int qz_iterate(BK& bk, int n, int ilo, int ihi, const SolveParams& P, SolveStats
       nd = nw - m;
       bk.update(kwtop, nw, 0);
     }
-    if (info3[1] != 0) m = 0;  // failed window QZ: no deflation, no shifts
+    // a failed window QZ deflates nothing but still supplies shifts (the
+    // diagonal ratios of the window), so the sweep changes the pencil and
+    // the next AED sees a different window (PDHGEQZ0.f:944-949)
+    if (info3[1] != 0) ++S.aed_fail;
     S.aed_defl += nd;
     kbot -= nd;
     if (kbot < ktop) continue;
     int nib = (P.nibble >= 0) ? P.nibble : nibble_table(nh);
-    if (100 * nd > nib * nw) continue;
+    if (info3[1] == 0 && 100 * nd > nib * nw) continue;
     // ---- multishift sweep ----
     int nsmax = (P.ns_max > 0) ? P.ns_max : ns_table(nh);
     int ns = std::min(nsmax, m - (m % 2));
@@ -199,53 +262,41 @@ int qz_iterate(BK& bk, int n, int ilo, int ihi, const SolveParams& P, SolveStats
     S.shifts += 2 * npairs;
     int W = P.w_chase;
     int cmax = (P.chain_max > 0) ? P.chain_max : std::max(1, (W - 4) / 6);
+    cmax = std::min(cmax, std::max(1, (W - 4) / 3 - 1));
+    // ---- plan every chain's windows (positions do not depend on data) ----
+    int nbig = std::min(cmax, npairs);
+    int adv = W - 4 - 3 * (nbig - 1);  // common advance per window
+    std::vector<ChainPlan> plans;
     for (int p0 = 0; p0 < npairs; p0 += cmax) {
+      ChainPlan cp;
       int nb = std::min(cmax, npairs - p0);
+      plan_chain(ktop, kbot, W, nb, pairs.data() + p0, adv, cp);
+      plans.push_back(std::move(cp));
       ++S.chains;
-      // next-step positions (global) of each bulge; bulge 0 is the deepest
-      std::vector<int> pos(nb);
-      bool first = true;
-      while (true) {
-        int w, wk;
-        if (first) {
-          w = ktop;
-        } else {
-          w = pos[nb - 1] - 1;
+    }
+    // ---- waves: chain c trails chain c-1 by lag windows with
+    // lag*adv >= W, so the windows of one wave are disjoint; the far
+    // updates of a wave run as one left batch then one right batch, and
+    // a left update of one window only meets a right update of another
+    // (commuting transformations, never in the same launch) ----
+    const int lag = (W + adv - 1) / adv;
+    const int G = std::max(1, std::min(P.max_wave, (int)plans.size()));
+    for (size_t g0 = 0; g0 < plans.size(); g0 += G) {
+      size_t g1 = std::min(plans.size(), g0 + G);
+      int tmax_wave = 0;
+      for (size_t c = g0; c < g1; ++c)
+        tmax_wave = std::max(tmax_wave, (int)(lag * (c - g0)) + (int)plans[c].wins.size());
+      for (int t = 0; t < tmax_wave; ++t) {
+        wave.clear();
+        for (size_t c = g0; c < g1; ++c) {
+          int i = t - lag * (int)(c - g0);
+          if (i < 0 || i >= (int)plans[c].wins.size()) continue;
+          wave.push_back(&plans[c].wins[i]);
         }
-        wk = std::min(W, kbot - w + 1);
-        bool fin = (w + wk - 1 >= kbot);
-        int last = fin ? (kbot - w) : (wk - 1);
-        bl.resize(nb);
-        int tmax = 0;
-        for (int k = 0; k < nb; ++k) {
-          Bulge& g = bl[k];
-          const ShiftPair& sp = pairs[p0 + k];
-          g.c2 = sp.c2; g.c1 = sp.c1; g.c0 = sp.c0;
-          if (first) {
-            g.base = -3 * k;
-            g.tlo = 3 * k;
-            g.intro = 1;
-          } else {
-            g.base = pos[k] - w;
-            g.tlo = 0;
-            g.intro = 0;
-          }
-          if (fin) {
-            // push-off: each bulge ends with its 2x2 step at row kbot-1
-            g.thi = (kbot - w) - g.base;
-          } else {
-            // lockstep: every bulge moves as far as the deepest one can
-            // (its last 3x3 step at window row wk-4)
-            g.thi = first ? (wk - 3) : (wk - 3 - (pos[0] - w));
-          }
-          tmax = std::max(tmax, g.thi);
-        }
-        bk.chase(w, wk, last, bl.data(), nb, tmax);
-        bk.update(w, wk, 1);
-        ++S.windows;
-        if (fin) break;
-        for (int k = 0; k < nb; ++k) pos[k] = w + bl[k].base + bl[k].thi;
-        first = false;
+        if (wave.empty()) continue;
+        bk.chase_wave(wave.data(), (int)wave.size());
+        bk.update_wave(wave.data(), (int)wave.size());
+        S.windows += (int64_t)wave.size();
       }
     }
   }

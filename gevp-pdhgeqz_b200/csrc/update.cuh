@@ -25,14 +25,16 @@ struct UpdJob {
   int len;         // slab extent along the non-k direction (L)
   const double* W; // k x k factor (column-major, ld = ldw)
   int ldw;
+  int k;           // window size of this job
   int tiles;       // number of 32-wide tiles of this job
 };
 
-constexpr int kUpdMaxJobs = 4;
+// one launch updates the slabs of several windows (a wave of chains)
+constexpr int kUpdMaxJobs = 32;
 struct UpdBatch {
   UpdJob job[kUpdMaxJobs];
   int njobs;
-  int k;           // window size (all jobs share it)
+  int k;           // largest window size in the batch (sizes shared memory)
 };
 
 constexpr int kUpdTile = 32;       // slab tile width (columns for left, rows for right)
@@ -67,7 +69,7 @@ __global__ void __launch_bounds__(kUpdThreads) k_update_left(UpdBatch B) {
   int jb = upd_find_job(B, tile);
   if (jb < 0) return;
   const UpdJob J = B.job[jb];
-  const int k = B.k;
+  const int k = J.k;
   const int kp = (k + 15) & ~15;
   const int ldw = kp + 4;
   const int ldx = 36;
@@ -134,7 +136,7 @@ __global__ void __launch_bounds__(kUpdThreads) k_update_right(UpdBatch B) {
   int jb = upd_find_job(B, tile);
   if (jb < 0) return;
   const UpdJob J = B.job[jb];
-  const int k = B.k;
+  const int k = J.k;
   const int kp = (k + 15) & ~15;
   const int ldw = kp + 4;
   const int ldx = kp + 4;
@@ -199,7 +201,7 @@ __global__ void __launch_bounds__(256) k_update_left_gen(UpdBatch B) {
   int jb = upd_find_job(B, tile);
   if (jb < 0) return;
   const UpdJob J = B.job[jb];
-  const int k = B.k;
+  const int k = J.k;
   const int c0 = J.c0 + tile * kUpdGenTile;
   const int ncol = min(kUpdGenTile, J.c0 + J.len - c0);
   double* Xs = smem;  // k x 8
@@ -222,7 +224,7 @@ __global__ void __launch_bounds__(256) k_update_right_gen(UpdBatch B) {
   int jb = upd_find_job(B, tile);
   if (jb < 0) return;
   const UpdJob J = B.job[jb];
-  const int k = B.k;
+  const int k = J.k;
   const int r0 = J.r0 + tile * kUpdGenTile;
   const int nrow = min(kUpdGenTile, J.r0 + J.len - r0);
   double* Xs = smem;  // 8 x k

@@ -86,7 +86,8 @@ int b200qz_solve_host(b200qz_ctx* ctx, char job, char compq, char compz, int n, 
  * 16 chase updates, 17 infinite-eigenvalue deflation, 18 finalisation,
  * and inside the AED kernel 19 small QZ, 20 reordering, 21 spike
  * reflector + RQ update, 22 Hessenberg-triangular re-reduction;
- * 23 kernel launches issued by the solve.
+ * 23 kernel launches issued by the solve, 24 AED windows whose small QZ
+ * did not converge (they deflate nothing and supply diagonal shifts).
  * Returns the number of values written. */
 int b200qz_get_stats(const b200qz_ctx* ctx, double* out, int nout);
 
@@ -99,8 +100,8 @@ int b200qz_set_params(b200qz_ctx* ctx, int nw_max, int w_chase, int nmin, int ni
 /* Set one tunable by name: "nw_max", "w_chase", "nmin", "nibble",
  * "ns_max", "maxit_factor", "chain_max" (bulges per chain), "aed_nskip"
  * (AED spike test stops after this many consecutive undeflatable blocks,
- * 0 = whole window).  Returns 0, -2 for an unknown name, -3 for a value
- * out of range. */
+ * 0 = whole window), "max_wave" (chains chased concurrently, 1..8).
+ * Returns 0, -2 for an unknown name, -3 for a value out of range. */
 int b200qz_set_param(b200qz_ctx* ctx, const char* name, double value);
 
 /* ------------------------------------------------------------------ */
