@@ -55,14 +55,15 @@ _c = ctypes.c_char
 EXPORTS = (
     "pdhgeqz_", "kkqzconf_", "b200qz_create", "b200qz_destroy", "b200qz_solve_dev",
     "b200qz_solve_host", "b200qz_get_stats", "b200qz_set_params", "b200qz_aed_window",
-    "b200qz_chase_window", "b200qz_update", "b200qz_set_param",
+    "b200qz_chase_window", "b200qz_update", "b200qz_set_param", "b200qz_solve_batched_dev",
+    "b200qz_batched_seconds", "b200qz_batched_autotune", "b200qz_batched_config",
 )
 
 STAT_NAMES = ("seconds", "iters", "aeds", "aed_deflations", "sweeps", "chains", "windows",
               "endgames", "inf_steps", "shifts", "update_flops", "window_bytes",
               "ms_scan", "ms_aed", "ms_aed_update", "ms_chase", "ms_chase_update", "ms_inf", "ms_final",
               "ms_aed_smallqz", "ms_aed_reorder", "ms_aed_spike", "ms_aed_hessred", "launches",
-              "aed_failures")
+              "aed_failures", "exceptional_sweeps")
 
 
 def lib() -> ctypes.CDLL:
@@ -102,6 +103,15 @@ def lib() -> ctypes.CDLL:
     L.b200qz_set_param.argtypes = [_vp, ctypes.c_char_p, _d]
     L.b200qz_update.restype = _i
     L.b200qz_update.argtypes = [_vp, _c, _vp, _i, _i, _i, _i, _vp, _i, _i]
+    _pl = ctypes.POINTER(ctypes.c_longlong)
+    L.b200qz_solve_batched_dev.argtypes = [_vp, _i, _pi, _pl, _pl] + [_vp] * 8
+    L.b200qz_solve_batched_dev.restype = _i
+    L.b200qz_batched_seconds.argtypes = [_vp]
+    L.b200qz_batched_seconds.restype = _d
+    L.b200qz_batched_autotune.argtypes = [_vp, _i, _pi, _pl, _vp, _vp, _i, _pd]
+    L.b200qz_batched_autotune.restype = _i
+    L.b200qz_batched_config.argtypes = [_vp, _pi, _pi, _pi]
+    L.b200qz_batched_config.restype = _i
     _lib = L
     return L
 
@@ -230,6 +240,68 @@ class Solver:
                                        _p(H), H.shape[0], _p(T), T.shape[0], _p(Qa), Qa.shape[0], _p(Za),
                                        Za.shape[0], _p(ar), _p(ai), _p(be))
         return ar, ai, be, info
+
+
+class Batch:
+    """Layout of a batch of independent pencils of uneven sizes packed in
+    one device buffer: pencil ``p`` (order ``n[p]``, column-major, leading
+    dimension ``n[p]``) starts at double offset ``moff[p]``; its eigenvalues
+    start at ``eoff[p]``."""
+
+    def __init__(self, sizes):
+        self.n = np.ascontiguousarray(sizes, dtype=np.int32)
+        sq = self.n.astype(np.int64) ** 2
+        self.moff = np.zeros(len(self.n), dtype=np.int64)
+        self.eoff = np.zeros(len(self.n), dtype=np.int64)
+        if len(self.n):
+            self.moff[1:] = np.cumsum(sq)[:-1]
+            self.eoff[1:] = np.cumsum(self.n.astype(np.int64))[:-1]
+        self.count = len(self.n)
+        self.elems = int(sq.sum())
+        self.neig = int(self.n.sum())
+
+    def pack(self, mats):
+        out = np.empty(self.elems)
+        for p, M in enumerate(mats):
+            out[self.moff[p]:self.moff[p] + M.size] = np.asarray(M, dtype=np.float64).ravel(order="F")
+        return out
+
+    def unpack(self, flat, p):
+        n = int(self.n[p])
+        return flat[self.moff[p]:self.moff[p] + n * n].reshape((n, n), order="F")
+
+
+def _batch_args(b: "Batch"):
+    _pl = ctypes.POINTER(ctypes.c_longlong)
+    return (b.n.ctypes.data_as(_pi), b.moff.ctypes.data_as(_pl), b.eoff.ctypes.data_as(_pl))
+
+
+def solve_batched_device(solver: "Solver", b: "Batch", h_ptr, t_ptr, q_ptr, z_ptr, ar_ptr, ai_ptr, be_ptr,
+                         info_ptr) -> float:
+    """Reduce every pencil of the batch to generalized Schur form with Q, Z
+    (device buffers given as integer pointers).  Returns device seconds;
+    per-pencil INFO goes to ``info_ptr`` (int32, device)."""
+    n, mo, eo = _batch_args(b)
+    rc = lib().b200qz_solve_batched_dev(solver.handle, b.count, n, mo, eo, _vp(h_ptr), _vp(t_ptr), _vp(q_ptr),
+                                        _vp(z_ptr), _vp(ar_ptr), _vp(ai_ptr), _vp(be_ptr), _vp(info_ptr))
+    if rc != 0:
+        raise RuntimeError("b200qz_solve_batched_dev failed: %d" % rc)
+    return lib().b200qz_batched_seconds(solver.handle)
+
+
+def autotune_batched(solver: "Solver", b: "Batch", h_ptr, t_ptr, sample=256):
+    """Pick threads per CTA, shared-memory cutoff and CTAs per SM for this
+    batch on a copy of ``sample`` of its pencils.  Returns
+    (threads, smem_max, ctas_per_sm, best_seconds)."""
+    n, mo, _ = _batch_args(b)
+    best = ctypes.c_double(0.0)
+    rc = lib().b200qz_batched_autotune(solver.handle, b.count, n, mo, _vp(h_ptr), _vp(t_ptr), sample,
+                                       ctypes.byref(best))
+    if rc != 0:
+        raise RuntimeError("b200qz_batched_autotune failed: %d" % rc)
+    th, sm, cps = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    lib().b200qz_batched_config(solver.handle, ctypes.byref(th), ctypes.byref(sm), ctypes.byref(cps))
+    return th.value, sm.value, cps.value, best.value
 
 
 def solve(H, T, job="S", compq="I", compz="I", device=0):

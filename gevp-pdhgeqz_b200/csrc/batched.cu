@@ -1,0 +1,155 @@
+// Batched QZ of many independent small pencils of uneven sizes.
+//
+// Role in the reference: none directly (PDHGEQZ solves one pencil); this is
+// the batched workload of the measurement plan, built from the same
+// CTA-level kernels as the endgame (PDHGEQZ4 -> KKQZ): every pencil is
+// reduced to generalized Schur form with Q and Z by one CTA.
+//
+// One persistent launch: CTAs pull pencils from an atomic queue ordered by
+// decreasing size (longest-first scheduling), solve a pencil in shared
+// memory when n <= kBatchSmemMax (H, T, Q, Z with an odd leading
+// dimension), in place in global memory otherwise, normalise beta >= 0 and
+// write the eigenvalues.  Per-pencil status words; no host round trip.
+#include <cuda_runtime.h>
+#include <float.h>
+#include <stdint.h>
+
+#include "kernels.h"
+#include "qz_cta.cuh"
+
+namespace qz {
+
+namespace {
+
+struct BExec {
+  int tid, nt;
+  int* si;
+  double* sd;
+  __device__ void sync() { __syncthreads(); }
+  __device__ void stamp(int) {}
+};
+
+__device__ __forceinline__ double block_sum(double v, double* red) {
+  for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) red[wid] = v;
+  __syncthreads();
+  double t = 0.0;
+  if (threadIdx.x == 0)
+    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) t += red[i];
+  __syncthreads();
+  if (threadIdx.x == 0) red[0] = t;
+  __syncthreads();
+  return red[0];
+}
+
+}  // namespace
+
+__global__ void __launch_bounds__(kBatchThreads) k_batch_qz(int count, const int* __restrict__ order,
+                                                            const int* __restrict__ nsz,
+                                                            const int64_t* __restrict__ moff,
+                                                            const int64_t* __restrict__ eoff, double* H, double* T,
+                                                            double* Q, double* Z, double* AR, double* AI, double* BE,
+                                                            int* status, int* counter, int smem_max) {
+  extern __shared__ double smem[];
+  __shared__ int s_next;
+  __shared__ double red[32];
+  __shared__ int si[64];
+  __shared__ double sd_small[64];
+  for (;;) {
+    if (threadIdx.x == 0) s_next = atomicAdd(counter, 1);
+    __syncthreads();
+    const int idx = s_next;
+    __syncthreads();
+    if (idx >= count) break;
+    const int p = order[idx];
+    const int n = nsz[p];
+    double* Hg = H + moff[p];
+    double* Tg = T + moff[p];
+    double* Qg = Q + moff[p];
+    double* Zg = Z + moff[p];
+    // tolerances of this pencil (PDHGEQZ.f:449-458)
+    double hs = 0.0, ts = 0.0;
+    for (int k = threadIdx.x; k < n * n; k += blockDim.x) {
+      hs += Hg[k] * Hg[k];
+      ts += Tg[k] * Tg[k];
+    }
+    hs = block_sum(hs, red);
+    ts = block_sum(ts, red);
+    Tol tol;
+    tol.safmin = DBL_MIN;
+    tol.ulp = DBL_EPSILON;
+    tol.smlnum = DBL_MIN * ((double)n / DBL_EPSILON);
+    tol.htol = fmax(DBL_MIN, DBL_EPSILON * sqrt(hs));
+    tol.ttol = fmax(DBL_MIN, DBL_EPSILON * sqrt(ts));
+    const bool in_smem = n <= smem_max;
+    const int lw = in_smem ? smem_ld(n) : n;
+    double *Hs, *Ts, *Qs, *Zs;
+    if (in_smem) {
+      Hs = smem;
+      Ts = Hs + n * lw;
+      Qs = Ts + n * lw;
+      Zs = Qs + n * lw;
+      for (int k = threadIdx.x; k < n * n; k += blockDim.x) {
+        int i = k % n, j = k / n;
+        Hs[i + j * lw] = Hg[k];
+        Ts[i + j * lw] = Tg[k];
+        Qs[i + j * lw] = (i == j) ? 1.0 : 0.0;
+        Zs[i + j * lw] = (i == j) ? 1.0 : 0.0;
+      }
+    } else {
+      Hs = Hg;
+      Ts = Tg;
+      Qs = Qg;
+      Zs = Zg;
+      for (int k = threadIdx.x; k < n * n; k += blockDim.x) {
+        int i = k % n, j = k / n;
+        Qs[k] = (i == j) ? 1.0 : 0.0;
+        Zs[k] = (i == j) ? 1.0 : 0.0;
+      }
+    }
+    __syncthreads();
+    BExec x{(int)threadIdx.x, (int)blockDim.x, si, sd_small};
+    WinState w;
+    w.n = n;
+    w.H = MatV{Hs, lw};
+    w.T = MatV{Ts, lw};
+    w.Q = MatV{Qs, lw};
+    w.Z = MatV{Zs, lw};
+    w.wantq = true;
+    w.wantz = true;
+    w.tol = tol;
+    int info = cta_small_qz(x, w, 30 * n);
+    __syncthreads();
+    if (info == 0) cta_finalize(x, w, AR + eoff[p], AI + eoff[p], BE + eoff[p]);
+    if (in_smem) {
+      for (int k = threadIdx.x; k < n * n; k += blockDim.x) {
+        int i = k % n, j = k / n;
+        Hg[k] = Hs[i + j * lw];
+        Tg[k] = Ts[i + j * lw];
+        Qg[k] = Qs[i + j * lw];
+        Zg[k] = Zs[i + j * lw];
+      }
+    }
+    if (threadIdx.x == 0) status[p] = info;
+    __syncthreads();
+  }
+}
+
+size_t batch_smem_bytes(int smem_max) { return (size_t)4 * smem_max * smem_ld(smem_max) * sizeof(double); }
+
+cudaError_t batch_init() {
+  return cudaFuncSetAttribute(k_batch_qz, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)batch_smem_bytes(kBatchSmemMax));
+}
+
+void launch_batch(cudaStream_t st, int grid, int threads, int smem_max, int count, const int* order, const int* nsz,
+                  const int64_t* moff, const int64_t* eoff, double* H, double* T, double* Q, double* Z, double* AR,
+                  double* AI, double* BE, int* status, int* counter) {
+  cudaMemsetAsync(counter, 0, sizeof(int), st);
+  k_batch_qz<<<grid, threads, batch_smem_bytes(smem_max), st>>>(count, order, nsz, moff, eoff, H, T, Q, Z, AR, AI, BE,
+                                                                status, counter, smem_max);
+}
+
+}  // namespace qz

@@ -12,6 +12,7 @@
 #include <mutex>
 #include <string>
 #include <vector>
+#include <functional>
 
 #include "../../include/b200qz.h"
 #include "kernels.h"
@@ -79,7 +80,7 @@ struct b200qz_ctx {
   double* shifts = nullptr;    // 3*kAedMax
   double* gscratch = nullptr;  // 2*kAedMax^2 (windows above the smem limit)
   double* norms = nullptr;     // 2
-  int* dinfo = nullptr;        // 8 ints
+  int* dinfo = nullptr;        // 16 ints: [4..6] AED info, [8..12] scan output
   int* hinfo = nullptr;        // pinned mirror
   double* hshifts = nullptr;   // pinned 3*kAedMax
   double* hnorms = nullptr;    // pinned 2
@@ -94,6 +95,15 @@ struct b200qz_ctx {
   unsigned long long* dts = nullptr;  // AED phase timestamps (device)
   double* dbuf = nullptr;             // cached device copy of H, T, Q, Z, eigenvalues (host entry)
   size_t dbuf_bytes = 0;
+  // batched solver
+  int* bdesc = nullptr;                // device: order, n, counter, moff/eoff (int64) packed
+  size_t bdesc_bytes = 0;
+  int batch_threads = 128, batch_smem_max = kBatchSmemMax, batch_ctas_per_sm = 1;
+  cudaGraph_t bgraph = nullptr;
+  cudaGraphExec_t bexec = nullptr;
+  size_t bkey = 0;                     // hash of the captured batch layout
+  int sm_count = 148;
+  double batch_seconds = 0.0;
   unsigned long long* hts = nullptr;  // pinned mirror
   double aed_ms[4] = {0, 0, 0, 0};   // small QZ, reorder, spike+RQ, HT re-reduction
 };
@@ -119,13 +129,13 @@ struct GpuBackend {
 
   void scan(int ifirst, int kbot, int* out) {
     c->timer.begin(kPhScan, c->stream);
-    launch_scan(c->stream, H, T, ld, ifirst, kbot, tol, c->dinfo);
+    launch_scan(c->stream, H, T, ld, ifirst, kbot, tol, c->dinfo + 8);
     c->stats.launches += 1;
     c->timer.end(c->stream);
-    QZ_CK(cudaMemcpyAsync(c->hinfo, c->dinfo, 4 * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    QZ_CK(cudaMemcpyAsync(c->hinfo, c->dinfo + 8, 5 * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     QZ_CK(cudaStreamSynchronize(c->stream));
-    if (c->err != cudaSuccess) { out[0] = ifirst; out[1] = 0; out[2] = -1; out[3] = -1; return; }
-    for (int i = 0; i < 4; ++i) out[i] = c->hinfo[i];
+    if (c->err != cudaSuccess) { out[0] = ifirst; out[1] = 0; out[2] = -1; out[3] = -1; out[4] = 1; return; }
+    for (int i = 0; i < 5; ++i) out[i] = c->hinfo[i];
   }
   void aed(int ktop, int kwtop, int kbot, int* info3, double* sh) {
     int nw = kbot - kwtop + 1;
@@ -338,6 +348,7 @@ int solve_dev_impl(b200qz_ctx* c, char job, char compq, char compz, int n, int i
   tol.ttol = std::max(DBL_MIN, DBL_EPSILON * std::sqrt(c->hnorms[1]));
   int info = 0;
   if (nh > 0) info = qz_iterate(bk, n, ilo - 1, ihi - 1, c->params, c->stats);
+  if (info < 0) info = 10002;  // non-finite entries appeared (or were given)
   c->timer.begin(kPhFinal, c->stream);
   launch_finalize(c->stream, h, t, z, ld, n, wantz ? 1 : 0, ar, ai, be);
   c->stats.launches += 2;
@@ -365,6 +376,8 @@ int b200qz_create(b200qz_ctx** out, int device) {
   c->device = device;
   cudaError_t e = cudaSetDevice(device);
   if (e == cudaSuccess) e = kernels_init();
+  if (e == cudaSuccess) e = batch_init();
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
   size_t a2 = (size_t)kAedMax * kAedMax * sizeof(double);
   size_t w2 = (size_t)kMaxWave * kUslot * sizeof(double);
@@ -375,8 +388,8 @@ int b200qz_create(b200qz_ctx** out, int device) {
   if (e == cudaSuccess) e = cudaMalloc(&c->shifts, 3 * kAedMax * sizeof(double));
   if (e == cudaSuccess) e = cudaMalloc(&c->gscratch, 2 * a2);
   if (e == cudaSuccess) e = cudaMalloc(&c->norms, 2 * sizeof(double));
-  if (e == cudaSuccess) e = cudaMalloc(&c->dinfo, 8 * sizeof(int));
-  if (e == cudaSuccess) e = cudaMallocHost(&c->hinfo, 8 * sizeof(int));
+  if (e == cudaSuccess) e = cudaMalloc(&c->dinfo, 16 * sizeof(int));
+  if (e == cudaSuccess) e = cudaMallocHost(&c->hinfo, 16 * sizeof(int));
   if (e == cudaSuccess) e = cudaMallocHost(&c->hshifts, 3 * kAedMax * sizeof(double));
   if (e == cudaSuccess) e = cudaMallocHost(&c->hnorms, 2 * sizeof(double));
   if (e == cudaSuccess) e = cudaMalloc(&c->dts, 8 * sizeof(unsigned long long));
@@ -404,6 +417,9 @@ void b200qz_destroy(b200qz_ctx* c) {
   cudaFree(c->dts);
   if (c->hts) cudaFreeHost(c->hts);
   if (c->dbuf) cudaFree(c->dbuf);
+  if (c->bexec) cudaGraphExecDestroy(c->bexec);
+  if (c->bgraph) cudaGraphDestroy(c->bgraph);
+  if (c->bdesc) cudaFree(c->bdesc);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -441,6 +457,7 @@ int b200qz_set_param(b200qz_ctx* c, const char* name, double value) {
   else if (k == "chain_max") { if (v < 1 || v > kMaxChain) return -3; P.chain_max = v; }
   else if (k == "aed_nskip") { if (v < 0) return -3; P.aed_nskip = v; }
   else if (k == "max_wave") { if (v < 1 || v > kMaxWave) return -3; P.max_wave = v; }
+  else if (k == "stall_limit") { if (v < 1) return -3; P.stall_limit = v; }
   else return -2;
   return 0;
 }
@@ -474,6 +491,9 @@ int b200qz_solve_host(b200qz_ctx* c, char job, char compq, char compz, int n, in
   size_t need = 4 * bytes + 3 * (size_t)n * sizeof(double);
   if (c->dbuf_bytes < need) {
     if (c->dbuf) cudaFree(c->dbuf);
+  if (c->bexec) cudaGraphExecDestroy(c->bexec);
+  if (c->bgraph) cudaGraphDestroy(c->bgraph);
+  if (c->bdesc) cudaFree(c->bdesc);
     c->dbuf = nullptr;
     c->dbuf_bytes = 0;
     QZ_CK(cudaMalloc(&c->dbuf, need));
@@ -515,13 +535,13 @@ int b200qz_get_stats(const b200qz_ctx* c, double* out, int nout) {
   if (!c || !out) return 0;
   const SolveStats& s = c->stats;
   const double* ph = c->timer.ms;
-  double v[25] = {c->seconds, (double)s.iters, (double)s.aeds, (double)s.aed_defl, (double)s.sweeps,
+  double v[26] = {c->seconds, (double)s.iters, (double)s.aeds, (double)s.aed_defl, (double)s.sweeps,
                   (double)s.chains, (double)s.windows, (double)s.endgames, (double)s.infs, (double)s.shifts,
                   s.upd_flops, s.win_bytes,
                   ph[kPhScan], ph[kPhAed], ph[kPhAedUpd], ph[kPhChase], ph[kPhChaseUpd], ph[kPhInf], ph[kPhFinal],
                   c->aed_ms[0], c->aed_ms[1], c->aed_ms[2], c->aed_ms[3], (double)s.launches,
-                  (double)s.aed_fail};
-  int k = std::min(nout, 25);
+                  (double)s.aed_fail, (double)s.exceptional};
+  int k = std::min(nout, 26);
   for (int i = 0; i < k; ++i) out[i] = v[i];
   return k;
 }
@@ -598,6 +618,165 @@ int b200qz_update(b200qz_ctx* c, char side, double* m, int ldm, int r0, int c0, 
   QZ_CK(cudaGetLastError());
   QZ_CK(cudaStreamSynchronize(c->stream));
   return c->err == cudaSuccess ? 0 : 10001;
+}
+
+// ---------------------------------------------------------------------------
+// Batched pencils
+// ---------------------------------------------------------------------------
+namespace {
+
+// order: pencils by decreasing size (longest first on the work queue)
+int batch_prepare(b200qz_ctx* c, int count, const int* n, const long long* moff, const long long* eoff, int** d_order,
+                  int** d_n, int** d_counter, int64_t** d_moff, int64_t** d_eoff) {
+  size_t need = (size_t)count * (2 * sizeof(int) + 2 * sizeof(int64_t)) + 64;
+  if (c->bdesc_bytes < need) {
+    if (c->bdesc) cudaFree(c->bdesc);
+    c->bdesc = nullptr;
+    c->bdesc_bytes = 0;
+    if (cudaMalloc(&c->bdesc, need) != cudaSuccess) return 10001;
+    c->bdesc_bytes = need;
+  }
+  std::vector<int> order(count);
+  for (int i = 0; i < count; ++i) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return n[a] > n[b]; });
+  char* base = (char*)c->bdesc;
+  *d_moff = (int64_t*)base;
+  *d_eoff = (int64_t*)(base + (size_t)count * sizeof(int64_t));
+  *d_order = (int*)(base + 2 * (size_t)count * sizeof(int64_t));
+  *d_n = *d_order + count;
+  *d_counter = *d_n + count;
+  QZ_CK(cudaMemcpyAsync(*d_moff, (const int64_t*)moff, count * sizeof(int64_t), cudaMemcpyHostToDevice, c->stream));
+  QZ_CK(cudaMemcpyAsync(*d_eoff, (const int64_t*)eoff, count * sizeof(int64_t), cudaMemcpyHostToDevice, c->stream));
+  QZ_CK(cudaMemcpyAsync(*d_order, order.data(), count * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+  QZ_CK(cudaMemcpyAsync(*d_n, n, count * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+  QZ_CK(cudaStreamSynchronize(c->stream));
+  return c->err == cudaSuccess ? 0 : 10001;
+}
+
+int batch_grid(const b200qz_ctx* c) { return std::max(1, c->sm_count * c->batch_ctas_per_sm); }
+
+}  // namespace
+
+extern "C" int b200qz_solve_batched_dev(b200qz_ctx* c, int count, const int* n, const long long* moff,
+                                        const long long* eoff, double* h, double* t, double* q, double* z,
+                                        double* alphar, double* alphai, double* beta, int* info) {
+  if (!c) return 10001;
+  if (count < 0) return -2;
+  for (int i = 0; i < count; ++i)
+    if (n[i] < 1 || n[i] > 46340) return -(3 * 1000 + 1);
+  if (count == 0) return 0;
+  c->err = cudaSuccess;
+  QZ_CK(cudaSetDevice(c->device));
+  int *d_order, *d_n, *d_counter;
+  int64_t *d_moff, *d_eoff;
+  if (batch_prepare(c, count, n, moff, eoff, &d_order, &d_n, &d_counter, &d_moff, &d_eoff) != 0) return 10001;
+  // one persistent launch, captured in a CUDA graph and replayed while the
+  // batch layout (pointers, count, configuration) stays the same
+  size_t key = std::hash<const void*>()(h) ^ (std::hash<const void*>()(t) << 1) ^ ((size_t)count << 7) ^
+               ((size_t)c->batch_threads << 3) ^ ((size_t)c->batch_smem_max << 11) ^
+               ((size_t)c->batch_ctas_per_sm << 19) ^ std::hash<const void*>()(info) ^
+               std::hash<const void*>()(alphar);
+  if (!c->bexec || key != c->bkey) {
+    if (c->bexec) { cudaGraphExecDestroy(c->bexec); c->bexec = nullptr; }
+    if (c->bgraph) { cudaGraphDestroy(c->bgraph); c->bgraph = nullptr; }
+    QZ_CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    launch_batch(c->stream, batch_grid(c), c->batch_threads, c->batch_smem_max, count, d_order, d_n, d_moff, d_eoff,
+                 h, t, q, z, alphar, alphai, beta, info, d_counter);
+    QZ_CK(cudaStreamEndCapture(c->stream, &c->bgraph));
+    if (c->err == cudaSuccess) QZ_CK(cudaGraphInstantiate(&c->bexec, c->bgraph, 0));
+    if (c->err != cudaSuccess) return 10001;
+    c->bkey = key;
+  }
+  QZ_CK(cudaEventRecord(c->ev0, c->stream));
+  QZ_CK(cudaGraphLaunch(c->bexec, c->stream));
+  QZ_CK(cudaEventRecord(c->ev1, c->stream));
+  QZ_CK(cudaEventSynchronize(c->ev1));
+  float ms = 0.f;
+  QZ_CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+  c->batch_seconds = ms * 1e-3;
+  return c->err == cudaSuccess ? 0 : 10001;
+}
+
+extern "C" double b200qz_batched_seconds(const b200qz_ctx* c) { return c ? c->batch_seconds : 0.0; }
+
+// Autotuner: time every configuration (threads per CTA, largest pencil kept
+// in shared memory, CTAs per SM) on a copy of a sample of the batch and keep
+// the fastest.  The caller's arrays are not modified.
+extern "C" int b200qz_batched_autotune(b200qz_ctx* c, int count, const int* n, const long long* moff,
+                                       const double* h, const double* t, int sample, double* best_seconds) {
+  if (!c || count <= 0) return -1;
+  c->err = cudaSuccess;
+  QZ_CK(cudaSetDevice(c->device));
+  // deterministic sample spread over the size range
+  int k = std::min(count, std::max(1, sample));
+  std::vector<int> idx(count);
+  for (int i = 0; i < count; ++i) idx[i] = i;
+  std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return n[a] > n[b]; });
+  std::vector<int> pick, sn;
+  std::vector<long long> so, se;
+  int64_t off = 0, eo = 0;
+  for (int j = 0; j < k; ++j) {
+    int p = idx[(int64_t)j * count / k];
+    pick.push_back(p);
+    sn.push_back(n[p]);
+    so.push_back(off);
+    se.push_back(eo);
+    off += (int64_t)n[p] * n[p];
+    eo += n[p];
+  }
+  double *bh = nullptr, *bt = nullptr, *bq = nullptr, *bz = nullptr, *bs = nullptr, *be = nullptr;
+  int* bi = nullptr;
+  QZ_CK(cudaMalloc(&bh, off * sizeof(double)));
+  QZ_CK(cudaMalloc(&bt, off * sizeof(double)));
+  QZ_CK(cudaMalloc(&bq, off * sizeof(double)));
+  QZ_CK(cudaMalloc(&bz, off * sizeof(double)));
+  QZ_CK(cudaMalloc(&bs, off * 2 * sizeof(double)));
+  QZ_CK(cudaMalloc(&be, eo * 3 * sizeof(double)));
+  QZ_CK(cudaMalloc(&bi, k * sizeof(int)));
+  if (c->err != cudaSuccess) return 10001;
+  for (int j = 0; j < k; ++j) {
+    size_t bytes = (size_t)sn[j] * sn[j] * sizeof(double);
+    QZ_CK(cudaMemcpyAsync(bs + so[j], h + moff[pick[j]], bytes, cudaMemcpyDeviceToDevice, c->stream));
+    QZ_CK(cudaMemcpyAsync(bs + off + so[j], t + moff[pick[j]], bytes, cudaMemcpyDeviceToDevice, c->stream));
+  }
+  const int threads[2] = {128, 256};
+  const int smems[4] = {0, 48, 64, kBatchSmemMax};
+  double best = 1e300;
+  int bt_ = c->batch_threads, bs_ = c->batch_smem_max, bc_ = c->batch_ctas_per_sm;
+  for (int th : threads)
+    for (int sm : smems)
+      for (int cps = 1; cps <= 4; cps *= 2) {
+        size_t smem = batch_smem_bytes(sm);
+        if (smem * cps > 220 * 1024) continue;
+        c->batch_threads = th;
+        c->batch_smem_max = sm;
+        c->batch_ctas_per_sm = cps;
+        QZ_CK(cudaMemcpyAsync(bh, bs, off * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+        QZ_CK(cudaMemcpyAsync(bt, bs + off, off * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+        int rc = b200qz_solve_batched_dev(c, k, sn.data(), so.data(), se.data(), bh, bt, bq, bz, be, be + eo,
+                                          be + 2 * eo, bi);
+        if (rc != 0) continue;
+        if (c->batch_seconds < best) {
+          best = c->batch_seconds;
+          bt_ = th; bs_ = sm; bc_ = cps;
+        }
+      }
+  c->batch_threads = bt_;
+  c->batch_smem_max = bs_;
+  c->batch_ctas_per_sm = bc_;
+  if (c->bexec) { cudaGraphExecDestroy(c->bexec); c->bexec = nullptr; }
+  if (c->bgraph) { cudaGraphDestroy(c->bgraph); c->bgraph = nullptr; }
+  cudaFree(bh); cudaFree(bt); cudaFree(bq); cudaFree(bz); cudaFree(bs); cudaFree(be); cudaFree(bi);
+  if (best_seconds) *best_seconds = best;
+  return c->err == cudaSuccess ? 0 : 10001;
+}
+
+extern "C" int b200qz_batched_config(const b200qz_ctx* c, int* threads, int* smem_max, int* ctas_per_sm) {
+  if (!c) return -1;
+  if (threads) *threads = c->batch_threads;
+  if (smem_max) *smem_max = c->batch_smem_max;
+  if (ctas_per_sm) *ctas_per_sm = c->batch_ctas_per_sm;
+  return 0;
 }
 
 // ---------------------------------------------------------------------------

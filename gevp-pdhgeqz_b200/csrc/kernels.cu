@@ -187,13 +187,20 @@ __global__ void __launch_bounds__(kWinThreads) k_inf_win(double* H, double* T, i
 // ---------------------------------------------------------------------------
 // deflation scan: ktop = largest k in (ifirst, kbot] with negligible
 // H(k,k-1) (zeroed), then zero T-diagonal entries in [ktop, kbot].
-// out = {ktop, ninf, jmax, jmin}
+// out = {ktop, ninf, jmax, jmin, nonfinite}
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(1024) k_scan(double* H, double* T, int64_t ld, int ifirst, int kbot, Tol tol,
                                                int* out) {
   __shared__ int s_best;
-  __shared__ int s_cnt, s_jmax, s_jmin;
-  if (threadIdx.x == 0) { s_best = -1; s_cnt = 0; s_jmax = -1; s_jmin = 0x7fffffff; }
+  __shared__ int s_cnt, s_jmax, s_jmin, s_bad;
+  if (threadIdx.x == 0) { s_best = -1; s_cnt = 0; s_jmax = -1; s_jmin = 0x7fffffff; s_bad = 0; }
+  __syncthreads();
+  // numerical breakdown guard: a non-finite entry on the diagonals of the
+  // active block is reported instead of being iterated on
+  for (int j = ifirst + (int)threadIdx.x; j <= kbot; j += blockDim.x) {
+    double a = G(H, ld, j, j), b = G(T, ld, j, j), c = (j > ifirst) ? G(H, ld, j, j - 1) : 0.0;
+    if (!isfinite(a) || !isfinite(b) || !isfinite(c)) s_bad = 1;
+  }
   __syncthreads();
   for (int base = kbot; base > ifirst; base -= blockDim.x) {
     int k = base - (int)threadIdx.x;
@@ -222,6 +229,7 @@ __global__ void __launch_bounds__(1024) k_scan(double* H, double* T, int64_t ld,
     out[1] = s_cnt;
     out[2] = s_jmax;
     out[3] = (s_cnt > 0) ? s_jmin : -1;
+    out[4] = s_bad;
   }
 }
 

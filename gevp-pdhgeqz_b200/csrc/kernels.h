@@ -9,7 +9,7 @@
 namespace qz {
 
 constexpr int kWinThreads = 128;   // threads of the one-CTA AED / zero-chase kernels
-constexpr int kChaseThreads = 256; // threads of the chase kernel
+constexpr int kChaseThreads = 512; // threads of the chase kernel
 constexpr int kWinSmemMax = 80;    // window size held entirely in shared memory (4 x 80^2 FP64 = 200 KB)
 constexpr int kMaxChain = 26;      // bulges per chain (3*26+2 rows fit a window of 80)
 
@@ -17,6 +17,15 @@ constexpr int kMaxChain = 26;      // bulges per chain (3*26+2 rows fit a window
 // a row then fall into distinct banks (an even one puts a whole row of an
 // 80-wide window into the same bank)
 __host__ __device__ constexpr int smem_ld(int n) { return (n % 2 == 0) ? n + 1 : n; }
+
+// batched solver: threads per CTA (upper bound) and pencils held in shared memory
+constexpr int kBatchThreads = 256;
+constexpr int kBatchSmemMax = 80;
+size_t batch_smem_bytes(int smem_max);
+cudaError_t batch_init();
+void launch_batch(cudaStream_t st, int grid, int threads, int smem_max, int count, const int* order, const int* nsz,
+                  const int64_t* moff, const int64_t* eoff, double* H, double* T, double* Q, double* Z, double* AR,
+                  double* AI, double* BE, int* status, int* counter);
 
 // chains chased concurrently (one CTA each) by one wave launch
 constexpr int kMaxWave = 8;

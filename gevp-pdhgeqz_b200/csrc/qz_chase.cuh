@@ -90,6 +90,94 @@ QZ_HD void bulge_step_compute(MatV H, MatV T, int j, int last, bool intro,
   }
 }
 
+// One application of a bulge's reflector (or rotation) to three (or two)
+// entries along a row or a column: p0 + k*stride, k = 0..2.
+struct ApplyItem {
+  double* p;       // first entry (nullptr: empty slot)
+  int stride;      // distance between the entries
+  int kind;        // 1: reflector on 3 entries, 2: rotation on 2 entries
+  const House3* h; // reflector (kind 1)
+  double c, s;     // rotation (kind 2)
+  double a0, a1, a2;
+  QZ_HD void load() {
+    if (!p) return;
+    a0 = p[0];
+    a1 = p[stride];
+    if (kind == 1) a2 = p[2 * stride];
+  }
+  QZ_HD void apply_store() {
+    if (!p) return;
+    if (kind == 1) {
+      house3_apply(*h, a0, a1, a2);
+      p[0] = a0; p[stride] = a1; p[2 * stride] = a2;
+    } else {
+      p[0] = c * a0 + s * a1;
+      p[stride] = -s * a0 + c * a1;
+    }
+  }
+};
+
+// item loc of bulge b in phase B: rows j.. of H (columns j..wk-1), rows
+// j.. of T (columns past the T block), columns j.. of U (all rows)
+QZ_HD ApplyItem left_item(const BulgeRec* rec, int idx, int tot, int S, int wk, MatV H, MatV T, MatV U) {
+  ApplyItem it;
+  it.p = nullptr;
+  if (idx >= tot) return it;
+  int b = idx / S;
+  int loc = idx - b * S;
+  const BulgeRec& r = rec[b];
+  if (r.kind == 0) return it;
+  int j = r.j;
+  int t0 = (r.kind == 1) ? j + 3 : j + 2;
+  int nh = wk - j, nt = wk - t0;
+  if (nt < 0) nt = 0;
+  it.kind = r.kind;
+  it.h = &r.L;
+  it.c = r.L.s;
+  it.s = r.L.u0;
+  if (loc < nh) {
+    it.p = &H(j, j + loc);
+    it.stride = 1;
+  } else if (loc < nh + nt) {
+    it.p = &T(j, t0 + (loc - nh));
+    it.stride = 1;
+  } else if (loc < nh + nt + wk) {
+    it.p = &U(loc - nh - nt, j);
+    it.stride = U.ld;
+  }
+  return it;
+}
+
+// item loc of bulge b in phase C: columns j.. of H (rows 0..min(j+3,last)
+// or 0..last), columns j.. of T above the T block, columns j.. of V
+QZ_HD ApplyItem right_item(const BulgeRec* rec, int idx, int tot, int S, int wk, int last, MatV H, MatV T,
+                           MatV V) {
+  ApplyItem it;
+  it.p = nullptr;
+  if (idx >= tot) return it;
+  int b = idx / S;
+  int loc = idx - b * S;
+  const BulgeRec& r = rec[b];
+  if (r.kind == 0) return it;
+  int j = r.j;
+  int hr = (r.kind == 1) ? ((j + 4 < last + 1) ? j + 4 : last + 1) : last + 1;
+  it.kind = r.kind;
+  it.h = &r.R;
+  it.c = r.R.s;
+  it.s = r.R.u0;
+  if (loc < hr) {
+    it.p = &H(loc, j);
+    it.stride = H.ld;
+  } else if (loc < hr + j) {
+    it.p = &T(loc - hr, j);
+    it.stride = T.ld;
+  } else if (loc < hr + j + wk) {
+    it.p = &V(loc - hr - j, j);
+    it.stride = V.ld;
+  }
+  return it;
+}
+
 // Chase a chain through a window of size wk held in H, T (wk x wk), while
 // accumulating U, V (wk x wk, identity on entry).  last = last row of the
 // active block inside the window (wk-1 if the block continues below).
@@ -121,97 +209,31 @@ QZ_HD void cta_chase_window(X& x, int wk, int last, MatV H, MatV T, MatV U, MatV
       H(j + 1, j - 1) = 0.0;
       if (r.kind == 1) H(j + 2, j - 1) = 0.0;
     }
-    for (int b = 0; b < nb; ++b) {
-      const BulgeRec& r = rec[b];
-      if (r.kind == 0) continue;
-      int j = r.j;
-      if (r.kind == 1) {
-        int nh = wk - j, nt = wk - (j + 3);
-        int tot = nh + (nt > 0 ? nt : 0) + wk;
-        for (int i = x.tid; i < tot; i += x.nt) {
-          if (i < nh) {
-            int c = j + i;
-            double a0 = H(j, c), a1 = H(j + 1, c), a2 = H(j + 2, c);
-            house3_apply(r.L, a0, a1, a2);
-            H(j, c) = a0; H(j + 1, c) = a1; H(j + 2, c) = a2;
-          } else if (i < nh + (nt > 0 ? nt : 0)) {
-            int c = j + 3 + (i - nh);
-            double a0 = T(j, c), a1 = T(j + 1, c), a2 = T(j + 2, c);
-            house3_apply(r.L, a0, a1, a2);
-            T(j, c) = a0; T(j + 1, c) = a1; T(j + 2, c) = a2;
-          } else {
-            int rr = i - nh - (nt > 0 ? nt : 0);
-            double a0 = U(rr, j), a1 = U(rr, j + 1), a2 = U(rr, j + 2);
-            house3_apply(r.L, a0, a1, a2);
-            U(rr, j) = a0; U(rr, j + 1) = a1; U(rr, j + 2) = a2;
-          }
-        }
-      } else {
-        double c = r.L.s, s = r.L.u0;
-        int nh = wk - j, nt = wk - (j + 2);
-        int tot = nh + (nt > 0 ? nt : 0) + wk;
-        for (int i = x.tid; i < tot; i += x.nt) {
-          if (i < nh) {
-            int cc = j + i;
-            double a = H(j, cc), bb = H(j + 1, cc);
-            H(j, cc) = c * a + s * bb; H(j + 1, cc) = -s * a + c * bb;
-          } else if (i < nh + (nt > 0 ? nt : 0)) {
-            int cc = j + 2 + (i - nh);
-            double a = T(j, cc), bb = T(j + 1, cc);
-            T(j, cc) = c * a + s * bb; T(j + 1, cc) = -s * a + c * bb;
-          } else {
-            int rr = i - nh - (nt > 0 ? nt : 0);
-            double a = U(rr, j), bb = U(rr, j + 1);
-            U(rr, j) = c * a + s * bb; U(rr, j + 1) = -s * a + c * bb;
-          }
-        }
-      }
+    // Flattened (bulge, item) space: bulge b owns slots [b*S, b*S + S) with
+    // S = 3*wk (an upper bound of its item count).  Items of different
+    // bulges, and different items of one bulge, touch disjoint entries, so
+    // each thread loads two items before storing either (latency overlap).
+    const int S = 3 * wk;
+    const int tot = nb * S;
+    for (int i0 = x.tid; i0 < tot; i0 += 2 * x.nt) {
+      ApplyItem it[2];
+      it[0] = left_item(rec, i0, tot, S, wk, H, T, U);
+      it[1] = left_item(rec, i0 + x.nt, tot, S, wk, H, T, U);
+      it[0].load();
+      it[1].load();
+      it[0].apply_store();
+      it[1].apply_store();
     }
     x.sync();
     // ---- phase C: right transformations ----
-    for (int b = 0; b < nb; ++b) {
-      const BulgeRec& r = rec[b];
-      if (r.kind == 0) continue;
-      int j = r.j;
-      if (r.kind == 1) {
-        int hr = (j + 4 < last + 1) ? j + 4 : last + 1;
-        int tot = hr + j + wk;
-        for (int i = x.tid; i < tot; i += x.nt) {
-          if (i < hr) {
-            double a0 = H(i, j), a1 = H(i, j + 1), a2 = H(i, j + 2);
-            house3_apply(r.R, a0, a1, a2);
-            H(i, j) = a0; H(i, j + 1) = a1; H(i, j + 2) = a2;
-          } else if (i < hr + j) {
-            int rr = i - hr;
-            double a0 = T(rr, j), a1 = T(rr, j + 1), a2 = T(rr, j + 2);
-            house3_apply(r.R, a0, a1, a2);
-            T(rr, j) = a0; T(rr, j + 1) = a1; T(rr, j + 2) = a2;
-          } else {
-            int rr = i - hr - j;
-            double a0 = V(rr, j), a1 = V(rr, j + 1), a2 = V(rr, j + 2);
-            house3_apply(r.R, a0, a1, a2);
-            V(rr, j) = a0; V(rr, j + 1) = a1; V(rr, j + 2) = a2;
-          }
-        }
-      } else {
-        double c = r.R.s, s = r.R.u0;
-        int hr = last + 1;
-        int tot = hr + j + wk;
-        for (int i = x.tid; i < tot; i += x.nt) {
-          if (i < hr) {
-            double a = H(i, j), bb = H(i, j + 1);
-            H(i, j) = c * a + s * bb; H(i, j + 1) = -s * a + c * bb;
-          } else if (i < hr + j) {
-            int rr = i - hr;
-            double a = T(rr, j), bb = T(rr, j + 1);
-            T(rr, j) = c * a + s * bb; T(rr, j + 1) = -s * a + c * bb;
-          } else {
-            int rr = i - hr - j;
-            double a = V(rr, j), bb = V(rr, j + 1);
-            V(rr, j) = c * a + s * bb; V(rr, j + 1) = -s * a + c * bb;
-          }
-        }
-      }
+    for (int i0 = x.tid; i0 < tot; i0 += 2 * x.nt) {
+      ApplyItem it[2];
+      it[0] = right_item(rec, i0, tot, S, wk, last, H, T, V);
+      it[1] = right_item(rec, i0 + x.nt, tot, S, wk, last, H, T, V);
+      it[0].load();
+      it[1].load();
+      it[0].apply_store();
+      it[1].apply_store();
     }
     // deferred stores owned by the bulge's thread
     for (int b = x.tid; b < nb; b += x.nt) {

@@ -864,3 +864,51 @@ QZ_HD void cta_aed(X& x, WinState& w, double s, double* sr, double* si_, double*
 }
 
 }  // namespace qz
+
+namespace qz {
+
+// ---------------------------------------------------------------------------
+// Finalisation of a Schur form held in one window: beta >= 0 for 1x1
+// blocks (negate the column of H, T and Z, as DHGEQZ does) and the
+// eigenvalues (alphar, alphai, beta) of every block.  2x2 blocks are
+// already standardised by cta_small_qz (B diagonal, positive).
+// ---------------------------------------------------------------------------
+template <class X>
+QZ_HD void cta_finalize(X& x, WinState& w, double* ar, double* ai, double* be) {
+  int n = w.n;
+  // column signs: columns are independent
+  for (int j = 0; j < n; ++j) {
+    bool below = (j + 1 < n) && w.H(j + 1, j) != 0.0;
+    bool above = (j > 0) && w.H(j, j - 1) != 0.0;
+    if (below || above) continue;
+    if (!(w.T(j, j) < 0.0)) continue;
+    x.sync();
+    for (int i = x.tid; i <= j; i += x.nt) {
+      w.H(i, j) = -w.H(i, j);
+      w.T(i, j) = -w.T(i, j);
+    }
+    if (w.wantz)
+      for (int i = x.tid; i < n; i += x.nt) w.Z(i, j) = -w.Z(i, j);
+  }
+  x.sync();
+  for (int j = x.tid; j < n; j += x.nt) {
+    bool below = (j + 1 < n) && w.H(j + 1, j) != 0.0;
+    bool above = (j > 0) && w.H(j, j - 1) != 0.0;
+    if (!below && !above) {
+      ar[j] = w.H(j, j);
+      ai[j] = 0.0;
+      be[j] = w.T(j, j);
+      continue;
+    }
+    int f = below ? j : j - 1;
+    double a[4] = {w.H(f, f), w.H(f + 1, f), w.H(f, f + 1), w.H(f + 1, f + 1)};
+    double o_ar[2], o_ai[2], o_be[2];
+    eig2_complex(a, w.T(f, f), w.T(f + 1, f + 1), o_ar, o_ai, o_be);
+    ar[j] = o_ar[j - f];
+    ai[j] = o_ai[j - f];
+    be[j] = o_be[j - f];
+  }
+  x.sync();
+}
+
+}  // namespace qz

@@ -154,20 +154,23 @@ QZ_HD void house3(double x0, double x1, double x2, House3& h, double& beta) {
     beta = x0;
     return;
   }
+  // P is invariant under scaling of u: outside the safe range work with
+  // x / max|x| so that u^T u can neither underflow (a collapsing bulge has
+  // entries far below 1e-140) nor overflow
   double m = dmax(fabs(x0), dmax(fabs(x1), fabs(x2)));
-  double nrm;
-  if (m > kSafeLo && m < kSafeHi) {
-    nrm = sqrt(x0 * x0 + x1 * x1 + x2 * x2);
-  } else {
-    double a = x0 / m, b = x1 / m, c = x2 / m;
-    nrm = sqrt(a * a + b * b + c * c) * m;
+  double sc = 1.0;
+  if (!(m > kSafeLo && m < kSafeHi)) {
+    sc = m;
+    x0 /= m; x1 /= m; x2 /= m;
   }
-  beta = -dsign(nrm, x0);
-  h.u0 = x0 - beta;
+  double nrm = sqrt(x0 * x0 + x1 * x1 + x2 * x2);
+  double b = -dsign(nrm, x0);
+  h.u0 = x0 - b;
   h.u1 = x1;
   h.u2 = x2;
   double uu = h.u0 * h.u0 + x1 * x1 + x2 * x2;
   h.s = 2.0 / uu;
+  beta = b * sc;
 }
 QZ_HD void house3_apply(const House3& h, double& a0, double& a1, double& a2) {
   double t = h.s * (h.u0 * a0 + h.u1 * a1 + h.u2 * a2);
@@ -225,16 +228,32 @@ QZ_HD void shift_column(double h11, double h21, double h12, double h22, double h
                         double t11, double t12, double t22,
                         double c2, double c1, double c0,
                         double& v0, double& v1, double& v2) {
-  // p(M) e1 multiplied by t11^2 * t22 (M = H T^{-1}): no division, so a
-  // tiny T diagonal entry (a nearly infinite eigenvalue) cannot overflow
+  // Scale H and T entries to at most one (M = H T^{-1} scales by k =
+  // tmax/hmax, so c1 -> c1*k, c0 -> c0*k^2), then form p(M) e1 multiplied
+  // by t11^2 * t22: no division by a possibly tiny T diagonal entry and no
+  // overflow for graded entries.
+  double hm = dmax(dmax(fabs(h11), fabs(h21)), dmax(dmax(fabs(h12), fabs(h22)), fabs(h32)));
+  double tm = dmax(fabs(t11), dmax(fabs(t12), fabs(t22)));
+  if (hm > 0.0 && tm > 0.0 && isfinite(hm) && isfinite(tm)) {
+    h11 /= hm; h21 /= hm; h12 /= hm; h22 /= hm; h32 /= hm;
+    t11 /= tm; t12 /= tm; t22 /= tm;
+    double k = tm / hm;
+    c1 *= k;
+    c0 *= k * k;
+    double cm = dmax(fabs(c2), dmax(fabs(c1), fabs(c0)));
+    if (cm > 0.0 && isfinite(cm)) { c2 /= cm; c1 /= cm; c0 /= cm; }
+  }
   double g = h11 * t22 - t12 * h21;
   v0 = c2 * (h11 * g + h12 * h21 * t11) - c1 * h11 * t11 * t22 + c0 * t11 * t11 * t22;
   v1 = c2 * (h21 * g + h22 * h21 * t11) - c1 * h21 * t11 * t22;
   v2 = c2 * h32 * h21 * t11;
   double m = dmax(fabs(v0), dmax(fabs(v1), fabs(v2)));
-  if (m > 0.0 && isfinite(m)) { v0 /= m; v1 /= m; v2 /= m; }
-  // the scaling by t11^2*t22 may flip the sign of the vector; the
-  // reflector built from it is the same
+  if (m > 0.0 && isfinite(m)) {
+    v0 /= m; v1 /= m; v2 /= m;
+  } else {
+    // degenerate polynomial column: no bulge (identity reflector)
+    v0 = 1.0; v1 = 0.0; v2 = 0.0;
+  }
 }
 
 // Eigenvalues of a 2x2 pencil (A, B), B upper triangular (b10 = 0), as

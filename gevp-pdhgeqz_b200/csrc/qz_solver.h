@@ -33,6 +33,7 @@ struct SolveParams {
   int aed_nskip = 0;     // AED spike test stops after this many consecutive
                          // undeflatable blocks (0: test the whole window)
   int max_wave = 8;      // chains chased concurrently (one CTA each)
+  int stall_limit = 300; // iterations without deflation before giving up
 };
 
 struct SolveStats {
@@ -42,6 +43,7 @@ struct SolveStats {
   double win_bytes = 0.0;  // algorithmic bytes of window kernels (load+store)
   int64_t launches = 0;    // kernel launches issued by the solve
   int64_t aed_fail = 0;    // AED windows whose small QZ did not converge
+  int64_t exceptional = 0; // sweeps with exceptional shifts
 };
 
 // reference shift-count table (piparmq.f:504-533)
@@ -163,7 +165,7 @@ inline void plan_chain(int ktop, int kbot, int W, int nb, const ShiftPair* sp, i
 }
 
 // Backend interface (implemented by the GPU backend):
-//   void scan(int ifirst, int kbot, int* out4)          // ktop, ninf, jmax, jmin
+//   void scan(int ifirst, int kbot, int* out5)          // ktop, ninf, jmax, jmin, nonfinite
 //   void aed(int ktop, int kwtop, int kbot, int* info3, double* shifts) // m, status, transformed
 //   void update(int w, int wk, int which)               // which 0: AED factors, 1: zero-chase U,V
 //   void chase_wave(const WinPlan* const* wins, int n)  // one CTA per window
@@ -178,14 +180,21 @@ int qz_iterate(BK& bk, int n, int ilo, int ihi, const SolveParams& P, SolveStats
   std::vector<double> sh(3 * std::max(P.nw_max, P.nmin) + 8);
   std::vector<ShiftPair> pairs;
   std::vector<const WinPlan*> wave;
-  int scan_out[4];
+  int scan_out[5];
   int info3[3];
+  int stall = 0;             // iterations since the last deflation
+  int last_kbot = kbot, last_ktop = -1;
   for (int64_t it = 0; it < maxit; ++it) {
     if (kbot < ifirst) return 0;
     ++S.iters;
     bk.scan(ifirst, kbot, scan_out);
     int ktop = scan_out[0];
     int ninf = scan_out[1];
+    if (scan_out[4]) return -1;  // non-finite entry in the active block
+    if (kbot != last_kbot || ktop != last_ktop) stall = 0; else ++stall;
+    last_kbot = kbot;
+    last_ktop = ktop;
+    if (stall > P.stall_limit) return kbot + 1;
     if (P.verbose)
       std::fprintf(stderr, "[b200qz] it=%lld ktop=%d kbot=%d ninf=%d\n", (long long)it, ktop, kbot, ninf);
     if (ktop == kbot) {
@@ -254,6 +263,21 @@ int qz_iterate(BK& bk, int n, int ilo, int ihi, const SolveParams& P, SolveStats
     int ns = std::min(nsmax, m - (m % 2));
     if (ns < 2) continue;
     pair_shifts(sh.data(), sh.data() + m, sh.data() + 2 * m, m, ns, pairs);
+    if (stall > 0 && stall % 40 == 0) {
+      // no deflation for a while: exceptional shifts (scaled pseudo-random
+      // real pairs spread over the spectrum's magnitude) break the cycle
+      double mag = 0.0;
+      for (int i = 0; i < m; ++i)
+        if (sh[2 * m + i] != 0.0) mag = std::max(mag, std::fabs(sh[i] / sh[2 * m + i]));
+      if (!(mag > 0.0) || !std::isfinite(mag)) mag = 1.0;
+      for (size_t k = 0; k < pairs.size(); ++k) {
+        double a = mag * std::sin(1.0 + 2.0 * k + 0.37 * stall), b = mag * std::cos(0.5 + 3.0 * k);
+        pairs[k].c2 = 1.0; pairs[k].c1 = a + b; pairs[k].c0 = a * b;
+        double mx = std::max(1.0, std::max(std::fabs(pairs[k].c1), std::fabs(pairs[k].c0)));
+        pairs[k].c2 /= mx; pairs[k].c1 /= mx; pairs[k].c0 /= mx;
+      }
+      ++S.exceptional;
+    }
     int npairs = (int)pairs.size();
     if (npairs == 0) continue;
     int nh2 = kbot - ktop + 1;

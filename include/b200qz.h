@@ -38,7 +38,9 @@ typedef struct b200qz_ctx b200qz_ctx;
  * INFO: -1 JOB, -2 COMPQ, -3 COMPZ, -4 N, -5 ILO, -6 IHI, -7 NB < 5,
  * -8 NB /= MB, -9 LDWORK, -10 LIWORK (PDHGEQZ.f:383-444), -(i*1000+9)
  * for a bad leading dimension of argument i; > 0 the index of the first
- * unconverged row (PDHGEQZ0.f:1207); 10001 a CUDA error. */
+ * unconverged row (PDHGEQZ0.f:1207), also returned when no eigenvalue
+ * deflates for "stall_limit" iterations; 10001 a CUDA error; 10002
+ * non-finite entries in the active block. */
 void pdhgeqz_(const char* job, const char* compq, const char* compz, const int* n, const int* ilo,
               const int* ihi, double* h, const int* desch, double* t, const int* desct, double* alphar,
               double* alphai, double* beta, double* q, const int* descq, double* z, const int* descz,
@@ -87,7 +89,9 @@ int b200qz_solve_host(b200qz_ctx* ctx, char job, char compq, char compz, int n, 
  * and inside the AED kernel 19 small QZ, 20 reordering, 21 spike
  * reflector + RQ update, 22 Hessenberg-triangular re-reduction;
  * 23 kernel launches issued by the solve, 24 AED windows whose small QZ
- * did not converge (they deflate nothing and supply diagonal shifts).
+ * did not converge (they deflate nothing and supply diagonal shifts),
+ * 25 sweeps run with exceptional shifts (after 40 iterations without
+ * deflation).
  * Returns the number of values written. */
 int b200qz_get_stats(const b200qz_ctx* ctx, double* out, int nout);
 
@@ -100,9 +104,40 @@ int b200qz_set_params(b200qz_ctx* ctx, int nw_max, int w_chase, int nmin, int ni
 /* Set one tunable by name: "nw_max", "w_chase", "nmin", "nibble",
  * "ns_max", "maxit_factor", "chain_max" (bulges per chain), "aed_nskip"
  * (AED spike test stops after this many consecutive undeflatable blocks,
- * 0 = whole window), "max_wave" (chains chased concurrently, 1..8).
+ * 0 = whole window), "max_wave" (chains chased concurrently, 1..8),
+ * "stall_limit" (iterations without deflation before INFO > 0).
  * Returns 0, -2 for an unknown name, -3 for a value out of range. */
 int b200qz_set_param(b200qz_ctx* ctx, const char* name, double value);
+
+/* ------------------------------------------------------------------ */
+/* Batched independent pencils (sizes may differ).                      */
+/* ------------------------------------------------------------------ */
+
+/* Reduce count independent pencils to generalized Schur form with Q, Z in
+ * one persistent launch (CUDA-graph captured, replayed while the layout
+ * stays the same).  Device buffers h, t, q, z hold pencil p (size n[p],
+ * leading dimension n[p]) at offset moff[p] (in doubles); its eigenvalues
+ * go to alphar/alphai/beta at offset eoff[p]; info[p] (device) is 0 or the
+ * 1-based row that did not converge.  n, moff, eoff are host arrays.
+ * Returns 0, a negative argument error, or 10001 (CUDA error).  No
+ * reference counterpart (the reference solves one pencil per call). */
+int b200qz_solve_batched_dev(b200qz_ctx* ctx, int count, const int* n, const long long* moff,
+                             const long long* eoff, double* h, double* t, double* q, double* z,
+                             double* alphar, double* alphai, double* beta, int* info);
+
+/* Device seconds of the last batched launch. */
+double b200qz_batched_seconds(const b200qz_ctx* ctx);
+
+/* Autotune the batched launch (threads per CTA, largest pencil kept in
+ * shared memory, CTAs per SM) on a copy of `sample` pencils spread over the
+ * size range of the batch; keeps the fastest configuration in the context.
+ * h, t are device buffers laid out as for b200qz_solve_batched_dev; they are
+ * not modified.  best_seconds (host, may be NULL) receives the best time. */
+int b200qz_batched_autotune(b200qz_ctx* ctx, int count, const int* n, const long long* moff,
+                            const double* h, const double* t, int sample, double* best_seconds);
+
+/* Current batched configuration. */
+int b200qz_batched_config(const b200qz_ctx* ctx, int* threads, int* smem_max, int* ctas_per_sm);
 
 /* ------------------------------------------------------------------ */
 /* Kernel-level entry points (device pointers), for parity tests.       */
