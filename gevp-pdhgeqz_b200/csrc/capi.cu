@@ -141,7 +141,7 @@ struct GpuBackend {
     int nw = kbot - kwtop + 1;
     c->timer.begin(kPhAed, c->stream);
     launch_aed(c->stream, H, T, ld, ktop, kwtop, nw, tol, c->Ua, c->Va, c->shifts, c->dinfo + 4, c->gscratch,
-               c->timer.on ? c->dts : nullptr, (kwtop > ktop) ? c->params.aed_nskip : 0);
+               c->timer.on ? c->dts : nullptr, (kwtop > ktop) ? c->params.aed_nskip : 0, c->params.aed_threads);
     c->stats.launches += 1;
     c->timer.end(c->stream);
     QZ_CK(cudaMemcpyAsync(c->hinfo + 4, c->dinfo + 4, 3 * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
@@ -458,6 +458,7 @@ int b200qz_set_param(b200qz_ctx* c, const char* name, double value) {
   else if (k == "aed_nskip") { if (v < 0) return -3; P.aed_nskip = v; }
   else if (k == "max_wave") { if (v < 1 || v > kMaxWave) return -3; P.max_wave = v; }
   else if (k == "stall_limit") { if (v < 1) return -3; P.stall_limit = v; }
+  else if (k == "aed_threads") { if (v != 32 && v != 64 && v != 128) return -3; P.aed_threads = v; }
   else return -2;
   return 0;
 }

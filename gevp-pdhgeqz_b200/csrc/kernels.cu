@@ -21,12 +21,18 @@
 
 namespace qz {
 
-struct DevExec {
+// Executor of the CTA-level algorithms.  With kWarp the CTA is one warp and
+// the barrier is __syncwarp (also a shared-memory fence for the warp).
+template <bool kWarp>
+struct DevExecT {
   int tid, nt;
   int* si;
   double* sd;
   unsigned long long* ts = nullptr;  // phase timestamps (ns), thread 0 writes
-  __device__ void sync() { __syncthreads(); }
+  __device__ void sync() {
+    if constexpr (kWarp) __syncwarp();
+    else __syncthreads();
+  }
   __device__ void stamp(int k) {
     if (ts && tid == 0) {
       unsigned long long t;
@@ -36,6 +42,8 @@ struct DevExec {
   }
 };
 
+using DevExec = DevExecT<false>;
+
 // shared-memory scratch carved at the end of the dynamic smem block
 constexpr int kSi = 64;
 
@@ -44,7 +52,8 @@ __device__ __forceinline__ double& G(double* p, int64_t ld, int i, int j) { retu
 // ---------------------------------------------------------------------------
 // AED / small-solve window kernel
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kWinThreads) k_aed_win(double* H, double* T, int64_t ld, int ktop, int kwtop,
+template <int kThreads>
+__global__ void __launch_bounds__(kThreads) k_aed_win(double* H, double* T, int64_t ld, int ktop, int kwtop,
                                                          int nw, Tol tol, double* Qw, double* Zw, double* shifts,
                                                          int* info, double* gscratch, int maxit,
                                                          unsigned long long* ts, int nskip) {
@@ -72,7 +81,7 @@ __global__ void __launch_bounds__(kWinThreads) k_aed_win(double* H, double* T, i
     sd = smem;
   }
   int* si = (int*)(sd + 64 + 4 * n);
-  DevExec x{(int)threadIdx.x, (int)blockDim.x, si, sd, ts};
+  DevExecT<kThreads == 32> x{(int)threadIdx.x, kThreads, si, sd, ts};
   for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
     int i = idx % n, j = idx / n;
     Hs[i + j * lw] = G(H, ld, kwtop + i, kwtop + j);
@@ -348,7 +357,11 @@ static size_t upd_smem(int k, int side) {
 
 cudaError_t kernels_init() {
   cudaError_t e;
-  e = cudaFuncSetAttribute(k_aed_win, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)aed_smem_bytes(kWinSmemMax));
+  e = cudaFuncSetAttribute(k_aed_win<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)aed_smem_bytes(kWinSmemMax));
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(k_aed_win<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)aed_smem_bytes(kWinSmemMax));
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(k_aed_win<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)aed_smem_bytes(kWinSmemMax));
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(k_chase_win, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)chase_smem_bytes(kWinSmemMax));
   if (e != cudaSuccess) return e;
@@ -365,9 +378,16 @@ cudaError_t kernels_init() {
 }
 
 void launch_aed(cudaStream_t st, double* H, double* T, int64_t ld, int ktop, int kwtop, int nw, const Tol& tol,
-                double* Qw, double* Zw, double* shifts, int* info, double* gscratch, unsigned long long* ts, int nskip) {
-  k_aed_win<<<1, kWinThreads, aed_smem_bytes(nw), st>>>(H, T, ld, ktop, kwtop, nw, tol, Qw, Zw, shifts, info, gscratch,
-                                                       30 * nw, ts, nskip);
+                double* Qw, double* Zw, double* shifts, int* info, double* gscratch, unsigned long long* ts, int nskip,
+                int threads) {
+  const size_t sm = aed_smem_bytes(nw);
+  if (threads <= 32)
+    k_aed_win<32><<<1, 32, sm, st>>>(H, T, ld, ktop, kwtop, nw, tol, Qw, Zw, shifts, info, gscratch, 30 * nw, ts, nskip);
+  else if (threads <= 64)
+    k_aed_win<64><<<1, 64, sm, st>>>(H, T, ld, ktop, kwtop, nw, tol, Qw, Zw, shifts, info, gscratch, 30 * nw, ts, nskip);
+  else
+    k_aed_win<128><<<1, 128, sm, st>>>(H, T, ld, ktop, kwtop, nw, tol, Qw, Zw, shifts, info, gscratch, 30 * nw, ts,
+                                       nskip);
 }
 void launch_chase_wave(cudaStream_t st, double* H, double* T, int64_t ld, const ChaseWave& wave, int njob, double* U,
                        double* V, int64_t ustride) {

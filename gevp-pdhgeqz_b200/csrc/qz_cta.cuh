@@ -351,245 +351,325 @@ QZ_HD int cta_small_qz(X& x, WinState& w, int maxit) {
 // ---------------------------------------------------------------------------
 // Block swapping (reordering) of a generalized real Schur form.
 // ---------------------------------------------------------------------------
-// Small dense helpers on m x m (m <= 4) column-major arrays.
-QZ_HD void small_mm(int m, const double* A, const double* B, double* C, bool ta, bool tb) {
-  for (int i = 0; i < m; ++i)
-    for (int j = 0; j < m; ++j) {
+// Small dense helpers on M x M (M <= 4) column-major arrays.  Every loop
+// bound is a compile-time constant so the arrays stay in registers.
+template <int M, bool TA, bool TB>
+QZ_HD void small_mm(const double* A, const double* B, double* C) {
+#pragma unroll
+  for (int i = 0; i < M; ++i)
+#pragma unroll
+    for (int j = 0; j < M; ++j) {
       double acc = 0.0;
-      for (int k = 0; k < m; ++k) {
-        double a = ta ? A[k + m * i] : A[i + m * k];
-        double b = tb ? B[j + m * k] : B[k + m * j];
+#pragma unroll
+      for (int k = 0; k < M; ++k) {
+        double a = TA ? A[k + M * i] : A[i + M * k];
+        double b = TB ? B[j + M * k] : B[k + M * j];
         acc += a * b;
       }
-      C[i + m * j] = acc;
+      C[i + M * j] = acc;
     }
 }
 
-// Full orthogonal Q (m x m) from Householder QR of the m x k matrix X
-// (column-major, ld m); the first k columns of Q span range(X).
-QZ_HD void small_qr_q(int m, int k, double* X, double* Q) {
-  for (int i = 0; i < m * m; ++i) Q[i] = 0.0;
-  for (int i = 0; i < m; ++i) Q[i + m * i] = 1.0;
-  for (int c = 0; c < k; ++c) {
-    // reflector for X(c:m, c)
-    double nrm = 0.0, mx = 0.0;
-    for (int i = c; i < m; ++i) mx = dmax(mx, fabs(X[i + m * c]));
+// Full orthogonal Q (M x M) from Householder QR of the M x K matrix X
+// (column-major, ld M); the first K columns of Q span range(X).
+template <int M, int K>
+QZ_HD void small_qr_q(double* X, double* Q) {
+#pragma unroll
+  for (int i = 0; i < M * M; ++i) Q[i] = (i % (M + 1) == 0) ? 1.0 : 0.0;
+#pragma unroll
+  for (int c = 0; c < K; ++c) {
+    double mx = 0.0;
+#pragma unroll
+    for (int i = c; i < M; ++i) mx = dmax(mx, fabs(X[i + M * c]));
     if (mx == 0.0) continue;
-    for (int i = c; i < m; ++i) { double t = X[i + m * c] / mx; nrm += t * t; }
+    double nrm = 0.0;
+    const double rmx = 1.0 / mx;
+#pragma unroll
+    for (int i = c; i < M; ++i) { double t = X[i + M * c] * rmx; nrm += t * t; }
     nrm = sqrt(nrm) * mx;
-    double alpha = X[c + m * c];
+    double alpha = X[c + M * c];
     double beta = -dsign(nrm, alpha);
-    double v[4];
+    double v[M];
     v[0] = 1.0;
     double sc = 1.0 / (alpha - beta);
-    for (int i = c + 1; i < m; ++i) v[i - c] = X[i + m * c] * sc;
+#pragma unroll
+    for (int i = c + 1; i < M; ++i) v[i - c] = X[i + M * c] * sc;
     double tau = (beta - alpha) / beta;
-    // apply to X(:, c:k) and accumulate Q = Q * P
-    for (int j = c; j < k; ++j) {
+#pragma unroll
+    for (int j = c; j < K; ++j) {
       double t = 0.0;
-      for (int i = c; i < m; ++i) t += v[i - c] * X[i + m * j];
+#pragma unroll
+      for (int i = c; i < M; ++i) t += v[i - c] * X[i + M * j];
       t *= tau;
-      for (int i = c; i < m; ++i) X[i + m * j] -= t * v[i - c];
+#pragma unroll
+      for (int i = c; i < M; ++i) X[i + M * j] -= t * v[i - c];
     }
-    for (int i = 0; i < m; ++i) {
+#pragma unroll
+    for (int i = 0; i < M; ++i) {
       double t = 0.0;
-      for (int r = c; r < m; ++r) t += Q[i + m * r] * v[r - c];
+#pragma unroll
+      for (int r = c; r < M; ++r) t += Q[i + M * r] * v[r - c];
       t *= tau;
-      for (int r = c; r < m; ++r) Q[i + m * r] -= t * v[r - c];
+#pragma unroll
+      for (int r = c; r < M; ++r) Q[i + M * r] -= t * v[r - c];
     }
   }
 }
 
-// Gaussian elimination with complete pivoting on an s x s system (s <= 8).
-// Tiny pivots are replaced by smin (the DGETC2 device); returns false if
-// that happened (swap then needs the stability test to decide).
-QZ_HD bool small_solve_cp(int s, double* M, double* rhs, double smin) {
-  int perm_r[8], perm_c[8];
+// Gaussian elimination with complete pivoting on an S x S system (S <= 8,
+// column-major, ld S).  Row and column exchanges are predicated moves so
+// the matrix stays in registers.  Tiny pivots are replaced by smin (the
+// DGETC2 device); returns false if that happened (the swap then relies on
+// the stability test).
+template <int S>
+QZ_HD bool small_solve_cp(double* A, double* rhs, double smin) {
+  int perm[S];
+#pragma unroll
+  for (int i = 0; i < S; ++i) perm[i] = i;
   bool exact = true;
-  for (int i = 0; i < s; ++i) { perm_r[i] = i; perm_c[i] = i; }
-  for (int k = 0; k < s; ++k) {
+#pragma unroll
+  for (int k = 0; k < S; ++k) {
     int pi = k, pj = k;
     double best = -1.0;
-    for (int i = k; i < s; ++i)
-      for (int j = k; j < s; ++j) {
-        double v = fabs(M[i + 8 * j]);
+#pragma unroll
+    for (int i = k; i < S; ++i)
+#pragma unroll
+      for (int j = k; j < S; ++j) {
+        double v = fabs(A[i + S * j]);
         if (v > best) { best = v; pi = i; pj = j; }
       }
-    if (pi != k) {
-      for (int j = 0; j < s; ++j) { double t = M[k + 8 * j]; M[k + 8 * j] = M[pi + 8 * j]; M[pi + 8 * j] = t; }
-      double t = rhs[k]; rhs[k] = rhs[pi]; rhs[pi] = t;
-    }
-    if (pj != k) {
-      for (int i = 0; i < s; ++i) { double t = M[i + 8 * k]; M[i + 8 * k] = M[i + 8 * pj]; M[i + 8 * pj] = t; }
-      int t = perm_c[k]; perm_c[k] = perm_c[pj]; perm_c[pj] = t;
-    }
-    if (fabs(M[k + 8 * k]) < smin) { M[k + 8 * k] = smin; exact = false; }
-    double piv = M[k + 8 * k];
-    for (int i = k + 1; i < s; ++i) {
-      double f = M[i + 8 * k] / piv;
-      if (f == 0.0) continue;
-      for (int j = k + 1; j < s; ++j) M[i + 8 * j] -= f * M[k + 8 * j];
+#pragma unroll
+    for (int i = k + 1; i < S; ++i)
+      if (pi == i) {
+#pragma unroll
+        for (int j = 0; j < S; ++j) { double t = A[k + S * j]; A[k + S * j] = A[i + S * j]; A[i + S * j] = t; }
+        double t = rhs[k]; rhs[k] = rhs[i]; rhs[i] = t;
+      }
+#pragma unroll
+    for (int j = k + 1; j < S; ++j)
+      if (pj == j) {
+#pragma unroll
+        for (int i = 0; i < S; ++i) { double t = A[i + S * k]; A[i + S * k] = A[i + S * j]; A[i + S * j] = t; }
+        int t = perm[k]; perm[k] = perm[j]; perm[j] = t;
+      }
+    if (fabs(A[k + S * k]) < smin) { A[k + S * k] = smin; exact = false; }
+    const double rpiv = 1.0 / A[k + S * k];
+#pragma unroll
+    for (int i = k + 1; i < S; ++i) {
+      double f = A[i + S * k] * rpiv;
+#pragma unroll
+      for (int j = k + 1; j < S; ++j) A[i + S * j] -= f * A[k + S * j];
       rhs[i] -= f * rhs[k];
-      M[i + 8 * k] = 0.0;
+      A[i + S * k] = 0.0;
     }
   }
-  double y[8];
-  for (int k = s - 1; k >= 0; --k) {
+  double y[S];
+#pragma unroll
+  for (int k = S - 1; k >= 0; --k) {
     double acc = rhs[k];
-    for (int j = k + 1; j < s; ++j) acc -= M[k + 8 * j] * y[j];
-    y[k] = acc / M[k + 8 * k];
+#pragma unroll
+    for (int j = k + 1; j < S; ++j) acc -= A[k + S * j] * y[j];
+    y[k] = acc / A[k + S * k];
   }
-  for (int k = 0; k < s; ++k) rhs[perm_c[k]] = y[k];
-  (void)perm_r;
+  // undo the column exchanges: x(perm[k]) = y(k)
+#pragma unroll
+  for (int t = 0; t < S; ++t) {
+    double v = 0.0;
+#pragma unroll
+    for (int k = 0; k < S; ++k)
+      if (perm[k] == t) v = y[k];
+    rhs[t] = v;
+  }
   return exact;
 }
 
-// Compute the orthogonal Qs, Zs (m x m, m = n1+n2) that swap the diagonal
-// blocks of the m x m pencil (S, T) (upper block triangular, column-major
-// ld m).  On success S, T are overwritten by Qs^T S Zs, Qs^T T Zs with the
-// lower-left n1 x n2 ... n2-row block exactly zero.  Returns false if the
-// swap fails the weak stability test (then nothing should be applied).
-QZ_HD bool swap_compute(int n1, int n2, double* S, double* T, double* Qs, double* Zs, double ulp, double smlnum) {
-  int m = n1 + n2;
-  // ||(S,T)||_F
+// Compute the orthogonal Qs, Zs (M x M, M = N1+N2) that swap the diagonal
+// blocks of the M x M pencil block (Hb, Tb) (upper block triangular, read
+// from the window) by the generalized Sylvester equation
+//   A11 R - L A22 = -A12,  B11 R - L B22 = -B12
+// (the DTGEX2 method, dtgex2.f).  On success S2, T2 receive
+// Qs^T (Hb, Tb) Zs with the new lower-left N1 x N2 block exactly zero.
+// Returns false if the swap fails the weak stability test (then nothing
+// is applied).
+template <int N1, int N2>
+QZ_HD bool swap_compute(MatV Hb, MatV Tb, double* S2, double* T2, double* Qs, double* Zs, double ulp,
+                        double smlnum) {
+  constexpr int M = N1 + N2, NQ = N1 * N2, NS = 2 * NQ;
   double fn = 0.0;
-  for (int i = 0; i < m * m; ++i) fn += S[i] * S[i] + T[i] * T[i];
+#pragma unroll
+  for (int c = 0; c < M; ++c)
+#pragma unroll
+    for (int r = 0; r < M; ++r) fn += Hb(r, c) * Hb(r, c) + Tb(r, c) * Tb(r, c);
   fn = sqrt(fn);
-  double thresh = dmax(20.0 * ulp * fn, smlnum);
-  // generalized Sylvester system in unknowns vec(R) (n1*n2), vec(L) (n1*n2)
-  //   A11 R - L A22 = -A12,  B11 R - L B22 = -B12
-  int q = n1 * n2;
-  int s = 2 * q;
-  double M[64];
-  double rhs[8];
-  for (int i = 0; i < 64; ++i) M[i] = 0.0;
-  for (int j = 0; j < n2; ++j)
-    for (int i = 0; i < n1; ++i) {
-      int row = i + n1 * j;  // equation index for entry (i,j)
-      // A11 R : sum_k A11(i,k) R(k,j)
-      for (int k = 0; k < n1; ++k) {
-        M[row + 8 * (k + n1 * j)] += S[i + m * k];
-        M[(row + q) + 8 * (k + n1 * j)] += T[i + m * k];
+  const double thresh = dmax(20.0 * ulp * fn, smlnum);
+  double XR[M * N2], XL[M * N2];
+  {
+    double A[NS * NS];
+    double rhs[NS];
+#pragma unroll
+    for (int i = 0; i < NS * NS; ++i) A[i] = 0.0;
+#pragma unroll
+    for (int j = 0; j < N2; ++j)
+#pragma unroll
+      for (int i = 0; i < N1; ++i) {
+        const int row = i + N1 * j;
+#pragma unroll
+        for (int k = 0; k < N1; ++k) {
+          A[row + NS * (k + N1 * j)] += Hb(i, k);
+          A[(row + NQ) + NS * (k + N1 * j)] += Tb(i, k);
+        }
+#pragma unroll
+        for (int k = 0; k < N2; ++k) {
+          A[row + NS * (NQ + i + N1 * k)] -= Hb(N1 + k, N1 + j);
+          A[(row + NQ) + NS * (NQ + i + N1 * k)] -= Tb(N1 + k, N1 + j);
+        }
+        rhs[row] = -Hb(i, N1 + j);
+        rhs[row + NQ] = -Tb(i, N1 + j);
       }
-      // - L A22 : - sum_k L(i,k) A22(k,j)
-      for (int k = 0; k < n2; ++k) {
-        M[row + 8 * (q + i + n1 * k)] -= S[(n1 + k) + m * (n1 + j)];
-        M[(row + q) + 8 * (q + i + n1 * k)] -= T[(n1 + k) + m * (n1 + j)];
+    small_solve_cp<NS>(A, rhs, dmax(ulp * fn * 1e-3, smlnum));
+#pragma unroll
+    for (int i = 0; i < NS; ++i)
+      if (!isfinite(rhs[i])) return false;
+    // [R; I] and [L; I] (M x N2)
+#pragma unroll
+    for (int j = 0; j < N2; ++j) {
+#pragma unroll
+      for (int i = 0; i < N1; ++i) {
+        XR[i + M * j] = rhs[i + N1 * j];
+        XL[i + M * j] = rhs[NQ + i + N1 * j];
       }
-      rhs[row] = -S[i + m * (n1 + j)];
-      rhs[row + q] = -T[i + m * (n1 + j)];
-    }
-  double smin = dmax(ulp * fn * 1e-3, smlnum);
-  small_solve_cp(s, M, rhs, smin);
-  for (int i = 0; i < s; ++i)
-    if (!isfinite(rhs[i])) return false;
-  // [R; I] and [L; I] (m x n2)
-  double XR[16], XL[16];
-  for (int j = 0; j < n2; ++j) {
-    for (int i = 0; i < n1; ++i) {
-      XR[i + m * j] = rhs[i + n1 * j];
-      XL[i + m * j] = rhs[q + i + n1 * j];
-    }
-    for (int i = 0; i < n2; ++i) {
-      XR[n1 + i + m * j] = (i == j) ? 1.0 : 0.0;
-      XL[n1 + i + m * j] = (i == j) ? 1.0 : 0.0;
+#pragma unroll
+      for (int i = 0; i < N2; ++i) {
+        XR[N1 + i + M * j] = (i == j) ? 1.0 : 0.0;
+        XL[N1 + i + M * j] = (i == j) ? 1.0 : 0.0;
+      }
     }
   }
-  small_qr_q(m, n2, XR, Zs);
-  small_qr_q(m, n2, XL, Qs);
-  double tmp[16], S2[16], T2[16];
-  small_mm(m, S, Zs, tmp, false, false);
-  small_mm(m, Qs, tmp, S2, true, false);
-  small_mm(m, T, Zs, tmp, false, false);
-  small_mm(m, Qs, tmp, T2, true, false);
+  small_qr_q<M, N2>(XR, Zs);
+  small_qr_q<M, N2>(XL, Qs);
+  double blk[M * M], tmp[M * M];
+#pragma unroll
+  for (int c = 0; c < M; ++c)
+#pragma unroll
+    for (int r = 0; r < M; ++r) blk[r + M * c] = Hb(r, c);
+  small_mm<M, false, false>(blk, Zs, tmp);
+  small_mm<M, true, false>(Qs, tmp, S2);
+#pragma unroll
+  for (int c = 0; c < M; ++c)
+#pragma unroll
+    for (int r = 0; r < M; ++r) blk[r + M * c] = Tb(r, c);
+  small_mm<M, false, false>(blk, Zs, tmp);
+  small_mm<M, true, false>(Qs, tmp, T2);
   double ll = 0.0;
-  for (int j = 0; j < n2; ++j)
-    for (int i = n2; i < m; ++i) ll += S2[i + m * j] * S2[i + m * j] + T2[i + m * j] * T2[i + m * j];
+#pragma unroll
+  for (int j = 0; j < N2; ++j)
+#pragma unroll
+    for (int i = N2; i < M; ++i) ll += S2[i + M * j] * S2[i + M * j] + T2[i + M * j] * T2[i + M * j];
   if (!(sqrt(ll) <= thresh)) return false;
-  for (int j = 0; j < n2; ++j)
-    for (int i = n2; i < m; ++i) { S2[i + m * j] = 0.0; T2[i + m * j] = 0.0; }
-  // 1x1 diagonal blocks of T: nothing below the diagonal
-  if (n2 == 1) {}
-  if (n1 == 1) {}
-  for (int i = 0; i < m * m; ++i) { S[i] = S2[i]; T[i] = T2[i]; }
+#pragma unroll
+  for (int j = 0; j < N2; ++j)
+#pragma unroll
+    for (int i = N2; i < M; ++i) { S2[i + M * j] = 0.0; T2[i + M * j] = 0.0; }
   return true;
 }
 
-// Swap the blocks at j1 (size n1) and j1+n1 (size n2) of the window.
+// Swap the blocks at j1 (size N1) and j1+N1 (size N2) of the window.
 // Thread 0 computes, everyone applies.  Returns false (nothing changed)
 // if the swap was rejected.
-template <class X>
-QZ_HD bool cta_swap(X& x, WinState& w, int j1, int n1, int n2) {
-  int m = n1 + n2;
+template <int N1, int N2, class X>
+QZ_HD bool cta_swap_t(X& x, WinState& w, int j1) {
+  constexpr int M = N1 + N2;
   double* sQ = x.sd;       // 16
   double* sZ = x.sd + 16;  // 16
   double* sS = x.sd + 32;  // 16
   double* sT = x.sd + 48;  // 16
   if (x.tid == 0) {
-    for (int c = 0; c < m; ++c)
-      for (int r = 0; r < m; ++r) {
-        sS[r + m * c] = w.H(j1 + r, j1 + c);
-        sT[r + m * c] = w.T(j1 + r, j1 + c);
-      }
-    bool ok = swap_compute(n1, n2, sS, sT, sQ, sZ, w.tol.ulp, w.tol.smlnum);
+    double S2[M * M], T2[M * M], Qs[M * M], Zs[M * M];
+    bool ok = swap_compute<N1, N2>(MatV{&w.H(j1, j1), w.H.ld}, MatV{&w.T(j1, j1), w.T.ld}, S2, T2, Qs, Zs,
+                                   w.tol.ulp, w.tol.smlnum);
+    if (ok) {
+#pragma unroll
+      for (int i = 0; i < M * M; ++i) { sQ[i] = Qs[i]; sZ[i] = Zs[i]; sS[i] = S2[i]; sT[i] = T2[i]; }
+    }
     x.si[2] = ok ? 1 : 0;
   }
   x.sync();
-  bool ok = x.si[2] != 0;
+  const bool ok = x.si[2] != 0;
   if (!ok) { x.sync(); return false; }
-  int n = w.n;
-  // rows j1..j1+m-1, cols j1+m..n-1 : Qs^T * rows
-  for (int j = j1 + m + x.tid; j < n; j += x.nt) {
-    double hv[4], tv[4];
-    for (int r = 0; r < m; ++r) { hv[r] = w.H(j1 + r, j); tv[r] = w.T(j1 + r, j); }
-    for (int r = 0; r < m; ++r) {
+  double q[M * M], z[M * M];
+#pragma unroll
+  for (int i = 0; i < M * M; ++i) { q[i] = sQ[i]; z[i] = sZ[i]; }
+  const int n = w.n;
+  // rows j1..j1+M-1, cols j1+M..n-1 : Qs^T * rows
+  for (int j = j1 + M + x.tid; j < n; j += x.nt) {
+    double hv[M], tv[M];
+#pragma unroll
+    for (int r = 0; r < M; ++r) { hv[r] = w.H(j1 + r, j); tv[r] = w.T(j1 + r, j); }
+#pragma unroll
+    for (int r = 0; r < M; ++r) {
       double ah = 0.0, at = 0.0;
-      for (int k = 0; k < m; ++k) { ah += sQ[k + m * r] * hv[k]; at += sQ[k + m * r] * tv[k]; }
+#pragma unroll
+      for (int k = 0; k < M; ++k) { ah += q[k + M * r] * hv[k]; at += q[k + M * r] * tv[k]; }
       w.H(j1 + r, j) = ah; w.T(j1 + r, j) = at;
     }
   }
-  // cols j1..j1+m-1, rows 0..j1-1 : cols * Zs
+  // cols j1..j1+M-1, rows 0..j1-1 : cols * Zs
   for (int i = x.tid; i < j1; i += x.nt) {
-    double hv[4], tv[4];
-    for (int c = 0; c < m; ++c) { hv[c] = w.H(i, j1 + c); tv[c] = w.T(i, j1 + c); }
-    for (int c = 0; c < m; ++c) {
+    double hv[M], tv[M];
+#pragma unroll
+    for (int c = 0; c < M; ++c) { hv[c] = w.H(i, j1 + c); tv[c] = w.T(i, j1 + c); }
+#pragma unroll
+    for (int c = 0; c < M; ++c) {
       double ah = 0.0, at = 0.0;
-      for (int k = 0; k < m; ++k) { ah += hv[k] * sZ[k + m * c]; at += tv[k] * sZ[k + m * c]; }
+#pragma unroll
+      for (int k = 0; k < M; ++k) { ah += hv[k] * z[k + M * c]; at += tv[k] * z[k + M * c]; }
       w.H(i, j1 + c) = ah; w.T(i, j1 + c) = at;
     }
   }
   if (w.wantq)
     for (int i = x.tid; i < n; i += x.nt) {
-      double v[4];
-      for (int c = 0; c < m; ++c) v[c] = w.Q(i, j1 + c);
-      for (int c = 0; c < m; ++c) {
+      double v[M];
+#pragma unroll
+      for (int c = 0; c < M; ++c) v[c] = w.Q(i, j1 + c);
+#pragma unroll
+      for (int c = 0; c < M; ++c) {
         double a = 0.0;
-        for (int k = 0; k < m; ++k) a += v[k] * sQ[k + m * c];
+#pragma unroll
+        for (int k = 0; k < M; ++k) a += v[k] * q[k + M * c];
         w.Q(i, j1 + c) = a;
       }
     }
   if (w.wantz)
     for (int i = x.tid; i < n; i += x.nt) {
-      double v[4];
-      for (int c = 0; c < m; ++c) v[c] = w.Z(i, j1 + c);
-      for (int c = 0; c < m; ++c) {
+      double v[M];
+#pragma unroll
+      for (int c = 0; c < M; ++c) v[c] = w.Z(i, j1 + c);
+#pragma unroll
+      for (int c = 0; c < M; ++c) {
         double a = 0.0;
-        for (int k = 0; k < m; ++k) a += v[k] * sZ[k + m * c];
+#pragma unroll
+        for (int k = 0; k < M; ++k) a += v[k] * z[k + M * c];
         w.Z(i, j1 + c) = a;
       }
     }
-  if (x.tid == 0) {
-    for (int c = 0; c < m; ++c)
-      for (int r = 0; r < m; ++r) {
-        w.H(j1 + r, j1 + c) = sS[r + m * c];
-        w.T(j1 + r, j1 + c) = sT[r + m * c];
-      }
+  // the block itself: M*M entries of H and T from the computed S2, T2
+  for (int i = x.tid; i < M * M; i += x.nt) {
+    w.H(j1 + i % M, j1 + i / M) = sS[i];
+    w.T(j1 + i % M, j1 + i / M) = sT[i];
   }
   x.sync();
-  // re-standardise the new diagonal blocks (moved block first, size n2)
-  if (n2 == 2) cta_std2x2(x, w, j1);
-  if (n1 == 2) cta_std2x2(x, w, j1 + n2);
+  // re-standardise the new diagonal blocks (moved block first, size N2)
+  if (N2 == 2) cta_std2x2(x, w, j1);
+  if (N1 == 2) cta_std2x2(x, w, j1 + N2);
   return true;
+}
+
+template <class X>
+QZ_HD bool cta_swap(X& x, WinState& w, int j1, int n1, int n2) {
+  if (n1 == 1 && n2 == 1) return cta_swap_t<1, 1>(x, w, j1);
+  if (n1 == 1) return cta_swap_t<1, 2>(x, w, j1);
+  if (n2 == 1) return cta_swap_t<2, 1>(x, w, j1);
+  return cta_swap_t<2, 2>(x, w, j1);
 }
 
 // Move the block starting at ifst (size nb) up to position ilst

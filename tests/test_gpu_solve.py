@@ -40,7 +40,10 @@ def test_solve_matches_lapack(pkg, lapack, n, seed, zf, kind):
     S, P, Q, Z, ar, ai, be, info = pkg.solve(H, T)
     check(lapack, H, T, S, P, Q, Z, ar, ai, be, info)
     if zf > 0:
-        assert np.sum(be == 0) >= round(zf * n)
+        # adjacent zeros on T's diagonal can carry fewer infinite
+        # eigenvalues than zeros: count against LAPACK's exact zeros
+        lbe = lapack.dhgeqz(H, T)[4]
+        assert np.sum(be == 0) >= np.sum(lbe == 0) > 0
 
 
 def test_pdhgeqz_dropin_accumulates_V(pkg, lapack):
