@@ -57,6 +57,7 @@ EXPORTS = (
     "b200qz_solve_host", "b200qz_get_stats", "b200qz_set_params", "b200qz_aed_window",
     "b200qz_chase_window", "b200qz_update", "b200qz_set_param", "b200qz_solve_batched_dev",
     "b200qz_batched_seconds", "b200qz_batched_autotune", "b200qz_batched_config",
+    "b200qz_solve_batched_noalloc",
 )
 
 STAT_NAMES = ("seconds", "iters", "aeds", "aed_deflations", "sweeps", "chains", "windows",
@@ -112,6 +113,8 @@ def lib() -> ctypes.CDLL:
     L.b200qz_batched_autotune.restype = _i
     L.b200qz_batched_config.argtypes = [_vp, _pi, _pi, _pi]
     L.b200qz_batched_config.restype = _i
+    L.b200qz_solve_batched_noalloc.argtypes = [_i, _pi, _pl, _pl] + [_vp] * 9
+    L.b200qz_solve_batched_noalloc.restype = _i
     _lib = L
     return L
 

@@ -14,6 +14,10 @@
 #include <float.h>
 #include <stdint.h>
 
+#include <algorithm>
+#include <mutex>
+
+#include "../../include/b200qz.h"
 #include "kernels.h"
 #include "qz_cta.cuh"
 
@@ -152,4 +156,89 @@ void launch_batch(cudaStream_t st, int grid, int threads, int smem_max, int coun
                                                                 status, counter, smem_max);
 }
 
+// ---------------------------------------------------------------------------
+// Batched solve that allocates nothing.
+//
+// For callers that may not allocate device memory themselves: code that
+// runs inside another library's memory pool or allocator, hosts that
+// reserve the whole device heap up front, or real-time loops where an
+// allocation could block.  The per-batch descriptors and the work-queue
+// counter live in one fixed array in the library's device memory instead
+// of a buffer from cudaMalloc.  Every GPU that loads the library holds the
+// array (kNoAllocBytes) until the process exits.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr int kNoAllocMaxPencils = 4096;
+// moff, eoff (int64), order, n (int32), queue counter
+constexpr size_t kNoAllocBytes = (size_t)kNoAllocMaxPencils * (2 * sizeof(int64_t) + 2 * sizeof(int)) + 256;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+constexpr int kNoAllocMaxDevices = 64;
+struct NoAllocDev {
+  bool ready = false;
+  unsigned char* scratch = nullptr;  // device address of g_noalloc_scratch
+  int sm_count = 0;
+};
+NoAllocDev g_noalloc_dev[kNoAllocMaxDevices];
+std::mutex g_noalloc_mu;
+
+// Once per device, with that device current: the device address of the
+// scratch array (its host-side name is only a stand-in), the SM count and
+// the kernel's shared-memory limit.
+int noalloc_setup(int dev, NoAllocDev** out) {
+  if (dev < 0 || dev >= kNoAllocMaxDevices) return 10001;
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  NoAllocDev& d = g_noalloc_dev[dev];
+  if (!d.ready) {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess) return 10001;
+    if (cudaDeviceGetAttribute(&d.sm_count, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 10001;
+    if (batch_init() != cudaSuccess) return 10001;
+    d.scratch = (unsigned char*)p;
+    d.ready = true;
+  }
+  *out = &d;
+  return 0;
+}
+
+}  // namespace
+
 }  // namespace qz
+
+extern "C" int b200qz_solve_batched_noalloc(int count, const int* n, const long long* moff, const long long* eoff,
+                                            double* h, double* t, double* q, double* z, double* alphar,
+                                            double* alphai, double* beta, int* info, void* stream) {
+  using namespace qz;
+  if (count < 0) return -1;
+  if (count > kNoAllocMaxPencils) return -2;
+  for (int i = 0; i < count; ++i)
+    if (n[i] < 1 || n[i] > 46340) return -3;
+  if (count == 0) return 0;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 10001;
+  NoAllocDev* d = nullptr;
+  if (noalloc_setup(dev, &d) != 0) return 10001;
+  cudaStream_t st = (cudaStream_t)stream;
+  // longest pencils first on the work queue (order held on the stack)
+  int order[kNoAllocMaxPencils];
+  for (int i = 0; i < count; ++i) order[i] = i;
+  std::sort(order, order + count, [&](int a, int b) { return n[a] != n[b] ? n[a] > n[b] : a < b; });
+  int64_t* d_moff = (int64_t*)d->scratch;
+  int64_t* d_eoff = d_moff + kNoAllocMaxPencils;
+  int* d_order = (int*)(d_eoff + kNoAllocMaxPencils);
+  int* d_n = d_order + kNoAllocMaxPencils;
+  int* d_counter = d_n + kNoAllocMaxPencils;
+  // pageable sources: each copy returns once its source has been staged
+  if (cudaMemcpyAsync(d_moff, moff, count * sizeof(int64_t), cudaMemcpyHostToDevice, st) != cudaSuccess ||
+      cudaMemcpyAsync(d_eoff, eoff, count * sizeof(int64_t), cudaMemcpyHostToDevice, st) != cudaSuccess ||
+      cudaMemcpyAsync(d_order, order, count * sizeof(int), cudaMemcpyHostToDevice, st) != cudaSuccess ||
+      cudaMemcpyAsync(d_n, n, count * sizeof(int), cudaMemcpyHostToDevice, st) != cudaSuccess)
+    return 10001;
+  // launch_batch zeroes the queue counter before the kernel starts
+  launch_batch(st, d->sm_count, 128, kBatchSmemMax, count, d_order, d_n, d_moff, d_eoff, h, t, q, z, alphar, alphai,
+               beta, info, d_counter);
+  return cudaGetLastError() == cudaSuccess ? 0 : 10001;
+}
+

@@ -139,6 +139,28 @@ int b200qz_batched_autotune(b200qz_ctx* ctx, int count, const int* n, const long
 /* Current batched configuration. */
 int b200qz_batched_config(const b200qz_ctx* ctx, int* threads, int* smem_max, int* ctas_per_sm);
 
+/* Batched solve that allocates no memory, for callers that cannot call
+ * cudaMalloc: code running inside another library's memory pool or
+ * allocator, hosts that reserve the device heap up front, and loops where
+ * an allocation could block.  Same arguments and results as
+ * b200qz_solve_batched_dev (device buffers h, t, q, z, alphar, alphai,
+ * beta, info; host arrays n, moff, eoff), but no context: it runs on the
+ * current device and on `stream` (a cudaStream_t, NULL for the default
+ * stream) and returns without waiting for the GPU.  The batch descriptors
+ * and the work-queue counter live in one fixed array in the library's
+ * device memory (about 96 KB, held by every GPU that loads the library
+ * until the process exits), so at most 4096 pencils per call: a larger
+ * count returns -2.  The first call on a device sets that device up (it
+ * looks up the array's device address and raises the kernel's shared-
+ * memory limit), so make it before any stream capture.  All calls share
+ * the array: calls whose work overlaps on the GPU (different streams, or
+ * host threads racing) corrupt each other's batches.  Returns 0, -1 bad
+ * count, -2 count above 4096, -3 a size outside 1..46340, or 10001 on a
+ * CUDA error.  No counterpart in the reference. */
+int b200qz_solve_batched_noalloc(int count, const int* n, const long long* moff, const long long* eoff,
+                                 double* h, double* t, double* q, double* z, double* alphar, double* alphai,
+                                 double* beta, int* info, void* stream);
+
 /* ------------------------------------------------------------------ */
 /* Kernel-level entry points (device pointers), for parity tests.       */
 /* ------------------------------------------------------------------ */
