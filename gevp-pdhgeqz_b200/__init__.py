@@ -32,18 +32,19 @@ LIB_PATH = os.path.join(HERE, "libb200qz.so")
 _lib = None
 
 
-def _pencils():
-    name = "gevp_pdhgeqz_b200_pencils"
+def _submodule(base):
+    name = "gevp_pdhgeqz_b200_" + base
     if name in sys.modules:
         return sys.modules[name]
-    spec = importlib.util.spec_from_file_location(name, os.path.join(HERE, "pencils.py"))
+    spec = importlib.util.spec_from_file_location(name, os.path.join(HERE, base + ".py"))
     mod = importlib.util.module_from_spec(spec)
     sys.modules[name] = mod
     spec.loader.exec_module(mod)
     return mod
 
 
-pencils = _pencils()
+pencils = _submodule("pencils")
+shard = _submodule("shard")
 
 _i = ctypes.c_int
 _d = ctypes.c_double

@@ -106,6 +106,11 @@ def batched_ht(count: int = 2048, seed: int = 4, lo: int = 32, hi: int = 512,
     return out
 
 
+def batched_pencil(index: int, n: int, seed: int = 4, zero_frac: float = 0.02):
+    """Pencil ``index`` of the batched workload (same draw as batched_ht)."""
+    return random_ht(int(n), seed * 1_000_003 + int(index), zero_frac)
+
+
 WORKLOADS = {
     "c1": dict(n=1000, seed=0, kind="random", zero_frac=0.0),
     "c2": dict(n=4000, seed=1, kind="random", zero_frac=0.05),
