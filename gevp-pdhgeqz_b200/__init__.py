@@ -45,6 +45,7 @@ def _submodule(base):
 
 pencils = _submodule("pencils")
 shard = _submodule("shard")
+learned = _submodule("learned")
 
 _i = ctypes.c_int
 _d = ctypes.c_double
@@ -58,14 +59,16 @@ EXPORTS = (
     "b200qz_solve_host", "b200qz_get_stats", "b200qz_set_params", "b200qz_aed_window",
     "b200qz_chase_window", "b200qz_update", "b200qz_set_param", "b200qz_solve_batched_dev",
     "b200qz_batched_seconds", "b200qz_batched_autotune", "b200qz_batched_config",
-    "b200qz_solve_batched_noalloc",
+    "b200qz_solve_batched_noalloc", "b200qz_policy_nparams", "b200qz_set_policy", "b200qz_policy_features",
+    "b200qz_mlp_forward", "b200qz_mlp_backward", "b200qz_mlp_train",
 )
 
 STAT_NAMES = ("seconds", "iters", "aeds", "aed_deflations", "sweeps", "chains", "windows",
               "endgames", "inf_steps", "shifts", "update_flops", "window_bytes",
               "ms_scan", "ms_aed", "ms_aed_update", "ms_chase", "ms_chase_update", "ms_inf", "ms_final",
               "ms_aed_smallqz", "ms_aed_reorder", "ms_aed_spike", "ms_aed_hessred", "launches",
-              "aed_failures", "exceptional_sweeps")
+              "aed_failures", "exceptional_sweeps", "remaining", "stop_ktop", "stop_kbot", "last_aed_fraction",
+              "policy_calls")
 
 
 def lib() -> ctypes.CDLL:
@@ -116,6 +119,19 @@ def lib() -> ctypes.CDLL:
     L.b200qz_batched_config.restype = _i
     L.b200qz_solve_batched_noalloc.argtypes = [_i, _pi, _pl, _pl] + [_vp] * 9
     L.b200qz_solve_batched_noalloc.restype = _i
+    _pf = ctypes.POINTER(ctypes.c_float)
+    L.b200qz_policy_nparams.argtypes = []
+    L.b200qz_policy_nparams.restype = _i
+    L.b200qz_set_policy.argtypes = [_vp, _pf, _i]
+    L.b200qz_set_policy.restype = _i
+    L.b200qz_policy_features.argtypes = [_vp, _vp, _i, _i, _i, _d, _pf]
+    L.b200qz_policy_features.restype = _i
+    L.b200qz_mlp_forward.argtypes = [_vp, _vp, _i, _vp, _vp, _vp, _vp]
+    L.b200qz_mlp_forward.restype = _i
+    L.b200qz_mlp_backward.argtypes = [_vp, _vp, _vp, _i] + [_vp] * 8
+    L.b200qz_mlp_backward.restype = _i
+    L.b200qz_mlp_train.argtypes = [_vp, _vp, _vp, _i, _i, ctypes.c_float, _pf]
+    L.b200qz_mlp_train.restype = _i
     _lib = L
     return L
 
@@ -214,6 +230,25 @@ class Solver:
         rc = lib().b200qz_set_param(self._h, name.encode(), float(value))
         if rc != 0:
             raise ValueError("b200qz_set_param(%s=%r) failed: %d" % (name, value, rc))
+
+    def set_policy(self, params) -> None:
+        """Load learned (nw, ns) MLP parameters (float32 array of
+        b200qz_policy_nparams() values); None switches back to the table."""
+        if params is None:
+            rc = lib().b200qz_set_policy(self._h, None, 0)
+        else:
+            p = np.ascontiguousarray(params, dtype=np.float32)
+            rc = lib().b200qz_set_policy(self._h, p.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), p.size)
+        if rc != 0:
+            raise ValueError("b200qz_set_policy failed: %d" % rc)
+
+    def policy_features(self, h_ptr, ld, ktop, kbot, lastfrac=0.0) -> np.ndarray:
+        out = np.zeros(64, dtype=np.float32)
+        rc = lib().b200qz_policy_features(self._h, _vp(h_ptr), ld, ktop, kbot, float(lastfrac),
+                                          out.ctypes.data_as(ctypes.POINTER(ctypes.c_float)))
+        if rc != 0:
+            raise RuntimeError("b200qz_policy_features failed: %d" % rc)
+        return out
 
     def stats(self) -> dict:
         out = np.zeros(len(STAT_NAMES))

@@ -16,6 +16,7 @@
 
 #include "../../include/b200qz.h"
 #include "kernels.h"
+#include "policy.h"
 #include "qz_solver.h"
 
 using namespace qz;
@@ -79,6 +80,10 @@ struct b200qz_ctx {
   double* Vc = nullptr;
   double* shifts = nullptr;    // 3*kAedMax
   double* gscratch = nullptr;  // 2*kAedMax^2 (windows above the smem limit)
+  // learned (nw, ns) policy: parameters, feature vector, activations, output
+  float* pol = nullptr;        // kPolicyParams + kPolicyIn + 2*kPolicyHidden + kPolicyOut floats
+  float* hpol_y = nullptr;     // pinned, kPolicyOut
+  bool pol_on = false;
   double* norms = nullptr;     // 2
   int* dinfo = nullptr;        // 16 ints: [4..6] AED info, [8..12] scan output
   int* hinfo = nullptr;        // pinned mirror
@@ -231,6 +236,33 @@ struct GpuBackend {
     c->kc = wk;
     c->stats.win_bytes += 2.0 * 2.0 * 8.0 * wk * wk + 2.0 * 8.0 * wk * wk;
   }
+  // Learned (nw, ns) for the AED decision on the active block [ktop, kbot]
+  // (features of the subdiagonal profile, then the MLP, on the device).
+  bool policy(int ktop, int kbot, double lastfrac, int* nw, int* ns) {
+    if (!c->pol_on) return false;
+    float* P = c->pol;
+    float* X = P + kPolicyParams;
+    float* A1 = X + kPolicyIn;
+    float* A2 = A1 + kPolicyHidden;
+    float* Y = A2 + kPolicyHidden;
+    launch_policy_features(c->stream, H, ld, ktop, kbot, (float)lastfrac, X);
+    launch_mlp_forward(c->stream, P, X, 1, A1, A2, Y);
+    c->stats.launches += 2;
+    QZ_CK(cudaMemcpyAsync(c->hpol_y, Y, kPolicyOut * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+    QZ_CK(cudaStreamSynchronize(c->stream));
+    if (c->err != cudaSuccess) return false;
+    float y0 = c->hpol_y[0], y1 = c->hpol_y[1];
+    if (!std::isfinite(y0) || !std::isfinite(y1)) return false;
+    y0 = std::min(1.f, std::max(0.f, y0));
+    y1 = std::min(1.f, std::max(0.f, y1));
+    int w = (int)std::lround(kPolicyNwMin + y0 * kPolicyNwSpan);
+    w = std::min(w, (int)kWinSmemMax);
+    int s = (int)std::lround(y1 * w);
+    s = std::max(2, s - s % 2);
+    *nw = w;
+    *ns = s;
+    return true;
+  }
   void inf_top(int f) {
     c->timer.begin(kPhInf, c->stream);
     launch_inf_top(c->stream, H, T, Q, ld, n, f, wantq ? 1 : 0);
@@ -348,11 +380,15 @@ int solve_dev_impl(b200qz_ctx* c, char job, char compq, char compz, int n, int i
   tol.ttol = std::max(DBL_MIN, DBL_EPSILON * std::sqrt(c->hnorms[1]));
   int info = 0;
   if (nh > 0) info = qz_iterate(bk, n, ilo - 1, ihi - 1, c->params, c->stats);
-  if (info < 0) info = 10002;  // non-finite entries appeared (or were given)
-  c->timer.begin(kPhFinal, c->stream);
-  launch_finalize(c->stream, h, t, z, ld, n, wantz ? 1 : 0, ar, ai, be);
-  c->stats.launches += 2;
-  c->timer.end(c->stream);
+  const bool stopped = (info == -2);  // AED limit reached (tuning traces)
+  if (stopped) info = 10003;
+  else if (info < 0) info = 10002;  // non-finite entries appeared (or were given)
+  if (!stopped) {
+    c->timer.begin(kPhFinal, c->stream);
+    launch_finalize(c->stream, h, t, z, ld, n, wantz ? 1 : 0, ar, ai, be);
+    c->stats.launches += 2;
+    c->timer.end(c->stream);
+  }
   QZ_CK(cudaGetLastError());
   QZ_CK(cudaEventRecord(c->ev1, c->stream));
   QZ_CK(cudaEventSynchronize(c->ev1));
@@ -387,6 +423,9 @@ int b200qz_create(b200qz_ctx** out, int device) {
   if (e == cudaSuccess) e = cudaMalloc(&c->Vc, w2);
   if (e == cudaSuccess) e = cudaMalloc(&c->shifts, 3 * kAedMax * sizeof(double));
   if (e == cudaSuccess) e = cudaMalloc(&c->gscratch, 2 * a2);
+  if (e == cudaSuccess)
+    e = cudaMalloc(&c->pol, (kPolicyParams + kPolicyIn + 2 * kPolicyHidden + kPolicyOut) * sizeof(float));
+  if (e == cudaSuccess) e = cudaMallocHost(&c->hpol_y, kPolicyOut * sizeof(float));
   if (e == cudaSuccess) e = cudaMalloc(&c->norms, 2 * sizeof(double));
   if (e == cudaSuccess) e = cudaMalloc(&c->dinfo, 16 * sizeof(int));
   if (e == cudaSuccess) e = cudaMallocHost(&c->hinfo, 16 * sizeof(int));
@@ -410,6 +449,8 @@ void b200qz_destroy(b200qz_ctx* c) {
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   cudaFree(c->Ua); cudaFree(c->Va); cudaFree(c->Uc); cudaFree(c->Vc);
+  if (c->pol) cudaFree(c->pol);
+  if (c->hpol_y) cudaFreeHost(c->hpol_y);
   cudaFree(c->shifts); cudaFree(c->gscratch); cudaFree(c->norms); cudaFree(c->dinfo);
   if (c->hinfo) cudaFreeHost(c->hinfo);
   if (c->hshifts) cudaFreeHost(c->hshifts);
@@ -458,6 +499,7 @@ int b200qz_set_param(b200qz_ctx* c, const char* name, double value) {
   else if (k == "aed_nskip") { if (v < 0) return -3; P.aed_nskip = v; }
   else if (k == "max_wave") { if (v < 1 || v > kMaxWave) return -3; P.max_wave = v; }
   else if (k == "stall_limit") { if (v < 1) return -3; P.stall_limit = v; }
+  else if (k == "aed_limit") { P.aed_limit = v < 0 ? -1 : v; }
   else if (k == "aed_threads") { if (v != 32 && v != 64 && v != 128) return -3; P.aed_threads = v; }
   else return -2;
   return 0;
@@ -536,13 +578,14 @@ int b200qz_get_stats(const b200qz_ctx* c, double* out, int nout) {
   if (!c || !out) return 0;
   const SolveStats& s = c->stats;
   const double* ph = c->timer.ms;
-  double v[26] = {c->seconds, (double)s.iters, (double)s.aeds, (double)s.aed_defl, (double)s.sweeps,
+  double v[31] = {c->seconds, (double)s.iters, (double)s.aeds, (double)s.aed_defl, (double)s.sweeps,
                   (double)s.chains, (double)s.windows, (double)s.endgames, (double)s.infs, (double)s.shifts,
                   s.upd_flops, s.win_bytes,
                   ph[kPhScan], ph[kPhAed], ph[kPhAedUpd], ph[kPhChase], ph[kPhChaseUpd], ph[kPhInf], ph[kPhFinal],
                   c->aed_ms[0], c->aed_ms[1], c->aed_ms[2], c->aed_ms[3], (double)s.launches,
-                  (double)s.aed_fail, (double)s.exceptional};
-  int k = std::min(nout, 26);
+                  (double)s.aed_fail, (double)s.exceptional, (double)s.remaining, (double)s.stop_ktop,
+                  (double)s.stop_kbot, s.last_frac, (double)s.policy_calls};
+  int k = std::min(nout, 31);
   for (int i = 0; i < k; ++i) out[i] = v[i];
   return k;
 }
@@ -778,6 +821,88 @@ extern "C" int b200qz_batched_config(const b200qz_ctx* c, int* threads, int* sme
   if (smem_max) *smem_max = c->batch_smem_max;
   if (ctas_per_sm) *ctas_per_sm = c->batch_ctas_per_sm;
   return 0;
+}
+
+// ---------------------------------------------------------------------------
+// Learned (nw, ns) policy
+// ---------------------------------------------------------------------------
+extern "C" int b200qz_policy_nparams(void) { return kPolicyParams; }
+
+extern "C" int b200qz_set_policy(b200qz_ctx* c, const float* params, int nparams) {
+  if (!c) return 10001;
+  if (nparams == 0 || params == nullptr) {
+    c->pol_on = false;
+    return 0;
+  }
+  if (nparams != kPolicyParams) return -3;
+  for (int i = 0; i < nparams; ++i)
+    if (!std::isfinite(params[i])) return -2;
+  c->err = cudaSuccess;
+  QZ_CK(cudaSetDevice(c->device));
+  QZ_CK(cudaMemcpy(c->pol, params, kPolicyParams * sizeof(float), cudaMemcpyHostToDevice));
+  if (c->err != cudaSuccess) return 10001;
+  c->pol_on = true;
+  return 0;
+}
+
+extern "C" int b200qz_policy_features(b200qz_ctx* c, const double* h, int ld, int ktop, int kbot, double lastfrac,
+                                      float* out) {
+  if (!c || !out) return 10001;
+  if (ktop < 0 || kbot <= ktop || ld < kbot + 1) return -1;
+  c->err = cudaSuccess;
+  QZ_CK(cudaSetDevice(c->device));
+  float* X = c->pol + kPolicyParams;
+  launch_policy_features(c->stream, h, ld, ktop, kbot, (float)lastfrac, X);
+  QZ_CK(cudaMemcpyAsync(out, X, kPolicyIn * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+  QZ_CK(cudaStreamSynchronize(c->stream));
+  return c->err == cudaSuccess ? 0 : 10001;
+}
+
+extern "C" int b200qz_mlp_forward(const float* params, const float* x, int batch, float* a1, float* a2, float* y,
+                                  void* stream) {
+  if (batch < 0) return -1;
+  launch_mlp_forward((cudaStream_t)stream, params, x, batch, a1, a2, y);
+  return cudaGetLastError() == cudaSuccess ? 0 : 10001;
+}
+
+extern "C" int b200qz_mlp_backward(const float* params, const float* x, const float* target, int batch,
+                                   const float* a1, const float* a2, const float* y, float* dy, float* d2,
+                                   float* d1, float* grad, void* stream) {
+  if (batch < 0) return -1;
+  launch_mlp_backward((cudaStream_t)stream, params, x, target, batch, a1, a2, y, dy, d2, d1, grad);
+  return cudaGetLastError() == cudaSuccess ? 0 : 10001;
+}
+
+extern "C" int b200qz_mlp_train(float* params, const float* x, const float* target, int batch, int epochs, float lr,
+                                float* loss) {
+  if (batch < 1 || epochs < 0) return -1;
+  cudaStream_t st = nullptr;
+  size_t nf = (size_t)batch * (2 * kPolicyHidden + kPolicyHidden * 2 + 2 * kPolicyOut) + 3 * kPolicyParams + 1;
+  float* w = nullptr;
+  if (cudaMalloc(&w, nf * sizeof(float)) != cudaSuccess) return 10001;
+  float* A1 = w;
+  float* A2 = A1 + (size_t)batch * kPolicyHidden;
+  float* D1 = A2 + (size_t)batch * kPolicyHidden;
+  float* D2 = D1 + (size_t)batch * kPolicyHidden;
+  float* Y = D2 + (size_t)batch * kPolicyHidden;
+  float* DY = Y + (size_t)batch * kPolicyOut;
+  float* G = DY + (size_t)batch * kPolicyOut;
+  float* M = G + kPolicyParams;
+  float* V = M + kPolicyParams;
+  float* L = V + kPolicyParams;
+  cudaMemsetAsync(M, 0, 2 * kPolicyParams * sizeof(float), st);
+  for (int e = 1; e <= epochs; ++e) {
+    launch_mlp_forward(st, params, x, batch, A1, A2, Y);
+    launch_mlp_backward(st, params, x, target, batch, A1, A2, Y, DY, D2, D1, G);
+    launch_adam(st, params, G, M, V, lr, e);
+  }
+  launch_mlp_forward(st, params, x, batch, A1, A2, Y);
+  launch_mse(st, Y, target, batch * kPolicyOut, L);
+  float hl = 0.f;
+  cudaError_t err = cudaMemcpy(&hl, L, sizeof(float), cudaMemcpyDeviceToHost);
+  cudaFree(w);
+  if (loss) *loss = hl;
+  return err == cudaSuccess && cudaGetLastError() == cudaSuccess ? 0 : 10001;
 }
 
 // ---------------------------------------------------------------------------

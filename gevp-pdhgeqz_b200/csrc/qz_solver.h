@@ -35,6 +35,8 @@ struct SolveParams {
   int max_wave = 8;      // chains chased concurrently (one CTA each)
   int stall_limit = 300; // iterations without deflation before giving up
   int aed_threads = 128; // threads of the AED / endgame window kernel (32: one warp)
+  int aed_limit = -1;    // >= 0: stop before the AED after this many AEDs
+                         // (tuning traces; the solve then returns -2)
 };
 
 struct SolveStats {
@@ -45,6 +47,10 @@ struct SolveStats {
   int64_t launches = 0;    // kernel launches issued by the solve
   int64_t aed_fail = 0;    // AED windows whose small QZ did not converge
   int64_t exceptional = 0; // sweeps with exceptional shifts
+  int64_t remaining = 0;   // rows of the active part left at exit (0: converged)
+  int stop_ktop = -1, stop_kbot = -1;  // active block where an AED limit stopped the solve
+  double last_frac = 0.0;  // deflated fraction of the last AED window
+  int64_t policy_calls = 0;  // AED decisions taken by the learned policy
 };
 
 // reference shift-count table (piparmq.f:504-533)
@@ -173,6 +179,8 @@ inline void plan_chain(int ktop, int kbot, int W, int nb, const ShiftPair* sp, i
 //   void update_wave(const WinPlan* const* wins, int n) // far updates of those windows
 //   void inf_window(int w, int wk, int top, int jz, int stop, bool deflate)
 //   void inf_top(int ktop)
+//   bool policy(int ktop, int kbot, double lastfrac, int* nw, int* ns)
+//                                                       // learned (nw, ns); false: use the table
 template <class BK>
 int qz_iterate(BK& bk, int n, int ilo, int ihi, const SolveParams& P, SolveStats& S) {
   int ifirst = ilo, kbot = ihi;
@@ -185,17 +193,21 @@ int qz_iterate(BK& bk, int n, int ilo, int ihi, const SolveParams& P, SolveStats
   int info3[3];
   int stall = 0;             // iterations since the last deflation
   int last_kbot = kbot, last_ktop = -1;
+  auto done = [&](int r) {
+    S.remaining = (kbot >= ifirst) ? kbot - ifirst + 1 : 0;
+    return r;
+  };
   for (int64_t it = 0; it < maxit; ++it) {
-    if (kbot < ifirst) return 0;
+    if (kbot < ifirst) return done(0);
     ++S.iters;
     bk.scan(ifirst, kbot, scan_out);
     int ktop = scan_out[0];
     int ninf = scan_out[1];
-    if (scan_out[4]) return -1;  // non-finite entry in the active block
+    if (scan_out[4]) return done(-1);  // non-finite entry in the active block
     if (kbot != last_kbot || ktop != last_ktop) stall = 0; else ++stall;
     last_kbot = kbot;
     last_ktop = ktop;
-    if (stall > P.stall_limit) return kbot + 1;
+    if (stall > P.stall_limit) return done(kbot + 1);
     if (P.verbose)
       std::fprintf(stderr, "[b200qz] it=%lld ktop=%d kbot=%d ninf=%d\n", (long long)it, ktop, kbot, ninf);
     if (ktop == kbot) {
@@ -232,13 +244,27 @@ int qz_iterate(BK& bk, int n, int ilo, int ihi, const SolveParams& P, SolveStats
       // small block: one CTA solves it (PDHGEQZ4 -> KKQZ role)
       ++S.endgames;
       bk.aed(ktop, ktop, kbot, info3, sh.data());
-      if (info3[1] != 0) return kbot + 1;
+      if (info3[1] != 0) return done(kbot + 1);
       bk.update(ktop, nh, 0);
       kbot = ktop - 1;
       continue;
     }
     // ---- aggressive early deflation ----
+    if (P.aed_limit >= 0 && S.aeds >= P.aed_limit) {
+      S.stop_ktop = ktop;
+      S.stop_kbot = kbot;
+      return done(-2);
+    }
     int nw = std::min(P.nw_max, nh);
+    int ns_pol = -1;
+    {
+      int pnw = 0, pns = 0;
+      if (bk.policy(ktop, kbot, S.last_frac, &pnw, &pns)) {
+        nw = std::max(std::min(4, nh), std::min(pnw, nw));
+        ns_pol = pns;
+        ++S.policy_calls;
+      }
+    }
     int kwtop = kbot - nw + 1;
     ++S.aeds;
     bk.aed(ktop, kwtop, kbot, info3, sh.data());
@@ -255,12 +281,14 @@ int qz_iterate(BK& bk, int n, int ilo, int ihi, const SolveParams& P, SolveStats
     // the next AED sees a different window (PDHGEQZ0.f:944-949)
     if (info3[1] != 0) ++S.aed_fail;
     S.aed_defl += nd;
+    S.last_frac = (double)nd / (double)nw;
     kbot -= nd;
     if (kbot < ktop) continue;
     int nib = (P.nibble >= 0) ? P.nibble : nibble_table(nh);
     if (info3[1] == 0 && 100 * nd > nib * nw) continue;
     // ---- multishift sweep ----
     int nsmax = (P.ns_max > 0) ? P.ns_max : ns_table(nh);
+    if (ns_pol > 0) nsmax = ns_pol;
     int ns = std::min(nsmax, m - (m % 2));
     if (ns < 2) continue;
     pair_shifts(sh.data(), sh.data() + m, sh.data() + 2 * m, m, ns, pairs);
@@ -325,7 +353,7 @@ int qz_iterate(BK& bk, int n, int ilo, int ihi, const SolveParams& P, SolveStats
       }
     }
   }
-  return kbot + 1;
+  return done(kbot + 1);
 }
 
 }  // namespace qz

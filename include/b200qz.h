@@ -110,6 +110,48 @@ int b200qz_set_params(b200qz_ctx* ctx, int nw_max, int w_chase, int nmin, int ni
 int b200qz_set_param(b200qz_ctx* ctx, const char* name, double value);
 
 /* ------------------------------------------------------------------ */
+/* Learned (nw, ns) policy: replaces the fixed tuning table of          */
+/* PIPARMQ / PILAENVX (src/pdhgeqz/piparmq.f:438-535) at every AED       */
+/* decision; the table stays the fallback.                              */
+/* ------------------------------------------------------------------ */
+
+/* Number of FP32 parameters of the 64-128-128-2 MLP (flat, row-major
+ * out x in: W1[128x64] b1[128] W2[128x128] b2[128] W3[2x128] b3[2]). */
+int b200qz_policy_nparams(void);
+
+/* Load the MLP's parameters (host array of b200qz_policy_nparams() floats)
+ * into the context; from then on every AED decision takes nw and ns from
+ * the network (outputs y0, y1 clamped to [0,1]: nw = 16 + 64*y0, at most
+ * the AED window limit; ns = y1*nw, even, at least 2).  params = NULL or
+ * nparams = 0 switches back to the table.  Returns 0, -2 (non-finite
+ * parameter), -3 (wrong count) or 10001. */
+int b200qz_set_policy(b200qz_ctx* ctx, const float* params, int nparams);
+
+/* The 64 features of the active block [ktop, kbot] (0-based) of the device
+ * matrix h (leading dimension ld): 62 log-spaced bins over the distance
+ * from the bottom of the mean -log10(|h(k+1,k)|/(|h(k,k)|+|h(k+1,k+1)|))/16
+ * (clipped to [0,1]), log2(nh)/14 and lastfrac (the deflated fraction of
+ * the previous AED window).  out: host array of 64 floats. */
+int b200qz_policy_features(b200qz_ctx* ctx, const double* h, int ld, int ktop, int kbot, double lastfrac,
+                           float* out);
+
+/* MLP forward and backward on device buffers (FP32, stream = cudaStream_t
+ * or NULL): x[batch x 64], a1, a2 [batch x 128] activations, y[batch x 2];
+ * the backward pass of the loss mean((y - target)^2) over batch x 2 fills
+ * dy[batch x 2], d2, d1 [batch x 128] and grad[nparams]. */
+int b200qz_mlp_forward(const float* params, const float* x, int batch, float* a1, float* a2, float* y,
+                       void* stream);
+int b200qz_mlp_backward(const float* params, const float* x, const float* target, int batch, const float* a1,
+                        const float* a2, const float* y, float* dy, float* d2, float* d1, float* grad,
+                        void* stream);
+
+/* Train the MLP in place (params: device, nparams floats) with Adam on the
+ * device for `epochs` full-batch steps; loss (host, may be NULL) receives
+ * the final mean squared error. */
+int b200qz_mlp_train(float* params, const float* x, const float* target, int batch, int epochs, float lr,
+                     float* loss);
+
+/* ------------------------------------------------------------------ */
 /* Batched independent pencils (sizes may differ).                      */
 /* ------------------------------------------------------------------ */
 
