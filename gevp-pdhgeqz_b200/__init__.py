@@ -60,7 +60,7 @@ EXPORTS = (
     "b200qz_chase_window", "b200qz_update", "b200qz_set_param", "b200qz_solve_batched_dev",
     "b200qz_batched_seconds", "b200qz_batched_autotune", "b200qz_batched_config",
     "b200qz_solve_batched_noalloc", "b200qz_policy_nparams", "b200qz_set_policy", "b200qz_policy_features",
-    "b200qz_mlp_forward", "b200qz_mlp_backward", "b200qz_mlp_train",
+    "b200qz_mlp_forward", "b200qz_mlp_backward", "b200qz_mlp_train", "b200qz_update_split",
 )
 
 STAT_NAMES = ("seconds", "iters", "aeds", "aed_deflations", "sweeps", "chains", "windows",
@@ -108,6 +108,8 @@ def lib() -> ctypes.CDLL:
     L.b200qz_set_param.argtypes = [_vp, ctypes.c_char_p, _d]
     L.b200qz_update.restype = _i
     L.b200qz_update.argtypes = [_vp, _c, _vp, _i, _i, _i, _i, _vp, _i, _i]
+    L.b200qz_update_split.argtypes = [_vp, _c, _vp, _i, _i, _i, _i, _vp, _i, _i, _i]
+    L.b200qz_update_split.restype = _i
     _pl = ctypes.POINTER(ctypes.c_longlong)
     L.b200qz_solve_batched_dev.argtypes = [_vp, _i, _pi, _pl, _pl] + [_vp] * 8
     L.b200qz_solve_batched_dev.restype = _i

@@ -16,6 +16,7 @@
 
 #include "../../include/b200qz.h"
 #include "kernels.h"
+#include "ozaki.h"
 #include "policy.h"
 #include "qz_solver.h"
 
@@ -84,6 +85,9 @@ struct b200qz_ctx {
   float* pol = nullptr;        // kPolicyParams + kPolicyIn + 2*kPolicyHidden + kPolicyOut floats
   float* hpol_y = nullptr;     // pinned, kPolicyOut
   bool pol_on = false;
+  // split-precision updates: prepared digits of up to kOzMaxFac factors
+  uint8_t* ozb = nullptr;
+  int* ozerr = nullptr;        // device flag: a tensor-core wait timed out
   double* norms = nullptr;     // 2
   int* dinfo = nullptr;        // 16 ints: [4..6] AED info, [8..12] scan output
   int* hinfo = nullptr;        // pinned mirror
@@ -236,6 +240,52 @@ struct GpuBackend {
     c->kc = wk;
     c->stats.win_bytes += 2.0 * 2.0 * 8.0 * wk * wk + 2.0 * 8.0 * wk * wk;
   }
+  // The same updates through the split-precision (INT8 Ozaki) tensor-core
+  // kernels: digits of every factor prepared once, then one launch for the
+  // left updates and one for the right updates.
+  void update_list_split(const int* w, const int* wk, int nwin, const double* Ub, const double* Vb, int64_t ustride,
+                         int phase) {
+    OzPrep P;
+    P.nfac = 0;
+    P.out = c->ozb;
+    OzBatch L, R;
+    L.njobs = 0;
+    R.njobs = 0;
+    L.bslices = R.bslices = c->ozb;
+    L.err = R.err = c->ozerr;
+    auto job = [&](OzBatch& B, double* M, int r0, int c0, int len, int k, int left, int fac) {
+      OzJob& j = B.job[B.njobs++];
+      j.M = M; j.ld = ld; j.r0 = r0; j.c0 = c0; j.len = len; j.k = k; j.left = left; j.fac = fac;
+      j.tiles = (len + 127) / 128;
+    };
+    for (int i = 0; i < nwin; ++i) {
+      const int k = wk[i], w0 = w[i];
+      const int fu = P.nfac, fv = P.nfac + 1;
+      P.W[fu] = Ub + i * ustride; P.ldw[fu] = k; P.k[fu] = k;
+      P.W[fv] = Vb + i * ustride; P.ldw[fv] = k; P.k[fv] = k;
+      P.nfac += 2;
+      const int right_len = n - (w0 + k);
+      if (right_len > 0) {
+        job(L, H, w0, w0 + k, right_len, k, 1, fu);
+        job(L, T, w0, w0 + k, right_len, k, 1, fu);
+        c->stats.upd_flops += 2.0 * 2.0 * k * k * right_len;
+      }
+      if (w0 > 0) {
+        job(R, H, 0, w0, w0, k, 0, fv);
+        job(R, T, 0, w0, w0, k, 0, fv);
+        c->stats.upd_flops += 2.0 * 2.0 * k * k * w0;
+      }
+      if (wantq) { job(R, Q, 0, w0, n, k, 0, fu); c->stats.upd_flops += 2.0 * k * k * n; }
+      if (wantz) { job(R, Z, 0, w0, n, k, 0, fv); c->stats.upd_flops += 2.0 * k * k * n; }
+    }
+    c->timer.begin(phase, c->stream);
+    const int sl = c->params.split;
+    launch_ozaki_prep(c->stream, P, sl);
+    c->stats.launches += 1;
+    if (L.njobs) { launch_ozaki_update(c->stream, L, sl); c->stats.launches += 1; }
+    if (R.njobs) { launch_ozaki_update(c->stream, R, sl); c->stats.launches += 1; }
+    c->timer.end(c->stream);
+  }
   // Learned (nw, ns) for the AED decision on the active block [ktop, kbot]
   // (features of the subdiagonal profile, then the MLP, on the device).
   bool policy(int ktop, int kbot, double lastfrac, int* nw, int* ns) {
@@ -281,6 +331,13 @@ struct GpuBackend {
   // right update (rows above a window, its columns; Q and Z columns).
   void update_list(const int* w, const int* wk, int nwin, const double* Ub, const double* Vb, int64_t ustride,
                    int phase) {
+    bool split = c->params.split != 0 && nwin <= kOzMaxFac / 2;
+    for (int i = 0; i < nwin && split; ++i)
+      if (wk[i] > kOzMaxK) split = false;
+    if (split) {
+      update_list_split(w, wk, nwin, Ub, Vb, ustride, phase);
+      return;
+    }
     UpdBatch L, R;
     L.njobs = 0;
     R.njobs = 0;
@@ -426,6 +483,10 @@ int b200qz_create(b200qz_ctx** out, int device) {
   if (e == cudaSuccess)
     e = cudaMalloc(&c->pol, (kPolicyParams + kPolicyIn + 2 * kPolicyHidden + kPolicyOut) * sizeof(float));
   if (e == cudaSuccess) e = cudaMallocHost(&c->hpol_y, kPolicyOut * sizeof(float));
+  if (e == cudaSuccess) e = cudaMalloc(&c->ozb, kOzMaxFac * kOzFacBytes);
+  if (e == cudaSuccess) e = cudaMalloc(&c->ozerr, sizeof(int));
+  if (e == cudaSuccess) e = cudaMemset(c->ozerr, 0, sizeof(int));
+  if (e == cudaSuccess) e = ozaki_init();
   if (e == cudaSuccess) e = cudaMalloc(&c->norms, 2 * sizeof(double));
   if (e == cudaSuccess) e = cudaMalloc(&c->dinfo, 16 * sizeof(int));
   if (e == cudaSuccess) e = cudaMallocHost(&c->hinfo, 16 * sizeof(int));
@@ -450,6 +511,8 @@ void b200qz_destroy(b200qz_ctx* c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   cudaFree(c->Ua); cudaFree(c->Va); cudaFree(c->Uc); cudaFree(c->Vc);
   if (c->pol) cudaFree(c->pol);
+  if (c->ozb) cudaFree(c->ozb);
+  if (c->ozerr) cudaFree(c->ozerr);
   if (c->hpol_y) cudaFreeHost(c->hpol_y);
   cudaFree(c->shifts); cudaFree(c->gscratch); cudaFree(c->norms); cudaFree(c->dinfo);
   if (c->hinfo) cudaFreeHost(c->hinfo);
@@ -500,6 +563,7 @@ int b200qz_set_param(b200qz_ctx* c, const char* name, double value) {
   else if (k == "max_wave") { if (v < 1 || v > kMaxWave) return -3; P.max_wave = v; }
   else if (k == "stall_limit") { if (v < 1) return -3; P.stall_limit = v; }
   else if (k == "aed_limit") { P.aed_limit = v < 0 ? -1 : v; }
+  else if (k == "split") { if (v != 0 && v != 7 && v != 8) return -3; P.split = v; }
   else if (k == "aed_threads") { if (v != 32 && v != 64 && v != 128) return -3; P.aed_threads = v; }
   else return -2;
   return 0;
@@ -662,6 +726,30 @@ int b200qz_update(b200qz_ctx* c, char side, double* m, int ldm, int r0, int c0, 
   QZ_CK(cudaGetLastError());
   QZ_CK(cudaStreamSynchronize(c->stream));
   return c->err == cudaSuccess ? 0 : 10001;
+}
+
+int b200qz_update_split(b200qz_ctx* c, char side, double* m, int ldm, int r0, int c0, int len, const double* w,
+                        int ldw, int k, int slices) {
+  if (!c) return 10001;
+  if (k < 1 || k > kOzMaxK || len < 0 || (slices != 7 && slices != 8)) return -1;
+  if (!is(side, 'L') && !is(side, 'R')) return -2;
+  c->err = cudaSuccess;
+  QZ_CK(cudaSetDevice(c->device));
+  OzPrep P;
+  P.nfac = 1; P.W[0] = w; P.ldw[0] = ldw; P.k[0] = k; P.out = c->ozb;
+  OzBatch B;
+  B.njobs = 1; B.bslices = c->ozb; B.err = c->ozerr;
+  OzJob& j = B.job[0];
+  j.M = m; j.ld = ldm; j.r0 = r0; j.c0 = c0; j.len = len; j.k = k; j.left = is(side, 'L') ? 1 : 0; j.fac = 0;
+  j.tiles = (len + 127) / 128;
+  launch_ozaki_prep(c->stream, P, slices);
+  launch_ozaki_update(c->stream, B, slices);
+  QZ_CK(cudaGetLastError());
+  int herr = 0;
+  QZ_CK(cudaMemcpyAsync(&herr, c->ozerr, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  QZ_CK(cudaStreamSynchronize(c->stream));
+  if (c->err != cudaSuccess) return 10001;
+  return herr ? 10004 : 0;
 }
 
 // ---------------------------------------------------------------------------

@@ -1,0 +1,380 @@
+// Split-precision off-diagonal updates: FP64 products recovered from INT8
+// tensor-core slices (Ozaki scheme) on the 5th-generation tensor cores.
+//
+// Role in the reference: the PDGEMM / DGEMM updates of PDHGEQZ6
+// (PDHGEQZ6.f:276-380, 1x1 grid) and after AED (PDHGEQZ0.f:776-864,
+// PDHGEQZ3.f:1630-1726):
+//   left :  M(r0:r0+k, c0:c0+L) <- W^T * M(r0:r0+k, c0:c0+L)
+//   right:  M(r0:r0+L, c0:c0+k) <- M(r0:r0+L, c0:c0+k) * W
+// Both are computed as one product D = A * W with A an L x k tile of the
+// slab (A = X^T for the left update, A = X for the right update).
+//
+// Scheme.  Each row i of A is scaled by 2^-e_i (e_i: exponent of its
+// largest entry) and each column j of W by 2^-f_j, so every entry x lies in
+// (-1, 1), and split into S (7 or 8) signed 7-bit digits
+//   x = sum_{s=1..S} q_s 2^(-6-7(s-1)) + r,   |q_s| <= 64,  |r| <= 2^(-7S).
+// With int8 digit matrices QA_s, QB_t the product is
+//   D(i,j) = 2^(e_i+f_j-12) * sum_{d=2..S+1} 2^(-7(d-2)) * acc_d(i,j),
+//   acc_d = sum_{s+t=d} QA_s * QB_t   (S(S+1)/2 slice products, exact in
+// int32: 28 for S = 7, 36 for S = 8); the products with s+t > S+1 are
+// dropped, at the same order as r.  S = 7 leaves errors near 2^-48 of the
+// row and column scales, S = 8 near 2^-55.  acc_d is formed on the tensor cores (tcgen05.mma kind::i8, A and
+// B from shared memory, accumulators in TMEM), read back with tcgen05.ld and
+// combined in FP64 by Horner's rule from d = 8 down.
+//
+// Kernels
+//   k_ozaki_prep    one CTA per factor W: column scales and the seven digit
+//                   matrices of W in the tensor cores' K-major layout
+//   k_ozaki_update  one CTA per 128-row tile of a slab: stages the FP64
+//                   tile in two halves and slices it, runs S(S+1)/2 x (k/32)
+//                   MMAs per 32-column output chunk into S TMEM
+//                   accumulators, combines them, and writes the chunk back
+//                   in place
+//
+// Shared-memory operand layout (K-major, no swizzle): 8-row x 16-byte core
+// matrices; rows of a core matrix 16 B apart, row groups SBO = 128 B apart,
+// 16-wide K chunks LBO apart (2048 B for A's 128 rows, kp/8 * 128 B for B).
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#include "ozaki.h"
+
+namespace qz {
+
+namespace {
+
+constexpr int kOzThreads = 128;
+constexpr int kOzRows = 128;  // MMA M
+constexpr int kOzChunkN = 32; // output columns per TMEM pass
+constexpr int kOzTmemCols = 256;  // (slices) accumulators x 32 columns
+constexpr uint32_t kOzSpinLimit = 1u << 22;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+// K-major, no-swizzle shared-memory matrix descriptor (Blackwell version 1)
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
+  d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+  d |= (uint64_t)1 << 46;
+  return d;
+}
+
+// instruction descriptor: S8 x S8 -> S32, both K-major, M = 128
+__device__ __forceinline__ uint32_t idesc_i8(int n) {
+  return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(kOzRows >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_i8(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+      "l"(a), "l"(b), "r"(idesc), "r"(acc));
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, int32_t (&v)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+        "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+      : "r"(taddr));
+}
+
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// S signed 7-bit digits of 16 values x (|x| < 1), packed per digit into 16 bytes.
+template <int S>
+__device__ __forceinline__ void digits16(const double (&x)[16], uint4 (&out)[S]) {
+  uint32_t w[S][4];
+#pragma unroll
+  for (int s = 0; s < S; ++s)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) w[s][q] = 0u;
+#pragma unroll
+  for (int e = 0; e < 16; ++e) {
+    double r = x[e] * 64.0;
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+      const double q = rint(r);
+      r = (r - q) * 128.0;
+      w[s][e >> 2] |= ((uint32_t)(uint8_t)(int8_t)(int)q) << (8 * (e & 3));
+    }
+  }
+#pragma unroll
+  for (int s = 0; s < S; ++s) out[s] = make_uint4(w[s][0], w[s][1], w[s][2], w[s][3]);
+}
+
+// ---------------------------------------------------------------------------
+template <int S>
+__global__ void __launch_bounds__(kOzThreads) k_ozaki_prep(OzPrep P) {
+  const int f = blockIdx.x;
+  const double* W = P.W[f];
+  const int ldw = P.ldw[f];
+  const int k = P.k[f];
+  const int kp = (k + 15) & ~15;
+  const int Kp = (k + 31) & ~31;
+  const int kc_n = Kp / 16;
+  uint8_t* out = P.out + (size_t)f * kOzFacBytes;
+  int* scale = (int*)(out + (size_t)S * kp * Kp);
+  for (int j = threadIdx.x; j < kp; j += blockDim.x) {
+    double mx = 0.0;
+    if (j < k)
+      for (int kk = 0; kk < k; ++kk) mx = fmax(mx, fabs(W[kk + (int64_t)j * ldw]));
+    int e = 0;
+    if (mx > 0.0) frexp(mx, &e);
+    scale[j] = e;
+    for (int kc = 0; kc < kc_n; ++kc) {
+      double x[16];
+#pragma unroll
+      for (int t = 0; t < 16; ++t) {
+        const int kk = kc * 16 + t;
+        x[t] = (j < k && kk < k) ? ldexp(W[kk + (int64_t)j * ldw], -e) : 0.0;
+      }
+      uint4 d[S];
+      digits16<S>(x, d);
+      const size_t off = (size_t)(kc * (kp / 8) + j / 8) * 128 + (j % 8) * 16;
+#pragma unroll
+      for (int s = 0; s < S; ++s) *(uint4*)(out + (size_t)s * kp * Kp + off) = d[s];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int oz_find_job(const OzBatch& B, int& tile) {
+  int t = blockIdx.x;
+  for (int j = 0; j < B.njobs; ++j) {
+    if (t < B.job[j].tiles) { tile = t; return j; }
+    t -= B.job[j].tiles;
+  }
+  tile = -1;
+  return -1;
+}
+
+// shared memory: A digits (S x 128 x Kp) | B digits + scales | FP64 staging
+// (64 input rows x (k+1), or one 128 x 33 output chunk)
+constexpr int kOzStageDoubles = 64 * (kOzMaxK + 1);
+static_assert(kOzStageDoubles >= kOzRows * (kOzChunkN + 1), "staging too small");
+
+template <int S>
+__global__ void __launch_bounds__(kOzThreads, 1) k_ozaki_update(const OzBatch B) {
+  extern __shared__ __align__(1024) uint8_t oz_smem[];
+  __shared__ uint64_t mbar;
+  __shared__ uint32_t tmem_base_s;
+  __shared__ int escale[kOzRows];
+  int tile;
+  const int jb = oz_find_job(B, tile);
+  if (jb < 0) return;
+  const OzJob J = B.job[jb];
+  const int k = J.k;
+  const int kp = (k + 15) & ~15;
+  const int Kp = (k + 31) & ~31;
+  const int kc_n = Kp / 16;
+  const int ldx = k + 1;
+  const int row0 = tile * kOzRows;
+  const int nrow = min(kOzRows, J.len - row0);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+  uint8_t* As = oz_smem;                                  // S x 128 x Kp
+  uint8_t* Bs = As + (size_t)S * kOzRows * kOzMaxKp;      // S x kp x Kp, then kp ints
+  double* Xs = (double*)(Bs + kOzFacBytes);               // staging
+  const uint8_t* Bg = B.bslices + (size_t)J.fac * kOzFacBytes;
+  const int* fscale = (const int*)(Bs + (size_t)S * kp * Kp);
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base_s)),
+                 "r"(kOzTmemCols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&mbar)), "r"(1));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  // B digits and column scales (prepared once per factor)
+  {
+    const int nb = (S * kp * Kp + 4 * kp) / 16;
+    const uint4* src = (const uint4*)Bg;
+    uint4* dst = (uint4*)Bs;
+    for (int i = tid; i < nb; i += kOzThreads) dst[i] = src[i];
+  }
+  // A: two halves of 64 rows staged in FP64 (coalesced), then sliced;
+  // thread t takes row (t & 63) of the half and every other K chunk
+  for (int h = 0; h < 2; ++h) {
+    const int rb = 64 * h;
+    if (J.left) {
+      // A(i, kk) = M(r0 + kk, c0 + row0 + i): contiguous in kk
+      for (int idx = tid; idx < 64 * k; idx += kOzThreads) {
+        const int kk = idx % k, i = idx / k;
+        Xs[i * ldx + kk] = (rb + i < nrow) ? J.M[(J.r0 + kk) + (int64_t)(J.c0 + row0 + rb + i) * J.ld] : 0.0;
+      }
+    } else {
+      // A(i, kk) = M(r0 + row0 + i, c0 + kk): contiguous in i
+      for (int idx = tid; idx < 64 * k; idx += kOzThreads) {
+        const int i = idx % 64, kk = idx / 64;
+        Xs[i * ldx + kk] = (rb + i < nrow) ? J.M[(J.r0 + row0 + rb + i) + (int64_t)(J.c0 + kk) * J.ld] : 0.0;
+      }
+    }
+    __syncthreads();
+    {
+      const int il = tid & 63, par = tid >> 6;
+      const int i = rb + il;
+      double mx = 0.0;
+      for (int kk = 0; kk < k; ++kk) mx = fmax(mx, fabs(Xs[il * ldx + kk]));
+      int e = 0;
+      if (mx > 0.0) frexp(mx, &e);
+      if (par == 0) escale[i] = e;
+      for (int kc = par; kc < kc_n; kc += 2) {
+        double x[16];
+#pragma unroll
+        for (int t = 0; t < 16; ++t) {
+          const int kk = kc * 16 + t;
+          x[t] = (kk < k) ? ldexp(Xs[il * ldx + kk], -e) : 0.0;
+        }
+        uint4 d[S];
+        digits16<S>(x, d);
+        const size_t off = (size_t)(kc * (kOzRows / 8) + i / 8) * 128 + (i % 8) * 16;
+#pragma unroll
+        for (int s = 0; s < S; ++s) *(uint4*)(As + (size_t)s * kOzRows * Kp + off) = d[s];
+      }
+    }
+    __syncthreads();
+  }
+  fence_async_smem();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_base_s;
+  const uint32_t a_base = smem_u32(As), b_base = smem_u32(Bs);
+  const uint32_t lbo_a = (kOzRows / 8) * 128, lbo_b = (uint32_t)(kp / 8) * 128;
+  const int nchunk = (kp + kOzChunkN - 1) / kOzChunkN;
+  const int ldo = kOzChunkN + 1;
+  bool ok = true;
+  for (int nc = 0; nc < nchunk; ++nc) {
+    const int n0 = nc * kOzChunkN;
+    const int nn = min(kOzChunkN, kp - n0);  // 16 or 32
+    if (tid == 0) {
+      tc_fence_after();
+      const uint32_t idesc = idesc_i8(nn);
+      for (int d = 2; d <= S + 1; ++d) {
+        uint32_t acc = 0;
+        const uint32_t dcol = tmem + (uint32_t)(d - 2) * kOzChunkN;
+        for (int s = (d - S > 1 ? d - S : 1); s <= (d - 1 < S ? d - 1 : S); ++s) {
+          const int t = d - s;
+          for (int ks = 0; ks < Kp / 32; ++ks) {
+            const uint64_t a = umma_desc(a_base + (uint32_t)((s - 1) * kOzRows * Kp) + (uint32_t)(2 * ks) * lbo_a,
+                                         lbo_a, 128);
+            const uint64_t b = umma_desc(b_base + (uint32_t)((t - 1) * kp * Kp) + (uint32_t)(2 * ks) * lbo_b +
+                                             (uint32_t)(n0 / 8) * 128,
+                                         lbo_b, 128);
+            mma_i8(dcol, a, b, idesc, acc);
+            acc = 1;
+          }
+        }
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                       smem_u32(&mbar))
+                   : "memory");
+    }
+    // wait for the chunk's MMAs (bounded)
+    {
+      uint32_t done = 0, spins = 0;
+      const uint32_t parity = (uint32_t)(nc & 1);
+      while (!done && spins < kOzSpinLimit) {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.b32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done)
+            : "r"(smem_u32(&mbar)), "r"(parity)
+            : "memory");
+        ++spins;
+      }
+      if (!done) ok = false;
+    }
+    tc_fence_after();
+    if (ok) {
+      // epilogue: thread = row i (TMEM lane), 16 columns per load, into
+      // the staging chunk
+      const int i = warp * 32 + lane;
+      const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
+      for (int g = 0; g < nn / 16; ++g) {
+        double val[16];
+        int32_t v[16];
+        tmem_ld16(lane_addr + (uint32_t)((S - 1) * kOzChunkN + 16 * g), v);
+        tmem_wait_ld();
+#pragma unroll
+        for (int e = 0; e < 16; ++e) val[e] = (double)v[e];
+        for (int d = S; d >= 2; --d) {
+          tmem_ld16(lane_addr + (uint32_t)((d - 2) * kOzChunkN + 16 * g), v);
+          tmem_wait_ld();
+#pragma unroll
+          for (int e = 0; e < 16; ++e) val[e] = fma(val[e], 0.0078125, (double)v[e]);
+        }
+#pragma unroll
+        for (int e = 0; e < 16; ++e) {
+          const int j = n0 + 16 * g + e;
+          Xs[i * ldo + 16 * g + e] = (j < k) ? ldexp(val[e], escale[i] + fscale[j] - 12) : 0.0;
+        }
+      }
+    }
+    tc_fence_before();
+    __syncthreads();
+    // the chunk's columns back in place, coalesced
+    if (ok) {
+      const int ncol = min(nn, k - n0);
+      if (J.left) {
+        // D(i, j) -> M(r0 + n0 + j, c0 + row0 + i)
+        for (int idx = tid; idx < kOzRows * ncol; idx += kOzThreads) {
+          const int j = idx % ncol, i = idx / ncol;
+          if (i < nrow) J.M[(J.r0 + n0 + j) + (int64_t)(J.c0 + row0 + i) * J.ld] = Xs[i * ldo + j];
+        }
+      } else {
+        // D(i, j) -> M(r0 + row0 + i, c0 + n0 + j)
+        for (int idx = tid; idx < kOzRows * ncol; idx += kOzThreads) {
+          const int i = idx % kOzRows, j = idx / kOzRows;
+          if (i < nrow) J.M[(J.r0 + row0 + i) + (int64_t)(J.c0 + n0 + j) * J.ld] = Xs[i * ldo + j];
+        }
+      }
+    }
+    __syncthreads();
+  }
+  if (!ok && tid == 0) atomicExch(B.err, 1);
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kOzTmemCols));
+}
+
+}  // namespace
+
+size_t ozaki_smem_bytes(int slices) {
+  return (size_t)slices * kOzRows * kOzMaxKp + kOzFacBytes + (size_t)kOzStageDoubles * sizeof(double);
+}
+
+cudaError_t ozaki_init() {
+  cudaError_t e = cudaFuncSetAttribute(k_ozaki_update<7>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)ozaki_smem_bytes(7));
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(k_ozaki_update<8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)ozaki_smem_bytes(8));
+}
+
+void launch_ozaki_prep(cudaStream_t st, const OzPrep& P, int slices) {
+  if (P.nfac <= 0) return;
+  if (slices == 8) k_ozaki_prep<8><<<P.nfac, kOzThreads, 0, st>>>(P);
+  else k_ozaki_prep<7><<<P.nfac, kOzThreads, 0, st>>>(P);
+}
+
+void launch_ozaki_update(cudaStream_t st, const OzBatch& B, int slices) {
+  int tiles = 0;
+  for (int j = 0; j < B.njobs; ++j) tiles += B.job[j].tiles;
+  if (tiles <= 0) return;
+  if (slices == 8) k_ozaki_update<8><<<tiles, kOzThreads, ozaki_smem_bytes(8), st>>>(B);
+  else k_ozaki_update<7><<<tiles, kOzThreads, ozaki_smem_bytes(7), st>>>(B);
+}
+
+}  // namespace qz

@@ -232,6 +232,18 @@ int b200qz_chase_window(b200qz_ctx* ctx, double* h, double* t, int ld, int w, in
 int b200qz_update(b200qz_ctx* ctx, char side, double* m, int ldm, int r0, int c0, int len,
                   const double* w, int ldw, int k);
 
+/* The same update through the split-precision path: the slab and W are
+ * split into `slices` (7 or 8) signed 7-bit INT8 digit matrices (Ozaki
+ * scheme, exact INT32 accumulation on the tensor cores, tcgen05.mma
+ * kind::i8), and the significant slice products (28 or 36) are recombined
+ * in FP64.  Error per entry about 2^-48 (7 slices) or 2^-55 (8 slices)
+ * times |a_i|_max |w_j|_max k.  k <= 80.  Returns 0, -1/-2 bad argument,
+ * 10001 CUDA error, 10004 tensor-core wait timed out.  Replaces the same
+ * DGEMM of PDHGEQZ6.f:296-375.  Solver parameter "split" = 7 or 8 routes
+ * every off-diagonal update of windows up to 80 through this path. */
+int b200qz_update_split(b200qz_ctx* ctx, char side, double* m, int ldm, int r0, int c0, int len, const double* w,
+                        int ldw, int k, int slices);
+
 #ifdef __cplusplus
 }
 #endif
