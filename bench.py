@@ -11,7 +11,12 @@ larger than L2, so no flush is needed between steps.
 
 value      mean device seconds per solve (CUDA events on the solver stream),
            inputs restored from a device-resident copy before each step
-           outside the timed events
+           outside the timed events, in --mode (default plain: FP64 DMMA
+           updates, (nw, ns) from the fixed table; split+learned: updates
+           through 8 INT8 Ozaki slices on the tensor cores and (nw, ns) from
+           the trained MLP); the other form is timed on the same pencil
+           after it and reported under "comparison" with the speed-up of
+           split+learned over plain
 e2e        the same solve through the public C-ABI entry b200qz_solve_host
            with pinned host buffers: H, T copied in, S, P, Q, Z and the
            eigenvalues copied out inside the timed region
@@ -191,6 +196,40 @@ def run_reference(args, pkg, rank):
             "cpu_baseline": {"value": v, "unit": "s", "cores": threads, "kind": "port", "sample": sample},
             "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+DEFAULT_MODE = "plain"
+
+
+def configure(pkg, solver, mode):
+    """Set the solver up for a benchmark mode: 'split' routes the
+    off-diagonal updates through 8 INT8 Ozaki slices on the tensor cores,
+    'learned' loads the trained (nw, ns) network (policy/weights.npz).
+    Returns a note on what was used."""
+    solver.set_param("split", 8 if "split" in mode else 0)
+    note = "split: 8 INT8 slices" if "split" in mode else "updates: FP64 DMMA"
+    if "learned" in mode:
+        P = pkg.learned.load_weights()
+        if P is None:
+            raise RuntimeError("mode %s needs gevp-pdhgeqz_b200/policy/weights.npz" % mode)
+        solver.set_policy(P)
+        note += "; (nw, ns): learned MLP"
+    else:
+        solver.set_policy(None)
+        note += "; (nw, ns): fixed table"
+    return note
+
+
+def errors(torch, dH0, dT0, dH, dT, dQ, dZ, n, dev):
+    """Backward errors and orthogonality (units of n*eps), FP64 on the GPU;
+    the tensors hold the transposes of the column-major matrices."""
+    Ht, Tt, S, P, Q, Z = dH0.t(), dT0.t(), dH.t(), dT.t(), dQ.t(), dZ.t()
+    res_h = (torch.linalg.norm(Q.T @ Ht @ Z - S).item() / torch.linalg.norm(Ht).item()) / (n * EPS)
+    res_t = (torch.linalg.norm(Q.T @ Tt @ Z - P).item() / torch.linalg.norm(Tt).item()) / (n * EPS)
+    I = torch.eye(n, dtype=torch.float64, device=dev)
+    orth_q = torch.linalg.norm(Q.T @ Q - I).item() / (n * EPS)
+    orth_z = torch.linalg.norm(Z.T @ Z - I).item() / (n * EPS)
+    return res_h, res_t, orth_q, orth_z
 
 
 C5_METRIC = ("batched pencils/s: 2048 pencils per GPU, n~U{32..512}, seed 4, 2% zero T diagonal, "
@@ -394,6 +433,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--param", action="append", default=[], help="solver tunable name=value")
     ap.add_argument("--batch", type=int, default=2048, help="pencils per GPU for --workload c5")
+    ap.add_argument("--mode", default=DEFAULT_MODE, choices=["split+learned", "split", "learned", "plain"],
+                    help="update arithmetic and tuning of the timed solves")
+    ap.add_argument("--no-compare", action="store_true", help="skip the comparison solves of the other form")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -430,6 +472,7 @@ def main():
     dZ = torch.empty_like(dH0)
     de = torch.empty(3 * n, dtype=torch.float64, device=dev)
     solver = pkg.Solver(dev)
+    mode_note = configure(pkg, solver, args.mode)
     for kv in args.param:
         k, v = kv.split("=")
         solver.set_param(k, float(v))
@@ -470,22 +513,31 @@ def main():
         t_mean = float(tt.item())
 
     # ---- backward errors of the last timed solve (FP64 on the GPU) ----
-    Ht = dH0.t()
-    Tt = dT0.t()
-    S = dH.t()
-    P = dT.t()
-    Q = dQ.t()
-    Z = dZ.t()
-    nrm_h = torch.linalg.norm(Ht).item()
-    nrm_t = torch.linalg.norm(Tt).item()
-    res_h = (torch.linalg.norm(Q.T @ Ht @ Z - S).item() / nrm_h) / (n * EPS)
-    res_t = (torch.linalg.norm(Q.T @ Tt @ Z - P).item() / nrm_t) / (n * EPS)
-    I = torch.eye(n, dtype=torch.float64, device=dev)
-    orth_q = torch.linalg.norm(Q.T @ Q - I).item() / (n * EPS)
-    orth_z = torch.linalg.norm(Z.T @ Z - I).item() / (n * EPS)
-    del I
+    res_h, res_t, orth_q, orth_z = errors(torch, dH0, dT0, dH, dT, dQ, dZ, n, dev)
 
-    # ---- profiled solve (untimed) for the phase breakdown / roofline ----
+    # ---- the other form on the same pencil: split+learned when the plain
+    # FP64 form is benchmarked, plain otherwise ----
+    comparison = None
+    if not args.no_compare:
+        cmode = "split+learned" if args.mode == "plain" else "plain"
+        cnote = configure(pkg, solver, cmode)
+        one_solve()
+        ct = [one_solve()[0] for _ in range(args.steps)]
+        t_c = float(np.mean(ct))
+        if dist is not None:
+            tt = torch.tensor([t_c], dtype=torch.float64, device=dev)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            t_c = float(tt.item())
+        ce = errors(torch, dH0, dT0, dH, dT, dQ, dZ, n, dev)
+        t_plain, t_split = (t_mean, t_c) if args.mode == "plain" else (t_c, t_mean)
+        comparison = {"mode": cmode, "note": cnote, "value": t_c, "unit": "s",
+                      "split_learned_speedup_over_plain": t_plain / t_split,
+                      "backward_error_neps": {"h": ce[0], "t": ce[1]},
+                      "orthogonality_neps": {"q": ce[2], "z": ce[3]}}
+        configure(pkg, solver, args.mode)
+
+    # ---- profiled solve (untimed, in the benchmarked mode) for the phase
+    # breakdown / roofline ----
     os.environ["B200QZ_PROFILE"] = "1"
     _, pst = one_solve()
     os.environ.pop("B200QZ_PROFILE", None)
@@ -496,7 +548,19 @@ def main():
     kernel_of = {"aed": "k_aed_win", "chase": "k_chase_win", "aed_update": "k_update_left/right",
                  "chase_update": "k_update_left/right", "scan": "k_scan", "inf": "k_inf_win", "final": "k_eigs"}
     nw = 80
-    if dom in ("aed_update", "chase_update"):
+    split = "split" in args.mode
+    if dom in ("aed_update", "chase_update") and split:
+        # INT8 Ozaki slices: bounded by HBM (each updated entry read and
+        # written once, 16 B; window size taken as the chase window, 80)
+        upd_ms = phases.get("aed_update", 0.0) + phases.get("chase_update", 0.0)
+        bytes_alg = 16.0 * pst["update_flops"] / (2.0 * nw)
+        ach = bytes_alg / (upd_ms * 1e-3) / 1e9
+        roof = {"kernel": "k_ozaki_update (INT8 tcgen05, 8 slices)", "bound": "hbm", "achieved": ach,
+                "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": ach / peaks["hbm_gbs"],
+                "traffic": read_ncu_traffic("k_ozaki_update"),
+                "fp64_equivalent_tflops": pst["update_flops"] / (upd_ms * 1e-3) / 1e12,
+                "peak_source": "%s HBM copy bandwidth" % peak_kind}
+    elif dom in ("aed_update", "chase_update"):
         upd_ms = phases.get("aed_update", 0.0) + phases.get("chase_update", 0.0)
         ach = pst["update_flops"] / (upd_ms * 1e-3) / 1e12
         fp64_peak = 37.0
@@ -543,6 +607,7 @@ def main():
     if rank == 0:
         line = {
             "metric": METRIC, "value": t_mean, "unit": "s", "n_gpus": world, "steps": args.steps,
+            "mode": args.mode, "mode_note": mode_note, "comparison": comparison,
             "warmup": args.warmup, "ms_per_step": t_mean * 1e3, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": "%s: %s n=%d" % (args.workload, desc, n), "n": n, "job": "S", "compq": "I",

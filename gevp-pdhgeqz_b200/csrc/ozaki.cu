@@ -46,8 +46,9 @@ namespace {
 
 constexpr int kOzThreads = 128;
 constexpr int kOzRows = 128;  // MMA M
-constexpr int kOzChunkN = 32; // output columns per TMEM pass
-constexpr int kOzTmemCols = 256;  // (slices) accumulators x 32 columns
+constexpr int kOzChunkN = 64; // output columns per MMA pass (one TMEM accumulator each)
+constexpr int kOzOutN = 32;   // output columns per staged write-back
+constexpr int kOzTmemCols = 512;  // (slices) accumulators x 64 columns
 constexpr uint32_t kOzSpinLimit = 1u << 22;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -77,12 +78,10 @@ __device__ __forceinline__ void mma_i8(uint32_t tmem_d, uint64_t a, uint64_t b, 
       "l"(a), "l"(b), "r"(idesc), "r"(acc));
 }
 
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, int32_t (&v)[16]) {
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
-      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-        "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
-      : "r"(taddr));
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, int32_t* v) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];\n"
+               : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
+               : "r"(taddr));
 }
 
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
@@ -90,9 +89,14 @@ __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence:
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
-// S signed 7-bit digits of 16 values x (|x| < 1), packed per digit into 16 bytes.
+// S signed 7-bit digits of 16 values y = x * 2^(6+7(S-1)) (|x| < 1, the
+// scale already applied), packed per digit into 16 bytes.  y is rounded to
+// an integer V (exact for |V| < 2^53, already integral above), and V is
+// written in balanced base 128 from the least significant digit up:
+//   d = ((V + 64) mod 128) - 64,  V <- (V - d) / 128,
+// the top digit taking what is left (|q_1| <= 64).
 template <int S>
-__device__ __forceinline__ void digits16(const double (&x)[16], uint4 (&out)[S]) {
+__device__ __forceinline__ void digits16(const double (&y)[16], uint4 (&out)[S]) {
   uint32_t w[S][4];
 #pragma unroll
   for (int s = 0; s < S; ++s)
@@ -100,17 +104,32 @@ __device__ __forceinline__ void digits16(const double (&x)[16], uint4 (&out)[S])
     for (int q = 0; q < 4; ++q) w[s][q] = 0u;
 #pragma unroll
   for (int e = 0; e < 16; ++e) {
-    double r = x[e] * 64.0;
+    long long v = __double2ll_rn(y[e]);
 #pragma unroll
-    for (int s = 0; s < S; ++s) {
-      const double q = rint(r);
-      r = (r - q) * 128.0;
-      w[s][e >> 2] |= ((uint32_t)(uint8_t)(int8_t)(int)q) << (8 * (e & 3));
+    for (int s = S - 1; s >= 1; --s) {
+      const long long d = ((v + 64) & 127) - 64;
+      v = (v - d) >> 7;
+      w[s][e >> 2] |= ((uint32_t)(d & 0xFF)) << (8 * (e & 3));
     }
+    w[0][e >> 2] |= ((uint32_t)(v & 0xFF)) << (8 * (e & 3));
   }
 #pragma unroll
   for (int s = 0; s < S; ++s) out[s] = make_uint4(w[s][0], w[s][1], w[s][2], w[s][3]);
 }
+
+// a * 2^(sh) for the digit grid: one multiplication when 2^sh is a normal
+// number, ldexp otherwise (rows whose scale is near the exponent range ends)
+struct DigitScale {
+  double m;
+  int sh;
+  bool fast;
+  __device__ DigitScale(int S, int e) {
+    sh = 6 + 7 * (S - 1) - e;
+    fast = sh > -1000 && sh < 1000;
+    m = fast ? ldexp(1.0, sh) : 0.0;
+  }
+  __device__ double operator()(double a) const { return fast ? a * m : ldexp(a, sh); }
+};
 
 // ---------------------------------------------------------------------------
 template <int S>
@@ -131,12 +150,13 @@ __global__ void __launch_bounds__(kOzThreads) k_ozaki_prep(OzPrep P) {
     int e = 0;
     if (mx > 0.0) frexp(mx, &e);
     scale[j] = e;
+    const DigitScale sc(S, e);
     for (int kc = 0; kc < kc_n; ++kc) {
       double x[16];
 #pragma unroll
       for (int t = 0; t < 16; ++t) {
         const int kk = kc * 16 + t;
-        x[t] = (j < k && kk < k) ? ldexp(W[kk + (int64_t)j * ldw], -e) : 0.0;
+        x[t] = (j < k && kk < k) ? sc(W[kk + (int64_t)j * ldw]) : 0.0;
       }
       uint4 d[S];
       digits16<S>(x, d);
@@ -161,7 +181,7 @@ __device__ __forceinline__ int oz_find_job(const OzBatch& B, int& tile) {
 // shared memory: A digits (S x 128 x Kp) | B digits + scales | FP64 staging
 // (64 input rows x (k+1), or one 128 x 33 output chunk)
 constexpr int kOzStageDoubles = 64 * (kOzMaxK + 1);
-static_assert(kOzStageDoubles >= kOzRows * (kOzChunkN + 1), "staging too small");
+static_assert(kOzStageDoubles >= kOzRows * (kOzOutN + 1), "staging too small");
 
 template <int S>
 __global__ void __launch_bounds__(kOzThreads, 1) k_ozaki_update(const OzBatch B) {
@@ -230,12 +250,13 @@ __global__ void __launch_bounds__(kOzThreads, 1) k_ozaki_update(const OzBatch B)
       int e = 0;
       if (mx > 0.0) frexp(mx, &e);
       if (par == 0) escale[i] = e;
+      const DigitScale sc(S, e);
       for (int kc = par; kc < kc_n; kc += 2) {
         double x[16];
 #pragma unroll
         for (int t = 0; t < 16; ++t) {
           const int kk = kc * 16 + t;
-          x[t] = (kk < k) ? ldexp(Xs[il * ldx + kk], -e) : 0.0;
+          x[t] = (kk < k) ? sc(Xs[il * ldx + kk]) : 0.0;
         }
         uint4 d[S];
         digits16<S>(x, d);
@@ -254,11 +275,11 @@ __global__ void __launch_bounds__(kOzThreads, 1) k_ozaki_update(const OzBatch B)
   const uint32_t a_base = smem_u32(As), b_base = smem_u32(Bs);
   const uint32_t lbo_a = (kOzRows / 8) * 128, lbo_b = (uint32_t)(kp / 8) * 128;
   const int nchunk = (kp + kOzChunkN - 1) / kOzChunkN;
-  const int ldo = kOzChunkN + 1;
+  const int ldo = kOzOutN + 1;
   bool ok = true;
   for (int nc = 0; nc < nchunk; ++nc) {
     const int n0 = nc * kOzChunkN;
-    const int nn = min(kOzChunkN, kp - n0);  // 16 or 32
+    const int nn = min(kOzChunkN, kp - n0);  // 16, 32, 48 or 64
     if (tid == 0) {
       tc_fence_after();
       const uint32_t idesc = idesc_i8(nn);
@@ -299,50 +320,51 @@ __global__ void __launch_bounds__(kOzThreads, 1) k_ozaki_update(const OzBatch B)
       if (!done) ok = false;
     }
     tc_fence_after();
-    if (ok) {
-      // epilogue: thread = row i (TMEM lane), 16 columns per load, into
-      // the staging chunk
-      const int i = warp * 32 + lane;
-      const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
-      for (int g = 0; g < nn / 16; ++g) {
-        double val[16];
-        int32_t v[16];
-        tmem_ld16(lane_addr + (uint32_t)((S - 1) * kOzChunkN + 16 * g), v);
-        tmem_wait_ld();
+    // epilogue in 32-column pieces: thread = row i (TMEM lane); per 8
+    // columns all S accumulators are loaded, then combined by Horner's
+    // rule from the smallest weight up; the piece is staged and written
+    // back in place, coalesced
+    for (int p0 = 0; p0 < nn; p0 += kOzOutN) {
+      const int pn = min(kOzOutN, nn - p0);
+      if (ok) {
+        const int i = warp * 32 + lane;
+        const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
+        for (int g = 0; g < pn / 8; ++g) {
+          int32_t v[S][8];
 #pragma unroll
-        for (int e = 0; e < 16; ++e) val[e] = (double)v[e];
-        for (int d = S; d >= 2; --d) {
-          tmem_ld16(lane_addr + (uint32_t)((d - 2) * kOzChunkN + 16 * g), v);
+          for (int d = 0; d < S; ++d) tmem_ld8(lane_addr + (uint32_t)(d * kOzChunkN + p0 + 8 * g), v[d]);
           tmem_wait_ld();
 #pragma unroll
-          for (int e = 0; e < 16; ++e) val[e] = fma(val[e], 0.0078125, (double)v[e]);
-        }
+          for (int e = 0; e < 8; ++e) {
+            double val = (double)v[S - 1][e];
 #pragma unroll
-        for (int e = 0; e < 16; ++e) {
-          const int j = n0 + 16 * g + e;
-          Xs[i * ldo + 16 * g + e] = (j < k) ? ldexp(val[e], escale[i] + fscale[j] - 12) : 0.0;
+            for (int d = S - 2; d >= 0; --d) val = fma(val, 0.0078125, (double)v[d][e]);
+            const int j = n0 + p0 + 8 * g + e;
+            Xs[i * ldo + 8 * g + e] = (j < k) ? ldexp(val, escale[i] + fscale[j] - 12) : 0.0;
+          }
         }
       }
+      __syncthreads();
+      if (ok) {
+        const int cb = n0 + p0;
+        const int ncol = min(pn, k - cb);
+        if (J.left) {
+          // D(i, cb + j) -> M(r0 + cb + j, c0 + row0 + i)
+          for (int idx = tid; idx < kOzRows * ncol; idx += kOzThreads) {
+            const int j = idx % ncol, i = idx / ncol;
+            if (i < nrow) J.M[(J.r0 + cb + j) + (int64_t)(J.c0 + row0 + i) * J.ld] = Xs[i * ldo + j];
+          }
+        } else {
+          // D(i, cb + j) -> M(r0 + row0 + i, c0 + cb + j)
+          for (int idx = tid; idx < kOzRows * ncol; idx += kOzThreads) {
+            const int i = idx % kOzRows, j = idx / kOzRows;
+            if (i < nrow) J.M[(J.r0 + row0 + i) + (int64_t)(J.c0 + cb + j) * J.ld] = Xs[i * ldo + j];
+          }
+        }
+      }
+      __syncthreads();
     }
     tc_fence_before();
-    __syncthreads();
-    // the chunk's columns back in place, coalesced
-    if (ok) {
-      const int ncol = min(nn, k - n0);
-      if (J.left) {
-        // D(i, j) -> M(r0 + n0 + j, c0 + row0 + i)
-        for (int idx = tid; idx < kOzRows * ncol; idx += kOzThreads) {
-          const int j = idx % ncol, i = idx / ncol;
-          if (i < nrow) J.M[(J.r0 + n0 + j) + (int64_t)(J.c0 + row0 + i) * J.ld] = Xs[i * ldo + j];
-        }
-      } else {
-        // D(i, j) -> M(r0 + row0 + i, c0 + n0 + j)
-        for (int idx = tid; idx < kOzRows * ncol; idx += kOzThreads) {
-          const int i = idx % kOzRows, j = idx / kOzRows;
-          if (i < nrow) J.M[(J.r0 + row0 + i) + (int64_t)(J.c0 + n0 + j) * J.ld] = Xs[i * ldo + j];
-        }
-      }
-    }
     __syncthreads();
   }
   if (!ok && tid == 0) atomicExch(B.err, 1);

@@ -12,11 +12,12 @@
 //            from the shift polynomial when the bulge is introduced), the
 //            left-updated 3x3 block of T, the opposite (right) reflector
 //            that clears T(j+1:j+2, j), and the final 3x3 block of T;
-//   phase B  all threads apply every left reflector to its three rows of
-//            H and T and to three columns of U;
-//   phase C  all threads apply every right reflector to its three columns
-//            of H and T and to three columns of V; thread b stores its T
-//            block (the finished column j-1 of H is stored in phase B).
+//   phase B  every left reflector is applied to its three rows of H and T
+//            and to three columns of U (one warp per bulge, lanes over
+//            the bulge's items);
+//   phase C  every right reflector is applied to its three columns of H
+//            and T and to three columns of V; thread b stores its T block
+//            (the finished column j-1 of H is stored in phase B).
 // Bulges are packed 3 rows apart: the rows touched by different left
 // reflectors and the columns touched by different right reflectors are
 // disjoint, and phase A reads only entries no other bulge changes in the
@@ -90,94 +91,6 @@ QZ_HD void bulge_step_compute(MatV H, MatV T, int j, int last, bool intro,
   }
 }
 
-// One application of a bulge's reflector (or rotation) to three (or two)
-// entries along a row or a column: p0 + k*stride, k = 0..2.
-struct ApplyItem {
-  double* p;       // first entry (nullptr: empty slot)
-  int stride;      // distance between the entries
-  int kind;        // 1: reflector on 3 entries, 2: rotation on 2 entries
-  const House3* h; // reflector (kind 1)
-  double c, s;     // rotation (kind 2)
-  double a0, a1, a2;
-  QZ_HD void load() {
-    if (!p) return;
-    a0 = p[0];
-    a1 = p[stride];
-    if (kind == 1) a2 = p[2 * stride];
-  }
-  QZ_HD void apply_store() {
-    if (!p) return;
-    if (kind == 1) {
-      house3_apply(*h, a0, a1, a2);
-      p[0] = a0; p[stride] = a1; p[2 * stride] = a2;
-    } else {
-      p[0] = c * a0 + s * a1;
-      p[stride] = -s * a0 + c * a1;
-    }
-  }
-};
-
-// item loc of bulge b in phase B: rows j.. of H (columns j..wk-1), rows
-// j.. of T (columns past the T block), columns j.. of U (all rows)
-QZ_HD ApplyItem left_item(const BulgeRec* rec, int idx, int tot, int S, int wk, MatV H, MatV T, MatV U) {
-  ApplyItem it;
-  it.p = nullptr;
-  if (idx >= tot) return it;
-  int b = idx / S;
-  int loc = idx - b * S;
-  const BulgeRec& r = rec[b];
-  if (r.kind == 0) return it;
-  int j = r.j;
-  int t0 = (r.kind == 1) ? j + 3 : j + 2;
-  int nh = wk - j, nt = wk - t0;
-  if (nt < 0) nt = 0;
-  it.kind = r.kind;
-  it.h = &r.L;
-  it.c = r.L.s;
-  it.s = r.L.u0;
-  if (loc < nh) {
-    it.p = &H(j, j + loc);
-    it.stride = 1;
-  } else if (loc < nh + nt) {
-    it.p = &T(j, t0 + (loc - nh));
-    it.stride = 1;
-  } else if (loc < nh + nt + wk) {
-    it.p = &U(loc - nh - nt, j);
-    it.stride = U.ld;
-  }
-  return it;
-}
-
-// item loc of bulge b in phase C: columns j.. of H (rows 0..min(j+3,last)
-// or 0..last), columns j.. of T above the T block, columns j.. of V
-QZ_HD ApplyItem right_item(const BulgeRec* rec, int idx, int tot, int S, int wk, int last, MatV H, MatV T,
-                           MatV V) {
-  ApplyItem it;
-  it.p = nullptr;
-  if (idx >= tot) return it;
-  int b = idx / S;
-  int loc = idx - b * S;
-  const BulgeRec& r = rec[b];
-  if (r.kind == 0) return it;
-  int j = r.j;
-  int hr = (r.kind == 1) ? ((j + 4 < last + 1) ? j + 4 : last + 1) : last + 1;
-  it.kind = r.kind;
-  it.h = &r.R;
-  it.c = r.R.s;
-  it.s = r.R.u0;
-  if (loc < hr) {
-    it.p = &H(loc, j);
-    it.stride = H.ld;
-  } else if (loc < hr + j) {
-    it.p = &T(loc - hr, j);
-    it.stride = T.ld;
-  } else if (loc < hr + j + wk) {
-    it.p = &V(loc - hr - j, j);
-    it.stride = V.ld;
-  }
-  return it;
-}
-
 // Chase a chain through a window of size wk held in H, T (wk x wk), while
 // accumulating U, V (wk x wk, identity on entry).  last = last row of the
 // active block inside the window (wk-1 if the block continues below).
@@ -209,31 +122,103 @@ QZ_HD void cta_chase_window(X& x, int wk, int last, MatV H, MatV T, MatV U, MatV
       H(j + 1, j - 1) = 0.0;
       if (r.kind == 1) H(j + 2, j - 1) = 0.0;
     }
-    // Flattened (bulge, item) space: bulge b owns slots [b*S, b*S + S) with
-    // S = 3*wk (an upper bound of its item count).  Items of different
-    // bulges, and different items of one bulge, touch disjoint entries, so
-    // each thread loads two items before storing either (latency overlap).
-    const int S = 3 * wk;
-    const int tot = nb * S;
-    for (int i0 = x.tid; i0 < tot; i0 += 2 * x.nt) {
-      ApplyItem it[2];
-      it[0] = left_item(rec, i0, tot, S, wk, H, T, U);
-      it[1] = left_item(rec, i0 + x.nt, tot, S, wk, H, T, U);
-      it[0].load();
-      it[1].load();
-      it[0].apply_store();
-      it[1].apply_store();
+    // Items of different bulges, and different items of one bulge, touch
+    // disjoint entries.  A warp takes one bulge at a time (reflector in
+    // registers) and its lanes walk the bulge's items: H columns j..wk-1,
+    // T columns past the T block, U rows 0..wk-1; two items per lane per
+    // round so their loads overlap.
+    const int lanes = x.nt < 32 ? x.nt : 32;
+    const int lane = x.tid % lanes;
+    const int nwarp = x.nt / lanes;
+    const int wid = x.tid / lanes;
+    for (int b = wid; b < nb; b += nwarp) {
+      const BulgeRec& r = rec[b];
+      if (r.kind == 0) continue;
+      const int j = r.j;
+      const int t0 = (r.kind == 1) ? j + 3 : j + 2;
+      const int nh = wk - j;
+      const int ntt = (wk - t0 > 0) ? wk - t0 : 0;
+      const int tot = nh + ntt + wk;
+      const House3 L = r.L;
+      const int kind = r.kind;
+      for (int l0 = lane; l0 < tot; l0 += 2 * lanes) {
+        double* p[2];
+        int st[2];
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+          const int loc = l0 + q * lanes;
+          p[q] = nullptr;
+          st[q] = 1;
+          if (loc < nh) p[q] = &H(j, j + loc);
+          else if (loc < nh + ntt) p[q] = &T(j, t0 + (loc - nh));
+          else if (loc < tot) { p[q] = &U(loc - nh - ntt, j); st[q] = U.ld; }
+        }
+        double a[2][3];
+#pragma unroll
+        for (int q = 0; q < 2; ++q)
+          if (p[q]) {
+            a[q][0] = p[q][0];
+            a[q][1] = p[q][st[q]];
+            a[q][2] = (kind == 1) ? p[q][2 * st[q]] : 0.0;
+          }
+#pragma unroll
+        for (int q = 0; q < 2; ++q)
+          if (p[q]) {
+            if (kind == 1) {
+              house3_apply(L, a[q][0], a[q][1], a[q][2]);
+              p[q][0] = a[q][0]; p[q][st[q]] = a[q][1]; p[q][2 * st[q]] = a[q][2];
+            } else {
+              const double c = L.s, sn = L.u0;
+              p[q][0] = c * a[q][0] + sn * a[q][1];
+              p[q][st[q]] = -sn * a[q][0] + c * a[q][1];
+            }
+          }
+      }
     }
     x.sync();
-    // ---- phase C: right transformations ----
-    for (int i0 = x.tid; i0 < tot; i0 += 2 * x.nt) {
-      ApplyItem it[2];
-      it[0] = right_item(rec, i0, tot, S, wk, last, H, T, V);
-      it[1] = right_item(rec, i0 + x.nt, tot, S, wk, last, H, T, V);
-      it[0].load();
-      it[1].load();
-      it[0].apply_store();
-      it[1].apply_store();
+    // ---- phase C: right transformations: H columns j.. (rows 0..hr-1),
+    // T columns j.. above the T block, V columns j.. (all rows) ----
+    for (int b = wid; b < nb; b += nwarp) {
+      const BulgeRec& r = rec[b];
+      if (r.kind == 0) continue;
+      const int j = r.j;
+      const int hr = (r.kind == 1) ? ((j + 4 < last + 1) ? j + 4 : last + 1) : last + 1;
+      const int tot = hr + j + wk;
+      const House3 R = r.R;
+      const int kind = r.kind;
+      for (int l0 = lane; l0 < tot; l0 += 2 * lanes) {
+        double* p[2];
+        int st[2];
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+          const int loc = l0 + q * lanes;
+          p[q] = nullptr;
+          st[q] = H.ld;
+          if (loc < hr) p[q] = &H(loc, j);
+          else if (loc < hr + j) { p[q] = &T(loc - hr, j); st[q] = T.ld; }
+          else if (loc < tot) { p[q] = &V(loc - hr - j, j); st[q] = V.ld; }
+        }
+        double a[2][3];
+#pragma unroll
+        for (int q = 0; q < 2; ++q)
+          if (p[q]) {
+            a[q][0] = p[q][0];
+            a[q][1] = p[q][st[q]];
+            a[q][2] = (kind == 1) ? p[q][2 * st[q]] : 0.0;
+          }
+#pragma unroll
+        for (int q = 0; q < 2; ++q)
+          if (p[q]) {
+            if (kind == 1) {
+              house3_apply(R, a[q][0], a[q][1], a[q][2]);
+              p[q][0] = a[q][0]; p[q][st[q]] = a[q][1]; p[q][2 * st[q]] = a[q][2];
+            } else {
+              const double c = R.s, sn = R.u0;
+              p[q][0] = c * a[q][0] + sn * a[q][1];
+              p[q][st[q]] = -sn * a[q][0] + c * a[q][1];
+            }
+          }
+      }
     }
     // deferred stores owned by the bulge's thread
     for (int b = x.tid; b < nb; b += x.nt) {

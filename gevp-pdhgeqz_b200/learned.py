@@ -11,9 +11,13 @@ Training data are traces the method generates itself:
 * seeded pencils (n ~ U{2000..8000}, N(0,1), every 50th subdiagonal scaled
   by 1e-8 so that deflation clusters) are run with the table up to a
   decision point (the solver stops before its j-th AED, ``aed_limit``);
-* from that state every candidate (nw, ns) of a small grid runs two AEDs
-  and the sweep between them; its score is deflations per flop (counted
-  off-diagonal update flops plus 10 nw^3 per AED window);
+* from that state every candidate (nw, ns) of a small grid runs three AEDs
+  and the sweeps between them; it is scored by deflations per flop (counted
+  off-diagonal update flops plus 10 nw^3 per AED window) and by deflations
+  per device second (its solve time minus that of a run that stops before
+  the first AED, i.e. without the restart's own cost).  The AED and chase
+  kernels are latency-bound on the GPU, so the label uses the per-second
+  score, the cost that time-to-Schur actually pays;
 * the label is the best candidate, encoded as y0 = (nw - 16) / 64 and
   y1 = ns / nw.
 
@@ -222,9 +226,10 @@ def _set(solver, nw_max, ns_max, aed_limit):
     solver.set_param("aed_limit", aed_limit)
 
 
-def trace_pencil(solver, H, T, decisions=(0, 3)):
-    """Samples (features, scores[len(GRID_NW), len(GRID_NSF)], nh) of one
-    pencil at the given AED decision points."""
+def trace_pencil(solver, H, T, decisions=(0, 3), horizon=3):
+    """Samples (features, scores_per_second, scores_per_flop, nh) of one
+    pencil at the given AED decision points; scores are arrays
+    [len(GRID_NW), len(GRID_NSF)]."""
     import torch
     n = H.shape[0]
     dev = torch.device("cuda", torch.cuda.current_device())
@@ -248,22 +253,29 @@ def trace_pencil(solver, H, T, decisions=(0, 3)):
         snapH.copy_(bufs[0])
         snapT.copy_(bufs[1])
         feat = solver.policy_features(snapH.data_ptr(), n, ktop, kbot, frac)
-        score = np.zeros((len(GRID_NW), len(GRID_NSF)))
+        # cost of restarting from the snapshot alone (scans down to kbot)
+        bufs[0].copy_(snapH)
+        bufs[1].copy_(snapT)
+        _set(solver, NW_MAX, 0, 0)
+        _solve(solver, bufs, n)
+        t0 = solver.stats()["seconds"]
+        s_time = np.zeros((len(GRID_NW), len(GRID_NSF)))
+        s_flop = np.zeros_like(s_time)
         for a, nw in enumerate(GRID_NW):
             for b, nsf in enumerate(GRID_NSF):
                 bufs[0].copy_(snapH)
                 bufs[1].copy_(snapT)
                 ns = max(2, int(round(nsf * nw)) // 2 * 2)
-                _set(solver, nw, ns, 2)
+                _set(solver, nw, ns, horizon)
                 info = _solve(solver, bufs, n)
                 st = solver.stats()
                 if info not in (0, 10003):
-                    score[a, b] = 0.0
                     continue
                 defl = rem0 - int(st["remaining"])
                 cost = st["update_flops"] + AED_FLOP_FACTOR * st["aeds"] * min(nw, kbot - ktop + 1) ** 3
-                score[a, b] = defl / max(cost, 1.0)
-        out.append((feat, score, kbot - ktop + 1))
+                s_flop[a, b] = defl / max(cost, 1.0)
+                s_time[a, b] = defl / max(st["seconds"] - t0, 1e-6)
+        out.append((feat, s_time, s_flop, kbot - ktop + 1))
     _set(solver, NW_MAX, 0, -1)
     return out
 
@@ -283,18 +295,19 @@ def score_of_choice(score, nw, nsf):
 
 
 def offline_gain(P, X, scores, nh):
-    """Mean over samples of score(network's choice) / score(table's
-    choice), both taken at the nearest grid candidate."""
+    """Geometric mean over samples of score(network's choice) /
+    score(table's choice), both taken at the nearest grid candidate (ratios
+    floored at 1e-3 so that a zero score counts as a large loss, not -inf)."""
     _, _, Y = forward_np(P, X)
-    ratios = []
+    logs = []
     for y, sc, h in zip(Y, scores, nh):
         nw, ns = decode(y, int(h))
         tnw, tnsf = table_choice(int(h))
         s_net = score_of_choice(sc, nw, ns / max(nw, 1))
         s_tab = score_of_choice(sc, tnw, tnsf)
         if s_tab > 0:
-            ratios.append(s_net / s_tab)
-    return float(np.mean(ratios)) if ratios else 1.0
+            logs.append(np.log(max(s_net / s_tab, 1e-3)))
+    return float(np.exp(np.mean(logs))) if logs else 1.0
 
 
 def generate_traces(count=200, decisions=(0, 3), device=0, log=None):
@@ -303,18 +316,19 @@ def generate_traces(count=200, decisions=(0, 3), device=0, log=None):
     pkg = _pkg()
     torch.cuda.set_device(device)
     solver = pkg.Solver(device)
-    feats, scores, nhs, ids = [], [], [], []
+    feats, scores, sflop, nhs, ids = [], [], [], [], []
     try:
         for i, n, seed in training_pencils(count):
             H, T = pkg.pencils.clustered_ht(n, seed, every=50, scale=1e-8)
-            for f, sc, nh in trace_pencil(solver, H, T, decisions):
+            for f, st, sf, nh in trace_pencil(solver, H, T, decisions):
                 feats.append(f)
-                scores.append(sc)
+                scores.append(st)
+                sflop.append(sf)
                 nhs.append(nh)
                 ids.append(i)
             if log:
                 log("pencil %d n=%d samples=%d" % (i, n, len(feats)))
     finally:
         solver.close()
-    return {"features": np.stack(feats).astype(np.float32), "scores": np.stack(scores), "nh": np.array(nhs),
-            "pencil": np.array(ids)}
+    return {"features": np.stack(feats).astype(np.float32), "scores": np.stack(scores),
+            "scores_per_flop": np.stack(sflop), "nh": np.array(nhs), "pencil": np.array(ids)}

@@ -60,6 +60,7 @@ def cmd_train(a):
     P, mse = lrn.train_device(P0, X[~hold], T[~hold], epochs=a.epochs, lr=a.lr)
     dt = time.time() - t0
     res = {"samples_train": int((~hold).sum()), "samples_holdout": int(hold.sum()), "mse_train": mse,
+           "label": "argmax deflations per device second",
            "mse_holdout": lrn.loss_np(P, X[hold], T[hold]), "train_seconds": dt,
            "gain_train": lrn.offline_gain(P, X[~hold], scores[~hold], nh[~hold]),
            "gain_holdout": lrn.offline_gain(P, X[hold], scores[hold], nh[hold])}
@@ -115,7 +116,7 @@ def main():
     p = sub.add_parser("train")
     p.add_argument("--traces", required=True)
     p.add_argument("--out", required=True)
-    p.add_argument("--epochs", type=int, default=4000)
+    p.add_argument("--epochs", type=int, default=300)
     p.add_argument("--lr", type=float, default=1e-3)
     p.add_argument("--seed", type=int, default=0)
     p = sub.add_parser("evaluate")
