@@ -89,6 +89,7 @@ struct b200qz_ctx {
   uint8_t* ozb = nullptr;
   int* ozerr = nullptr;        // device flag: a tensor-core wait timed out
   double* norms = nullptr;     // 2
+  double* npart = nullptr;     // 592 per-block partial sums of the norm kernel
   int* dinfo = nullptr;        // 16 ints: [4..6] AED info, [8..12] scan output
   int* hinfo = nullptr;        // pinned mirror
   double* hshifts = nullptr;   // pinned 3*kAedMax
@@ -377,8 +378,8 @@ struct GpuBackend {
       }
     }
     c->timer.begin(phase, c->stream);
-    if (L.njobs) { launch_update(c->stream, L, 0); c->stats.launches += 1; }
-    if (R.njobs) { launch_update(c->stream, R, 1); c->stats.launches += 1; }
+    if (L.njobs) { launch_update(c->stream, L, 0, c->params.upd_persist); c->stats.launches += 1; }
+    if (R.njobs) { launch_update(c->stream, R, 1, c->params.upd_persist); c->stats.launches += 1; }
     c->timer.end(c->stream);
   }
 };
@@ -416,8 +417,8 @@ int solve_dev_impl(b200qz_ctx* c, char job, char compq, char compz, int n, int i
   int nh = ihi - ilo + 1;
   // /PREC/ constants (PDHGEQZ.f:449-458): ulp, smlnum, Frobenius norms
   QZ_CK(cudaMemsetAsync(c->norms, 0, 2 * sizeof(double), c->stream));
-  launch_sumsq(c->stream, h, ld, ilo - 1, nh, c->norms);
-  launch_sumsq(c->stream, t, ld, ilo - 1, nh, c->norms + 1);
+  launch_sumsq(c->stream, h, ld, ilo - 1, nh, c->norms, c->npart);
+  launch_sumsq(c->stream, t, ld, ilo - 1, nh, c->norms + 1, c->npart);
   c->stats.launches += 2;
   QZ_CK(cudaMemcpyAsync(c->hnorms, c->norms, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   QZ_CK(cudaStreamSynchronize(c->stream));
@@ -488,6 +489,7 @@ int b200qz_create(b200qz_ctx** out, int device) {
   if (e == cudaSuccess) e = cudaMemset(c->ozerr, 0, sizeof(int));
   if (e == cudaSuccess) e = ozaki_init();
   if (e == cudaSuccess) e = cudaMalloc(&c->norms, 2 * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc(&c->npart, 592 * sizeof(double));
   if (e == cudaSuccess) e = cudaMalloc(&c->dinfo, 16 * sizeof(int));
   if (e == cudaSuccess) e = cudaMallocHost(&c->hinfo, 16 * sizeof(int));
   if (e == cudaSuccess) e = cudaMallocHost(&c->hshifts, 3 * kAedMax * sizeof(double));
@@ -514,7 +516,7 @@ void b200qz_destroy(b200qz_ctx* c) {
   if (c->ozb) cudaFree(c->ozb);
   if (c->ozerr) cudaFree(c->ozerr);
   if (c->hpol_y) cudaFreeHost(c->hpol_y);
-  cudaFree(c->shifts); cudaFree(c->gscratch); cudaFree(c->norms); cudaFree(c->dinfo);
+  cudaFree(c->shifts); cudaFree(c->gscratch); cudaFree(c->norms); cudaFree(c->npart); cudaFree(c->dinfo);
   if (c->hinfo) cudaFreeHost(c->hinfo);
   if (c->hshifts) cudaFreeHost(c->hshifts);
   if (c->hnorms) cudaFreeHost(c->hnorms);
@@ -563,6 +565,7 @@ int b200qz_set_param(b200qz_ctx* c, const char* name, double value) {
   else if (k == "max_wave") { if (v < 1 || v > kMaxWave) return -3; P.max_wave = v; }
   else if (k == "stall_limit") { if (v < 1) return -3; P.stall_limit = v; }
   else if (k == "aed_limit") { P.aed_limit = v < 0 ? -1 : v; }
+  else if (k == "upd_persist") { if (v != 0 && v != 1) return -3; P.upd_persist = v; }
   else if (k == "split") { if (v != 0 && v != 7 && v != 8) return -3; P.split = v; }
   else if (k == "aed_threads") { if (v != 32 && v != 64 && v != 128) return -3; P.aed_threads = v; }
   else return -2;
@@ -664,8 +667,8 @@ int b200qz_aed_window(b200qz_ctx* c, double* h, double* t, int ld, int ktop, int
   // norms of the whole leading (kbot+1) block give the tolerances
   int nh = kbot + 1;
   QZ_CK(cudaMemsetAsync(c->norms, 0, 2 * sizeof(double), c->stream));
-  launch_sumsq(c->stream, h, ld, 0, nh, c->norms);
-  launch_sumsq(c->stream, t, ld, 0, nh, c->norms + 1);
+  launch_sumsq(c->stream, h, ld, 0, nh, c->norms, c->npart);
+  launch_sumsq(c->stream, t, ld, 0, nh, c->norms + 1, c->npart);
   QZ_CK(cudaMemcpyAsync(c->hnorms, c->norms, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   QZ_CK(cudaStreamSynchronize(c->stream));
   Tol tol;

@@ -314,7 +314,11 @@ __global__ void k_set_identity(double* Q, int64_t ld, int n) {
 }
 
 // sum of squares of the n x n block at (o, o)
-__global__ void k_sumsq(const double* A, int64_t ld, int o, int n, double* out) {
+// Sum of squares in a fixed order: each block writes its partial sum, then
+// one warp adds the partials in block order (no floating-point atomics, so
+// the tolerances derived from the norms are identical from run to run).
+constexpr int kSumsqBlocks = 592;
+__global__ void k_sumsq(const double* A, int64_t ld, int o, int n, double* partial) {
   double acc = 0.0;
   int64_t total = (int64_t)n * n;
   for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total; idx += (int64_t)gridDim.x * blockDim.x) {
@@ -330,8 +334,15 @@ __global__ void k_sumsq(const double* A, int64_t ld, int o, int n, double* out) 
   if (wid == 0) {
     acc = (lane < (int)(blockDim.x >> 5)) ? red[lane] : 0.0;
     for (int off = 16; off > 0; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
-    if (lane == 0) atomicAdd(out, acc);
+    if (lane == 0) partial[blockIdx.x] = acc;
   }
+}
+
+__global__ void k_sumsq_final(const double* partial, int np, double* out) {
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < np; i += 32) acc += partial[i];
+  for (int off = 16; off > 0; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
+  if (threadIdx.x == 0) out[0] = acc;
 }
 
 // ---------------------------------------------------------------------------
@@ -355,6 +366,14 @@ static size_t upd_smem(int k, int side) {
   return ((size_t)kp * (kp + 4) + (size_t)32 * (kp + 4)) * sizeof(double);
 }
 
+static size_t upd_smem_persist(int k, int side) {
+  int kp = (k + 15) & ~15;
+  if (side == 0) return ((size_t)kp * (kp + 4) + 2 * (size_t)kp * 36) * sizeof(double);
+  return ((size_t)kp * (kp + 4) + 2 * (size_t)kUpdTile * (kp + 4)) * sizeof(double);
+}
+
+static int g_sm_count = 0;
+
 cudaError_t kernels_init() {
   cudaError_t e;
   e = cudaFuncSetAttribute(k_aed_win<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)aed_smem_bytes(kWinSmemMax));
@@ -371,6 +390,19 @@ cudaError_t kernels_init() {
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(k_update_right, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)upd_smem(kUpdMaxK, 1));
   if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(k_update_persist<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)upd_smem_persist(kUpdMaxK, 0));
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(k_update_persist<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)upd_smem_persist(kUpdMaxK, 1));
+  if (e != cudaSuccess) return e;
+  {
+    int dev = 0;
+    e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    e = cudaDeviceGetAttribute(&g_sm_count, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return e;
+  }
   e = cudaFuncSetAttribute(k_update_left_gen, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(k_update_right_gen, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
@@ -406,7 +438,7 @@ void launch_scan(cudaStream_t st, double* H, double* T, int64_t ld, int ifirst, 
 void launch_inf_top(cudaStream_t st, double* H, double* T, double* Q, int64_t ld, int n, int f, int wantq) {
   k_inf_top<<<1, 1024, 0, st>>>(H, T, Q, ld, n, f, wantq);
 }
-void launch_update(cudaStream_t st, const UpdBatch& B_in, int side) {
+void launch_update(cudaStream_t st, const UpdBatch& B_in, int side, int persist) {
   UpdBatch B = B_in;
   int tiles = 0;
   B.k = 0;
@@ -418,6 +450,17 @@ void launch_update(cudaStream_t st, const UpdBatch& B_in, int side) {
   if (B.k > kUpdMaxK) {
     if (side == 0) k_update_left_gen<<<tiles, 256, upd_smem(B.k, 0), st>>>(B);
     else k_update_right_gen<<<tiles, 256, upd_smem(B.k, 1), st>>>(B);
+  } else if (persist) {
+    const size_t sm = upd_smem_persist(B.k, side);
+    int per_sm = (int)((220 * 1024) / sm);
+    per_sm = per_sm < 1 ? 1 : (per_sm > 4 ? 4 : per_sm);
+    int grid = (g_sm_count > 0 ? g_sm_count : 148) * per_sm;
+    if (grid > tiles) grid = tiles;
+    // one warp per 16-row (left) / 16-column (right) slice of the largest window
+    int warps = ((B.k + 15) & ~15) / 16;
+    warps = warps < 1 ? 1 : (warps > kUpdMaxThreads / 32 ? kUpdMaxThreads / 32 : warps);
+    if (side == 0) k_update_persist<0><<<grid, 32 * warps, sm, st>>>(B, tiles);
+    else k_update_persist<1><<<grid, 32 * warps, sm, st>>>(B, tiles);
   } else {
     if (side == 0) k_update_left<<<tiles, kUpdThreads, upd_smem(B.k, 0), st>>>(B);
     else k_update_right<<<tiles, kUpdThreads, upd_smem(B.k, 1), st>>>(B);
@@ -433,8 +476,9 @@ void launch_finalize(cudaStream_t st, double* H, double* T, double* Z, int64_t l
 void launch_identity(cudaStream_t st, double* Q, int64_t ld, int n) {
   k_set_identity<<<592, 256, 0, st>>>(Q, ld, n);
 }
-void launch_sumsq(cudaStream_t st, const double* A, int64_t ld, int o, int n, double* out) {
-  k_sumsq<<<592, 256, 0, st>>>(A, ld, o, n, out);
+void launch_sumsq(cudaStream_t st, const double* A, int64_t ld, int o, int n, double* out, double* partial) {
+  k_sumsq<<<kSumsqBlocks, 256, 0, st>>>(A, ld, o, n, partial);
+  k_sumsq_final<<<1, 32, 0, st>>>(partial, kSumsqBlocks, out);
 }
 
 }  // namespace qz

@@ -54,11 +54,13 @@ void launch_inf(cudaStream_t st, double* H, double* T, int64_t ld, int w0, int w
                 int deflate, double* U, double* V);
 void launch_scan(cudaStream_t st, double* H, double* T, int64_t ld, int ifirst, int kbot, const Tol& tol, int* out);
 void launch_inf_top(cudaStream_t st, double* H, double* T, double* Q, int64_t ld, int n, int f, int wantq);
-void launch_update(cudaStream_t st, const UpdBatch& B, int side);
+// persist: one CTA per SM slot walking a run of tiles (factor kept, next tile prefetched)
+void launch_update(cudaStream_t st, const UpdBatch& B, int side, int persist = 1);
 int update_tile(int k);
 void launch_finalize(cudaStream_t st, double* H, double* T, double* Z, int64_t ld, int n, int wantz, double* ar,
                      double* ai, double* be);
 void launch_identity(cudaStream_t st, double* Q, int64_t ld, int n);
-void launch_sumsq(cudaStream_t st, const double* A, int64_t ld, int o, int n, double* out);
+// out[0] = sum of squares of A(o:o+n, o:o+n); partial: 592 doubles of scratch
+void launch_sumsq(cudaStream_t st, const double* A, int64_t ld, int o, int n, double* out, double* partial);
 
 }  // namespace qz

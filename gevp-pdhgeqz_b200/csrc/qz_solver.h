@@ -37,6 +37,7 @@ struct SolveParams {
   int aed_threads = 128; // threads of the AED / endgame window kernel (32: one warp)
   int split = 0;         // 7 or 8: off-diagonal updates through that many INT8
                          // Ozaki slices on the tensor cores (windows up to 80)
+  int upd_persist = 1;   // 1: persistent, prefetching DMMA update kernels
   int aed_limit = -1;    // >= 0: stop before the AED after this many AEDs
                          // (tuning traces; the solve then returns -2)
 };
