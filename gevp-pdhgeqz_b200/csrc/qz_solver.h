@@ -30,8 +30,9 @@ struct SolveParams {
   int maxit_factor = 30; // MAXIT = 30*NH
   int chain_max = -1;    // bulges per chain, -1: from w_chase
   int verbose = 0;       // progress lines on stderr (B200QZ_VERBOSE=1)
-  int aed_nskip = 4;     // AED spike test stops after this many consecutive
-                         // undeflatable blocks (0: test the whole window)
+  int aed_nskip = -1;    // AED spike test stops after this many consecutive
+                         // undeflatable blocks (0: test the whole window;
+                         // -1: whole window for n >= 6000, else 4)
   int max_wave = 8;      // chains chased concurrently (one CTA each)
   int stall_limit = 300; // iterations without deflation before giving up
   int aed_threads = 128; // threads of the AED / endgame window kernel (32: one warp)
