@@ -22,7 +22,7 @@ namespace qz {
 // Tunables (defaults follow the reference's PIPARMQ table where the GPU
 // window limits allow; see piparmq.f:438-535).
 struct SolveParams {
-  int nw_max = 80;       // AED window (one CTA, shared memory)
+  int nw_max = 48;       // AED window (one CTA, shared memory; up to 80)
   int w_chase = 80;      // chase window
   int nmin = 80;         // active blocks this small are solved by one CTA
   int nibble = -1;       // -1: table (14 in PDHGEQZ1 regime, 335*nh^-0.44 above)
@@ -264,7 +264,9 @@ int qz_iterate(BK& bk, int n, int ilo, int ihi, const SolveParams& P, SolveStats
     {
       int pnw = 0, pns = 0;
       if (bk.policy(ktop, kbot, S.last_frac, &pnw, &pns)) {
-        nw = std::max(std::min(4, nh), std::min(pnw, nw));
+        // the network's window, up to the window kernel's limit (which the
+        // decoded output already respects) rather than the table's nw_max
+        nw = std::max(std::min(4, nh), std::min(pnw, nh));
         ns_pol = pns;
         ++S.policy_calls;
       }
