@@ -1,6 +1,6 @@
 """LAPACK side of the oracle (test infrastructure only).
 
-This module is the checker, never the product: only ``tests/``,
+This module is part of the oracle, never the product: only ``tests/``,
 ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline leg use it.
 
 It calls FP64 LAPACK through ctypes in the OpenBLAS build that ships inside

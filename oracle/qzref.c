@@ -1,8 +1,8 @@
 /*
  * qzref.c -- CPU restatement of the reference's multishift QZ path on a
- * 1x1 process grid.  TEST INFRASTRUCTURE ONLY: used by tests/ as the
- * checker and by bench.py as the timed CPU baseline ("port").  The product
- * (libb200qz.so) never links or calls it.
+ * 1x1 process grid.  TEST INFRASTRUCTURE ONLY: the oracle tests/ compare
+ * the GPU path with, and bench.py's timed CPU baseline ("port").  The
+ * product (libb200qz.so) never links or calls it.
  *
  * Parity status: the reference ships no golden vectors (testing/EXRAND1.f
  * only checks residual thresholds on non-reproducible inputs), so this

@@ -1,6 +1,6 @@
 """ctypes wrapper of the oracle's C restatement (oracle/qzref.c).
 
-Test infrastructure: the checker and the CPU baseline, never the product."""
+Test infrastructure: an oracle for the tests and the CPU baseline, never the product."""
 import ctypes
 import os
 
