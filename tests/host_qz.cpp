@@ -1,0 +1,257 @@
+// Host build of the library's CTA-level QZ algorithms, for the CPU tests.
+//
+// The window routines of the device kernels (qz_cta.cuh, qz_chase.cuh) and
+// the iteration driver (qz_solver.h) are templates over an executor; here
+// they run with a single host "thread" (tid 0 of 1, barriers are no-ops),
+// and a host backend plays the part of the device kernels with the same
+// window copies, factor updates and deflation scan.  This checks the
+// algorithms and the solver's control logic against LAPACK without a GPU;
+// thread-level concurrency is checked by the GPU tests.
+//
+// Built by tests/test_cpu_host_algorithms.py with g++ into a temporary
+// directory.
+#include <cfloat>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "../gevp-pdhgeqz_b200/csrc/qz_solver.h"
+
+using namespace qz;
+
+namespace {
+
+struct HostExec {
+  int tid = 0, nt = 1;
+  int si[64];
+  double* sd;
+  std::vector<double> sdv;
+  HostExec() : sdv(16384, 0.0) { sd = sdv.data(); }
+  void sync() {}
+  void stamp(int) {}
+};
+
+Tol make_tol(const double* H, const double* T, int ld, int o, int nh) {
+  double hn = 0.0, tn = 0.0;
+  for (int j = 0; j < nh; ++j)
+    for (int i = 0; i < nh; ++i) {
+      const double a = H[(o + i) + (size_t)(o + j) * ld], b = T[(o + i) + (size_t)(o + j) * ld];
+      hn += a * a;
+      tn += b * b;
+    }
+  Tol t;
+  t.safmin = DBL_MIN;
+  t.ulp = DBL_EPSILON;
+  t.smlnum = DBL_MIN * ((double)nh / DBL_EPSILON);
+  t.htol = dmax(DBL_MIN, DBL_EPSILON * sqrt(hn));
+  t.ttol = dmax(DBL_MIN, DBL_EPSILON * sqrt(tn));
+  return t;
+}
+
+struct HostBK {
+  int n, ld;
+  double *H, *T, *Q, *Z;
+  bool wantq = true, wantz = true;
+  int nskip = 4;
+  Tol tol;
+  HostExec x;
+  std::vector<double> Ua, Va;                 // last AED window factors
+  std::vector<std::vector<double>> Uc, Vc;    // chase / zero-chase factors per window of a wave
+  double& h(int i, int j) { return H[i + (size_t)j * ld]; }
+  double& t(int i, int j) { return T[i + (size_t)j * ld]; }
+
+  void scan(int ifirst, int kbot, int* out) {
+    int bad = 0;
+    for (int j = ifirst; j <= kbot; ++j) {
+      const double a = h(j, j), b = t(j, j), c = (j > ifirst) ? h(j, j - 1) : 0.0;
+      if (!std::isfinite(a) || !std::isfinite(b) || !std::isfinite(c)) bad = 1;
+    }
+    int ktop = ifirst;
+    for (int k = kbot; k > ifirst; --k)
+      if (negligible_sub(h(k, k - 1), h(k - 1, k - 1), h(k, k), tol)) { ktop = k; break; }
+    if (ktop > ifirst) h(ktop, ktop - 1) = 0.0;
+    int cnt = 0, jmax = -1, jmin = -1;
+    for (int j = ktop; j <= kbot; ++j)
+      if (fabs(t(j, j)) <= tol.ttol) {
+        t(j, j) = 0.0;
+        ++cnt;
+        jmax = j;
+        if (jmin < 0) jmin = j;
+      }
+    out[0] = ktop; out[1] = cnt; out[2] = jmax; out[3] = jmin; out[4] = bad;
+  }
+
+  void load(int w, int wk, std::vector<double>& Hs, std::vector<double>& Ts, std::vector<double>& Us,
+            std::vector<double>& Vs) {
+    Hs.assign((size_t)wk * wk, 0.0); Ts = Hs; Us = Hs; Vs = Hs;
+    for (int j = 0; j < wk; ++j) {
+      for (int i = 0; i < wk; ++i) { Hs[i + (size_t)j * wk] = h(w + i, w + j); Ts[i + (size_t)j * wk] = t(w + i, w + j); }
+      Us[j + (size_t)j * wk] = 1.0;
+      Vs[j + (size_t)j * wk] = 1.0;
+    }
+  }
+  void store(int w, int wk, const std::vector<double>& Hs, const std::vector<double>& Ts) {
+    for (int j = 0; j < wk; ++j)
+      for (int i = 0; i < wk; ++i) { h(w + i, w + j) = Hs[i + (size_t)j * wk]; t(w + i, w + j) = Ts[i + (size_t)j * wk]; }
+  }
+
+  void aed(int ktop, int kwtop, int kbot, int* info3, double* sh) {
+    const int nw = kbot - kwtop + 1;
+    std::vector<double> Hs, Ts, Us, Vs, s3(3 * (size_t)nw);
+    load(kwtop, nw, Hs, Ts, Us, Vs);
+    const double s = (kwtop > ktop) ? h(kwtop, kwtop - 1) : 0.0;
+    WinState w;
+    w.n = nw; w.H = MatV{Hs.data(), nw}; w.T = MatV{Ts.data(), nw}; w.Q = MatV{Us.data(), nw};
+    w.Z = MatV{Vs.data(), nw}; w.wantq = true; w.wantz = true; w.tol = tol;
+    cta_aed(x, w, s, s3.data(), s3.data() + nw, s3.data() + 2 * nw, 30 * nw, (kwtop > ktop) ? nskip : 0);
+    const int m = x.si[8], st = x.si[9], tr = x.si[10];
+    if (st == 0 && tr) {
+      store(kwtop, nw, Hs, Ts);
+      if (kwtop > ktop) h(kwtop, kwtop - 1) = s * Us[0];
+      Ua = Us;
+      Va = Vs;
+    }
+    info3[0] = m; info3[1] = st; info3[2] = tr;
+    const int mm = m < nw ? m : nw;
+    for (int i = 0; i < mm; ++i) { sh[i] = s3[i]; sh[mm + i] = s3[nw + i]; sh[2 * mm + i] = s3[2 * nw + i]; }
+  }
+
+  // off-diagonal updates with a window's factors, left part or right part
+  void apply_left(int w, int wk, const std::vector<double>& U) {
+    std::vector<double> col(wk);
+    for (double* M : {H, T})
+      for (int c = w + wk; c < n; ++c) {
+        for (int i = 0; i < wk; ++i) {
+          double a = 0.0;
+          for (int k = 0; k < wk; ++k) a += U[k + (size_t)i * wk] * M[(w + k) + (size_t)c * ld];
+          col[i] = a;
+        }
+        for (int i = 0; i < wk; ++i) M[(w + i) + (size_t)c * ld] = col[i];
+      }
+  }
+  void apply_right(int w, int wk, const std::vector<double>& U, const std::vector<double>& V) {
+    std::vector<double> row(wk);
+    auto right = [&](double* M, int rows, const std::vector<double>& W) {
+      for (int r = 0; r < rows; ++r) {
+        for (int j = 0; j < wk; ++j) {
+          double a = 0.0;
+          for (int k = 0; k < wk; ++k) a += M[r + (size_t)(w + k) * ld] * W[k + (size_t)j * wk];
+          row[j] = a;
+        }
+        for (int j = 0; j < wk; ++j) M[r + (size_t)(w + j) * ld] = row[j];
+      }
+    };
+    right(H, w, V);
+    right(T, w, V);
+    if (wantq) right(Q, n, U);
+    if (wantz) right(Z, n, V);
+  }
+  void update(int w, int wk, int which) {
+    const std::vector<double>& U = which == 0 ? Ua : Uc[0];
+    const std::vector<double>& V = which == 0 ? Va : Vc[0];
+    apply_left(w, wk, U);
+    apply_right(w, wk, U, V);
+  }
+
+  void chase_wave(const WinPlan* const* wins, int nw) {
+    Uc.assign(nw, {});
+    Vc.assign(nw, {});
+    for (int i = 0; i < nw; ++i) {
+      const WinPlan& p = *wins[i];
+      std::vector<double> Hs, Ts, Us, Vs;
+      load(p.w, p.wk, Hs, Ts, Us, Vs);
+      std::vector<BulgeRec> rec(p.nb);
+      cta_chase_window(x, p.wk, p.last, MatV{Hs.data(), p.wk}, MatV{Ts.data(), p.wk}, MatV{Us.data(), p.wk},
+                       MatV{Vs.data(), p.wk}, p.bl.data(), p.nb, p.tmax, rec.data());
+      store(p.w, p.wk, Hs, Ts);
+      Uc[i] = Us;
+      Vc[i] = Vs;
+    }
+  }
+  // as on the device: every left update of the wave, then every right one
+  void update_wave(const WinPlan* const* wins, int nw) {
+    for (int i = 0; i < nw; ++i) apply_left(wins[i]->w, wins[i]->wk, Uc[i]);
+    for (int i = 0; i < nw; ++i) apply_right(wins[i]->w, wins[i]->wk, Uc[i], Vc[i]);
+  }
+  void inf_window(int w, int wk, int top, int jz, int stop, bool deflate) {
+    std::vector<double> Hs, Ts, Us, Vs;
+    load(w, wk, Hs, Ts, Us, Vs);
+    cta_inf_window(x, wk, top, jz, stop, deflate, MatV{Hs.data(), wk}, MatV{Ts.data(), wk}, MatV{Us.data(), wk},
+                   MatV{Vs.data(), wk});
+    store(w, wk, Hs, Ts);
+    Uc.assign(1, Us);
+    Vc.assign(1, Vs);
+  }
+  void inf_top(int f) {
+    double c, s, r;
+    lartg(h(f, f), h(f + 1, f), c, s, r);
+    for (int j = f + 1; j < n; ++j) {
+      double a = h(f, j), b = h(f + 1, j);
+      h(f, j) = c * a + s * b; h(f + 1, j) = -s * a + c * b;
+      a = t(f, j); b = t(f + 1, j);
+      t(f, j) = c * a + s * b; t(f + 1, j) = -s * a + c * b;
+    }
+    if (wantq)
+      for (int i = 0; i < n; ++i) {
+        double a = Q[i + (size_t)f * ld], b = Q[i + (size_t)(f + 1) * ld];
+        Q[i + (size_t)f * ld] = c * a + s * b; Q[i + (size_t)(f + 1) * ld] = -s * a + c * b;
+      }
+    h(f, f) = r;
+    h(f + 1, f) = 0.0;
+  }
+  bool policy(int, int, double, int*, int*) { return false; }
+};
+
+}  // namespace
+
+extern "C" {
+
+// Window QZ of an n x n pencil (Q, Z accumulate from their input).
+int host_small_qz(int n, double* H, double* T, double* Q, double* Z) {
+  static HostExec x;
+  WinState w;
+  w.n = n; w.H = MatV{H, n}; w.T = MatV{T, n}; w.Q = MatV{Q, n}; w.Z = MatV{Z, n};
+  w.wantq = w.wantz = true;
+  w.tol = make_tol(H, T, n, 0, n);
+  return cta_small_qz(x, w, 30 * n);
+}
+
+// AED on a whole window with spike s (Q, Z identity on entry); out3 =
+// {undeflated m, status, transformed}; shifts: alphar, alphai, beta (n each).
+void host_aed(int n, double* H, double* T, double* Q, double* Z, double s, int nskip, double* shifts, int* out3) {
+  static HostExec x;
+  WinState w;
+  w.n = n; w.H = MatV{H, n}; w.T = MatV{T, n}; w.Q = MatV{Q, n}; w.Z = MatV{Z, n};
+  w.wantq = w.wantz = true;
+  w.tol = make_tol(H, T, n, 0, n);
+  cta_aed(x, w, s, shifts, shifts + n, shifts + 2 * n, 30 * n, nskip);
+  out3[0] = x.si[8]; out3[1] = x.si[9]; out3[2] = x.si[10];
+}
+
+// Full solve with the library's iteration driver and the host backend
+// (COMPQ = COMPZ = 'I'); eigenvalues to ar, ai, be.  stats: iterations,
+// AEDs, sweeps, chase windows, zero-chase steps.
+int host_solve(int n, double* H, double* T, double* Q, double* Z, int nw_max, int w_chase, int nmin, int nskip,
+               double* ar, double* ai, double* be, int* stats) {
+  HostBK bk;
+  bk.n = n; bk.ld = n; bk.H = H; bk.T = T; bk.Q = Q; bk.Z = Z; bk.nskip = nskip;
+  bk.tol = make_tol(H, T, n, 0, n);
+  for (int j = 0; j < n; ++j)
+    for (int i = 0; i < n; ++i) { Q[i + (size_t)j * n] = (i == j); Z[i + (size_t)j * n] = (i == j); }
+  SolveParams P;
+  P.nw_max = nw_max; P.w_chase = w_chase; P.nmin = nmin;
+  SolveStats S;
+  int info = (n > 0) ? qz_iterate(bk, n, 0, n - 1, P, S) : 0;
+  if (info == 0) {
+    WinState w;
+    w.n = n; w.H = MatV{H, n}; w.T = MatV{T, n}; w.Q = MatV{Q, n}; w.Z = MatV{Z, n};
+    w.wantq = w.wantz = true;
+    w.tol = bk.tol;
+    cta_finalize(bk.x, w, ar, ai, be);
+  }
+  stats[0] = (int)S.iters; stats[1] = (int)S.aeds; stats[2] = (int)S.sweeps; stats[3] = (int)S.windows;
+  stats[4] = (int)S.infs;
+  return info;
+}
+
+}  // extern "C"

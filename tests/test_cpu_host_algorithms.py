@@ -1,0 +1,97 @@
+"""The library's window algorithms and iteration driver, built for the host
+(tests/host_qz.cpp: one host thread, the same template source as the device
+kernels, and a host backend in place of the kernels), checked against the
+LAPACK DHGEQZ oracle without a GPU: backward errors and orthogonality
+within 50*n*eps, generalized Schur structure, and eigenvalue sets within
+the condition-scaled chordal tolerance."""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_pd = ctypes.POINTER(ctypes.c_double)
+_pi = ctypes.POINTER(ctypes.c_int)
+
+
+@pytest.fixture(scope="module")
+def host(tmp_path_factory):
+    out = str(tmp_path_factory.mktemp("hostqz") / "libhostqz.so")
+    cmd = ["g++", "-O2", "-shared", "-fPIC", "-std=c++17", "-Wno-unknown-pragmas", os.path.join(HERE, "host_qz.cpp"),
+           "-o", out]
+    subprocess.run(cmd, check=True, capture_output=True, timeout=300)
+    L = ctypes.CDLL(out)
+    L.host_small_qz.argtypes = [ctypes.c_int] + [_pd] * 4
+    L.host_small_qz.restype = ctypes.c_int
+    L.host_aed.argtypes = [ctypes.c_int] + [_pd] * 4 + [ctypes.c_double, ctypes.c_int, _pd, _pi]
+    L.host_aed.restype = None
+    L.host_solve.argtypes = [ctypes.c_int] + [_pd] * 4 + [ctypes.c_int] * 4 + [_pd] * 3 + [_pi]
+    L.host_solve.restype = ctypes.c_int
+    return L
+
+
+def _p(a):
+    return a.ctypes.data_as(_pd)
+
+
+def _check(lapack, H, T, S, P, Q, Z, eig=None):
+    r = lapack.residuals(H, T, S, P, Q, Z)
+    for key in ("h", "t", "q", "z"):
+        assert r[key] <= 50 * r["neps"], (key, r[key] / r["neps"])
+    So, Po, lar, lai, lbe, _, _, _ = lapack.dhgeqz(H, T)
+    e = eig if eig is not None else lapack.eig_from_schur(S, P)
+    ok, ratio, _ = lapack.match_eigenvalues((lar, lai, lbe), e, lapack.eig_tolerance(So, Po, H, T))
+    assert ok, ratio
+
+
+@pytest.mark.parametrize("n,seed,zf", [(1, 0, 0.0), (2, 1, 0.0), (3, 2, 0.0), (17, 3, 0.0), (60, 4, 0.05),
+                                       (80, 5, 0.0), (120, 6, 0.02)])
+def test_host_window_qz(pkg, lapack, host, n, seed, zf):
+    H, T = pkg.pencils.random_ht(n, seed, zf)
+    S, P, Q, Z = (np.array(M, order="F", copy=True) for M in (H, T, np.eye(n), np.eye(n)))
+    assert host.host_small_qz(n, _p(S), _p(P), _p(Q), _p(Z)) == 0
+    _check(lapack, H, T, S, P, Q, Z)
+
+
+@pytest.mark.parametrize("nskip", [0, 4])
+def test_host_aed_window(pkg, lapack, host, nskip):
+    """AED on a window whose spike is small near the bottom: the deflated
+    part is decoupled, the whole window stays an orthogonal equivalence."""
+    n = 48
+    H, T = pkg.pencils.clustered_ht(n, 7, every=11, scale=1e-9)
+    s = 1e-7
+    S, P, Q, Z = (np.array(M, order="F", copy=True) for M in (H, T, np.eye(n), np.eye(n)))
+    shifts = np.zeros(3 * n)
+    out3 = np.zeros(3, dtype=np.int32)
+    host.host_aed(n, _p(S), _p(P), _p(Q), _p(Z), s, nskip, _p(shifts), out3.ctypes.data_as(_pi))
+    m, st, tr = (int(v) for v in out3)
+    assert st == 0 and 0 <= m <= n
+    eps = np.finfo(float).eps
+    assert np.linalg.norm(Q @ S @ Z.T - H) <= 50 * n * eps * np.linalg.norm(H)
+    assert np.linalg.norm(Q @ P @ Z.T - T) <= 50 * n * eps * np.linalg.norm(T)
+    assert np.linalg.norm(Q.T @ Q - np.eye(n)) <= 50 * n * eps
+    # spike s * Q(0, :) is negligible over the deflated positions
+    assert np.all(np.abs(s * Q[0, m:]) <= 1e-12 * max(1.0, np.abs(s)))
+    assert np.all(np.tril(P, -1) == 0.0)
+
+
+@pytest.mark.parametrize("n,seed,kind", [(150, 1, "r"), (230, 2, "z"), (260, 3, "g"), (200, 4, "c")])
+def test_host_full_solve(pkg, lapack, host, n, seed, kind):
+    """The iteration driver with AED windows of 32, chase windows of 40 and
+    an endgame below 40, so that every phase runs: AED, multishift sweeps
+    in waves of chains, zero chasing, the endgame and the finalisation."""
+    P_ = pkg.pencils
+    H, T = {"r": lambda: P_.random_ht(n, seed), "z": lambda: P_.random_ht(n, seed, 0.05),
+            "g": lambda: P_.graded_ht(n, seed), "c": lambda: P_.clustered_ht(n, seed, every=30, scale=1e-8)}[kind]()
+    S, P, Q, Z = (np.array(M, order="F", copy=True) for M in (H, T, np.zeros((n, n)), np.zeros((n, n))))
+    ar, ai, be = np.zeros(n), np.zeros(n), np.zeros(n)
+    st = np.zeros(5, dtype=np.int32)
+    info = host.host_solve(n, _p(S), _p(P), _p(Q), _p(Z), 32, 40, 40, 4, _p(ar), _p(ai), _p(be),
+                           st.ctypes.data_as(_pi))
+    assert info == 0
+    assert st[1] > 0 and st[2] > 0 and st[3] > 0  # AEDs, sweeps and chase windows ran
+    assert lapack.schur_structure_ok(S, P)
+    assert np.all(be >= 0)
+    _check(lapack, H, T, S, P, Q, Z, eig=(ar, ai, be))
