@@ -228,6 +228,22 @@ void host_aed(int n, double* H, double* T, double* Q, double* Z, double s, int n
   out3[0] = x.si[8]; out3[1] = x.si[9]; out3[2] = x.si[10];
 }
 
+// Chase a chain of nb bulges through an n x n window (the whole matrix):
+// bulges int[4*nb] = {base, tlo, thi, intro} per bulge, coef double[3*nb]
+// = {c2, c1, c0}; U, V identity on entry accumulate the transformations.
+void host_chase(int n, double* H, double* T, double* U, double* V, const int* bulges, const double* coef, int nb,
+                int tmax, int last) {
+  static HostExec x;
+  std::vector<Bulge> bl(nb);
+  for (int b = 0; b < nb; ++b) {
+    bl[b].base = bulges[4 * b]; bl[b].tlo = bulges[4 * b + 1]; bl[b].thi = bulges[4 * b + 2];
+    bl[b].intro = bulges[4 * b + 3];
+    bl[b].c2 = coef[3 * b]; bl[b].c1 = coef[3 * b + 1]; bl[b].c0 = coef[3 * b + 2];
+  }
+  std::vector<BulgeRec> rec(nb);
+  cta_chase_window(x, n, last, MatV{H, n}, MatV{T, n}, MatV{U, n}, MatV{V, n}, bl.data(), nb, tmax, rec.data());
+}
+
 // Full solve with the library's iteration driver and the host backend
 // (COMPQ = COMPZ = 'I'); eigenvalues to ar, ai, be.  stats: iterations,
 // AEDs, sweeps, chase windows, zero-chase steps.

@@ -29,6 +29,8 @@ def host(tmp_path_factory):
     L.host_aed.restype = None
     L.host_solve.argtypes = [ctypes.c_int] + [_pd] * 4 + [ctypes.c_int] * 4 + [_pd] * 3 + [_pi]
     L.host_solve.restype = ctypes.c_int
+    L.host_chase.argtypes = [ctypes.c_int] + [_pd] * 4 + [_pi, _pd] + [ctypes.c_int] * 3
+    L.host_chase.restype = None
     return L
 
 
@@ -95,3 +97,45 @@ def test_host_full_solve(pkg, lapack, host, n, seed, kind):
     assert lapack.schur_structure_ok(S, P)
     assert np.all(be >= 0)
     _check(lapack, H, T, S, P, Q, Z, eig=(ar, ai, be))
+
+
+def _shift_set(rng, nb, cplx):
+    sr, si, sb, coef = [], [], [], []
+    for b in range(nb):
+        if cplx and b % 2 == 0:
+            ar, ai = rng.standard_normal(), abs(rng.standard_normal()) + 0.1
+            sr += [ar, ar]; si += [ai, -ai]; sb += [1.0, 1.0]
+            coef += [1.0, 2 * ar, ar * ar + ai * ai]
+        else:
+            a1, a2 = rng.standard_normal(2)
+            sr += [a1, a2]; si += [0.0, 0.0]; sb += [1.0, 1.0]
+            coef += [1.0, a1 + a2, a1 * a2]
+    return np.array(sr), np.array(si), np.array(sb), np.array(coef)
+
+
+@pytest.mark.parametrize("n,nb,cplx", [(12, 1, False), (30, 3, False), (50, 5, True), (80, 12, True)])
+def test_host_chase_matches_restatement(pkg, host, n, nb, cplx):
+    """Lockstep chase of an introduced chain (the library's chase routine on
+    the host) against the oracle's bulge-by-bulge PDHGEQZB/DHGEQZ5
+    restatement from the same state (after the oracle's PDHGEQZA
+    introduction): the same reflectors in exact arithmetic, so H, T, U, V
+    agree to rounding (1e-9 relative)."""
+    from oracle import qzref as R
+    H, T = pkg.pencils.random_ht(n, 20 + n)
+    rng = np.random.default_rng(n)
+    sr, si, sb, coef = _shift_set(rng, nb, cplx)
+    H1, T1, _, _ = R.sweep(H, T, sr, si, sb, phase=1)
+    S_ref, P_ref, Q_ref, Z_ref = R.sweep(H1, T1, sr, si, sb, phase=2)
+    bul, tmax = [], 0
+    for k in range(nb):
+        base = 3 * (nb - 1 - k) + 1
+        thi = (n - 1) - base
+        bul += [base, 0, thi, 0]
+        tmax = max(tmax, thi)
+    bul = np.array(bul, dtype=np.int32)
+    S, P = np.array(H1, order="F", copy=True), np.array(T1, order="F", copy=True)
+    U, V = np.eye(n, order="F"), np.eye(n, order="F")
+    host.host_chase(n, _p(S), _p(P), _p(U), _p(V), bul.ctypes.data_as(_pi), _p(np.ascontiguousarray(coef)), nb,
+                    tmax, n - 1)
+    for a, b in ((S, S_ref), (P, P_ref), (U, Q_ref), (V, Z_ref)):
+        assert np.linalg.norm(a - b) <= 1e-9 * max(1.0, np.linalg.norm(b)), np.linalg.norm(a - b)
