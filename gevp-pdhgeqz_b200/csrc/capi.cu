@@ -433,6 +433,33 @@ int solve_dev_impl(b200qz_ctx* c, char job, char compq, char compz, int n, int i
   QZ_CK(cudaMemcpyAsync(c->hnorms, c->norms, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   QZ_CK(cudaStreamSynchronize(c->stream));
   if (c->err != cudaSuccess) return 10001;
+  // T far from H in magnitude (or sums of squares out of range): balance T
+  // by a power of two for the iteration, undone before the finalisation
+  int ebal = 0;
+  {
+    const double hs = c->hnorms[0], ts = c->hnorms[1];
+    const bool plain = hs > 1e-280 && hs < 1e280 && ts > 1e-280 && ts < 1e280 &&
+                       std::fabs(0.5 * (std::log2(hs) - std::log2(ts))) <= 28.0;
+    if (!plain && nh > 0) {
+      launch_maxabs(c->stream, h, ld, ilo - 1, nh, c->norms, c->npart);
+      launch_maxabs(c->stream, t, ld, ilo - 1, nh, c->norms + 1, c->npart);
+      c->stats.launches += 4;
+      QZ_CK(cudaMemcpyAsync(c->hnorms, c->norms, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+      QZ_CK(cudaStreamSynchronize(c->stream));
+      if (c->err != cudaSuccess) return 10001;
+      ebal = balance_exponent(c->hnorms[0], c->hnorms[1]);
+      if (ebal != 0) {
+        launch_scale_pow2(c->stream, t, ld, n, ebal);
+        c->stats.launches += 1;
+      }
+      launch_sumsq(c->stream, h, ld, ilo - 1, nh, c->norms, c->npart);
+      launch_sumsq(c->stream, t, ld, ilo - 1, nh, c->norms + 1, c->npart);
+      c->stats.launches += 4;
+      QZ_CK(cudaMemcpyAsync(c->hnorms, c->norms, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+      QZ_CK(cudaStreamSynchronize(c->stream));
+      if (c->err != cudaSuccess) return 10001;
+    }
+  }
   GpuBackend bk;
   bk.c = c;
   bk.H = h; bk.T = t; bk.Q = q; bk.Z = z;
@@ -448,6 +475,10 @@ int solve_dev_impl(b200qz_ctx* c, char job, char compq, char compz, int n, int i
   tol.ttol = std::max(DBL_MIN, DBL_EPSILON * std::sqrt(c->hnorms[1]));
   int info = 0;
   if (nh > 0) info = qz_iterate(bk, n, ilo - 1, ihi - 1, c->params, c->stats);
+  if (ebal != 0) {
+    launch_scale_pow2(c->stream, t, ld, n, -ebal);
+    c->stats.launches += 1;
+  }
   const bool stopped = (info == -2);  // AED limit reached (tuning traces)
   if (stopped) info = 10003;
   else if (info < 0) info = 10002;  // non-finite entries appeared (or were given)

@@ -345,6 +345,43 @@ __global__ void k_sumsq_final(const double* partial, int np, double* out) {
   if (threadIdx.x == 0) out[0] = acc;
 }
 
+// largest absolute entry, same two-stage fixed-order reduction
+__global__ void k_maxabs(const double* A, int64_t ld, int o, int n, double* partial) {
+  double m = 0.0;
+  int64_t total = (int64_t)n * n;
+  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total; idx += (int64_t)gridDim.x * blockDim.x) {
+    int i = (int)(idx % n), j = (int)(idx / n);
+    m = fmax(m, fabs(A[(o + i) + (int64_t)(o + j) * ld]));
+  }
+  for (int off = 16; off > 0; off >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, off));
+  __shared__ double red[32];
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) red[wid] = m;
+  __syncthreads();
+  if (wid == 0) {
+    m = (lane < (int)(blockDim.x >> 5)) ? red[lane] : 0.0;
+    for (int off = 16; off > 0; off >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, off));
+    if (lane == 0) partial[blockIdx.x] = m;
+  }
+}
+
+__global__ void k_max_final(const double* partial, int np, double* out) {
+  double m = 0.0;
+  for (int i = threadIdx.x; i < np; i += 32) m = fmax(m, partial[i]);
+  for (int off = 16; off > 0; off >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, off));
+  if (threadIdx.x == 0) out[0] = m;
+}
+
+// A(0:n, 0:n) <- 2^e A (exact unless the result leaves the normal range)
+__global__ void k_scale_pow2(double* A, int64_t ld, int n, int e) {
+  int64_t total = (int64_t)n * n;
+  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total; idx += (int64_t)gridDim.x * blockDim.x) {
+    int i = (int)(idx % n), j = (int)(idx / n);
+    double& a = A[i + (int64_t)j * ld];
+    a = ldexp(a, e);
+  }
+}
+
 // ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
@@ -475,6 +512,13 @@ void launch_finalize(cudaStream_t st, double* H, double* T, double* Z, int64_t l
 }
 void launch_identity(cudaStream_t st, double* Q, int64_t ld, int n) {
   k_set_identity<<<592, 256, 0, st>>>(Q, ld, n);
+}
+void launch_maxabs(cudaStream_t st, const double* A, int64_t ld, int o, int n, double* out, double* partial) {
+  k_maxabs<<<kSumsqBlocks, 256, 0, st>>>(A, ld, o, n, partial);
+  k_max_final<<<1, 32, 0, st>>>(partial, kSumsqBlocks, out);
+}
+void launch_scale_pow2(cudaStream_t st, double* A, int64_t ld, int n, int e) {
+  if (n > 0 && e != 0) k_scale_pow2<<<592, 256, 0, st>>>(A, ld, n, e);
 }
 void launch_sumsq(cudaStream_t st, const double* A, int64_t ld, int o, int n, double* out, double* partial) {
   k_sumsq<<<kSumsqBlocks, 256, 0, st>>>(A, ld, o, n, partial);

@@ -60,6 +60,10 @@ int update_tile(int k);
 void launch_finalize(cudaStream_t st, double* H, double* T, double* Z, int64_t ld, int n, int wantz, double* ar,
                      double* ai, double* be);
 void launch_identity(cudaStream_t st, double* Q, int64_t ld, int n);
+// out[0] = largest |A(i,j)| over A(o:o+n, o:o+n); partial: 592 doubles of scratch
+void launch_maxabs(cudaStream_t st, const double* A, int64_t ld, int o, int n, double* out, double* partial);
+// A(0:n, 0:n) <- 2^e A
+void launch_scale_pow2(cudaStream_t st, double* A, int64_t ld, int n, int e);
 // out[0] = sum of squares of A(o:o+n, o:o+n); partial: 592 doubles of scratch
 void launch_sumsq(cudaStream_t st, const double* A, int64_t ld, int o, int n, double* out, double* partial);
 

@@ -74,6 +74,19 @@ inline int nibble_table(int nh) {
   return std::min(100, (int)std::ceil(335.0 * std::pow((double)nh, -0.44)));
 }
 
+// Power of two applied to T before the iteration when T's magnitude is far
+// from H's (more than 2^30 apart), so that shift polynomials, whose
+// coefficients grow like the square of the eigenvalues' magnitude, stay in
+// the floating-point range; undone on T (and hence beta) at the end.  The
+// scaling is exact and commutes with the orthogonal transformations.
+// Arguments are the largest absolute entries of the two active blocks.
+inline int balance_exponent(double hmax, double tmax) {
+  if (!(hmax > 0.0) || !(tmax > 0.0) || !std::isfinite(hmax) || !std::isfinite(tmax)) return 0;
+  const double l2 = std::log2(hmax) - std::log2(tmax);
+  if (std::fabs(l2) <= 30.0) return 0;
+  return (int)std::lround(l2);
+}
+
 struct ShiftPair { double c2, c1, c0; };
 
 // Pair the shifts (alphar, alphai, beta) into real quadratics: complex

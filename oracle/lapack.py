@@ -231,6 +231,12 @@ def _sphere(ar, ai, be):
     images."""
     a = ar + 1j * ai
     b = be.astype(np.complex128)
+    # scale by the larger modulus first so that the squares below neither
+    # underflow nor overflow (pencils with entries near the range limits)
+    sc = np.maximum(np.abs(a), np.abs(b))
+    sc[sc == 0] = 1.0
+    a = a / sc
+    b = b / sc
     nrm = np.sqrt(np.abs(a) ** 2 + np.abs(b) ** 2)
     nrm[nrm == 0] = 1.0
     a = a / nrm

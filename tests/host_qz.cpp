@@ -48,6 +48,16 @@ Tol make_tol(const double* H, const double* T, int ld, int o, int nh) {
   return t;
 }
 
+int balance_exponent(const double* H, const double* T, int ld, int o, int nh) {
+  double hm = 0.0, tm = 0.0;
+  for (int j = 0; j < nh; ++j)
+    for (int i = 0; i < nh; ++i) {
+      hm = dmax(hm, fabs(H[(o + i) + (size_t)(o + j) * ld]));
+      tm = dmax(tm, fabs(T[(o + i) + (size_t)(o + j) * ld]));
+    }
+  return qz::balance_exponent(hm, tm);
+}
+
 struct HostBK {
   int n, ld;
   double *H, *T, *Q, *Z;
@@ -251,6 +261,11 @@ int host_solve(int n, double* H, double* T, double* Q, double* Z, int nw_max, in
                double* ar, double* ai, double* be, int* stats) {
   HostBK bk;
   bk.n = n; bk.ld = n; bk.H = H; bk.T = T; bk.Q = Q; bk.Z = Z; bk.nskip = nskip;
+  // as the library does: T scaled by a power of two when its norm is far
+  // from H's (shifts and their polynomials stay in range), undone at the end
+  const int e = balance_exponent(H, T, n, 0, n);
+  if (e != 0)
+    for (size_t i = 0; i < (size_t)n * n; ++i) T[i] = ldexp(T[i], e);
   bk.tol = make_tol(H, T, n, 0, n);
   for (int j = 0; j < n; ++j)
     for (int i = 0; i < n; ++i) { Q[i + (size_t)j * n] = (i == j); Z[i + (size_t)j * n] = (i == j); }
@@ -258,6 +273,8 @@ int host_solve(int n, double* H, double* T, double* Q, double* Z, int nw_max, in
   P.nw_max = nw_max; P.w_chase = w_chase; P.nmin = nmin;
   SolveStats S;
   int info = (n > 0) ? qz_iterate(bk, n, 0, n - 1, P, S) : 0;
+  if (e != 0)
+    for (size_t i = 0; i < (size_t)n * n; ++i) T[i] = ldexp(T[i], -e);
   if (info == 0) {
     WinState w;
     w.n = n; w.H = MatV{H, n}; w.T = MatV{T, n}; w.Q = MatV{Q, n}; w.Z = MatV{Z, n};

@@ -139,3 +139,51 @@ def test_host_chase_matches_restatement(pkg, host, n, nb, cplx):
                     tmax, n - 1)
     for a, b in ((S, S_ref), (P, P_ref), (U, Q_ref), (V, Z_ref)):
         assert np.linalg.norm(a - b) <= 1e-9 * max(1.0, np.linalg.norm(b)), np.linalg.norm(a - b)
+
+
+def _edge_pencil(pkg, kind):
+    P_ = pkg.pencils
+    if kind == "n1":
+        return P_.random_ht(1, 1)
+    if kind == "n2":
+        return P_.random_ht(2, 2)
+    if kind == "zeros30":
+        return P_.random_ht(200, 3, 0.3)
+    if kind == "splits":
+        H, T = P_.random_ht(240, 4)
+        for k in (30, 31, 100, 180):
+            H[k, k - 1] = 0.0
+        return H, T
+    if kind == "tinyT":
+        H, T = P_.random_ht(200, 5)
+        return H, T * 1e-200
+    if kind == "hugeT":
+        H, T = P_.random_ht(180, 6)
+        return H, T * 1e150
+    if kind == "Tdiag0":
+        H, T = P_.random_ht(150, 7)
+        T[np.arange(150), np.arange(150)] = 0.0
+        return H, T
+    if kind == "triH":
+        H, T = P_.random_ht(150, 8)
+        return np.triu(H), T
+    raise ValueError(kind)
+
+
+@pytest.mark.parametrize("kind", ["n1", "n2", "zeros30", "splits", "tinyT", "hugeT", "Tdiag0", "triH"])
+def test_host_solve_edge_cases(pkg, lapack, host, kind):
+    """Edge cases of the driver: orders 1 and 2, 30 % zero T diagonal,
+    exact splits of H, T scaled by 1e-200 and 1e150 against H (T is balanced
+    by a power of two for the iteration), an all-zero T diagonal and an
+    already triangular H."""
+    H, T = _edge_pencil(pkg, kind)
+    n = H.shape[0]
+    S, P, Q, Z = (np.array(M, order="F", copy=True) for M in (H, T, np.zeros((n, n)), np.zeros((n, n))))
+    ar, ai, be = np.zeros(n), np.zeros(n), np.zeros(n)
+    st = np.zeros(5, dtype=np.int32)
+    info = host.host_solve(n, _p(S), _p(P), _p(Q), _p(Z), 32, 40, 40, 4, _p(ar), _p(ai), _p(be),
+                           st.ctypes.data_as(_pi))
+    assert info == 0
+    assert lapack.schur_structure_ok(S, P)
+    assert np.all(be >= 0)
+    _check(lapack, H, T, S, P, Q, Z, eig=(ar, ai, be))

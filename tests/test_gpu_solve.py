@@ -85,3 +85,14 @@ def test_compq_n_eigenvalues_only(pkg, lapack):
     tol = lapack.eig_tolerance(So, Po, H, T)
     ok, ratio, _ = lapack.match_eigenvalues((lar, lai, lbe), (ar, ai, be), tol)
     assert ok, ratio
+
+
+@pytest.mark.parametrize("scale", [1e-200, 1e150])
+def test_solve_with_T_far_from_H(pkg, lapack, scale):
+    """T scaled far from H: the library balances T by a power of two for the
+    iteration (shift polynomials stay in range) and undoes it at the end."""
+    n = 200
+    H, T = pkg.pencils.random_ht(n, 31)
+    T = T * scale
+    S, P, Q, Z, ar, ai, be, info = pkg.solve(H, T)
+    check(lapack, H, T, S, P, Q, Z, ar, ai, be, info)
