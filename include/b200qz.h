@@ -67,7 +67,10 @@ void b200qz_destroy(b200qz_ctx* ctx);
  * dimension ld >= n for H, T, Q, Z).  job/compq/compz and ilo/ihi
  * (1-based) as in PDHGEQZ.  alphar/alphai/beta are device arrays of
  * length n.  Returns INFO (0 ok, > 0 unconverged row, < 0 bad argument,
- * 10001 CUDA error). */
+ * 10001 CUDA error, 10002 non-finite entries, 10003 stopped by the
+ * "aed_limit" parameter).  When T's largest entry is more than 2^30 away
+ * from H's, T is scaled by a power of two during the iteration and scaled
+ * back before returning. */
 int b200qz_solve_dev(b200qz_ctx* ctx, char job, char compq, char compz, int n, int ilo, int ihi,
                      double* h, double* t, double* q, double* z, int ld,
                      double* alphar, double* alphai, double* beta);
