@@ -187,3 +187,18 @@ def test_host_solve_edge_cases(pkg, lapack, host, kind):
     assert lapack.schur_structure_ok(S, P)
     assert np.all(be >= 0)
     _check(lapack, H, T, S, P, Q, Z, eig=(ar, ai, be))
+
+
+def test_host_solve_default_windows(pkg, lapack, host):
+    """The library's default window sizes (AED 48, chase 80, endgame 80) on
+    an N(0,1) pencil of order 500."""
+    n = 500
+    H, T = pkg.pencils.random_ht(n, 41)
+    S, P, Q, Z = (np.array(M, order="F", copy=True) for M in (H, T, np.zeros((n, n)), np.zeros((n, n))))
+    ar, ai, be = np.zeros(n), np.zeros(n), np.zeros(n)
+    st = np.zeros(5, dtype=np.int32)
+    info = host.host_solve(n, _p(S), _p(P), _p(Q), _p(Z), 48, 80, 80, 4, _p(ar), _p(ai), _p(be),
+                           st.ctypes.data_as(_pi))
+    assert info == 0 and st[2] > 0
+    assert lapack.schur_structure_ok(S, P)
+    _check(lapack, H, T, S, P, Q, Z, eig=(ar, ai, be))
