@@ -55,3 +55,21 @@ def test_pdhgeqz_argument_errors_need_no_gpu(pkg):
     H0 = H.copy()
     assert pkg.pdhgeqz("S", "I", "I", H, T, Q, Z, ilo=5, ihi=4)[3] == 0
     assert np.array_equal(H, H0)
+
+
+def test_header_compiles_as_c99_and_links(tmp_path, pkg):
+    """include/b200qz.h is plain C: a C99 program (pedantic, warnings as
+    errors) includes it, links libb200qz.so and calls an entry point that
+    needs no GPU."""
+    import subprocess
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    src = tmp_path / "use_header.c"
+    src.write_text('#include "b200qz.h"\n#include <stdio.h>\n'
+                   'int main(void) { printf("%d\\n", b200qz_policy_nparams()); return 0; }\n')
+    libdir = os.path.join(root, "gevp-pdhgeqz_b200")
+    exe = str(tmp_path / "use_header")
+    subprocess.run(["gcc", "-std=c99", "-Wall", "-Wextra", "-pedantic", "-Werror", "-I", os.path.join(root, "include"),
+                    str(src), "-L", libdir, "-lb200qz", "-Wl,-rpath," + libdir, "-o", exe], check=True,
+                   capture_output=True, timeout=120)
+    out = subprocess.run([exe], check=True, capture_output=True, text=True, timeout=60)
+    assert int(out.stdout.strip()) == pkg.learned.nparams()
