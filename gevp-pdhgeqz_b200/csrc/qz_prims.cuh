@@ -419,13 +419,22 @@ QZ_HD void std2x2(const double* A, const double* B, Std2& o) {
 // both rows, alphai > 0 on the first.
 QZ_HD void eig2_complex(const double* a, double b0, double b1, double* ar, double* ai, double* be) {
   double m00 = a[0] / b0, m01 = a[2] / b0, m10 = a[1] / b1, m11 = a[3] / b1;
+  // M = diag(b)^-1 A scaled by a power of two to at most 1 in magnitude, so
+  // that the discriminant cannot overflow for eigenvalues far from 1 in
+  // magnitude; the scaling is exact and is folded back into b, so the
+  // results are the unscaled formula's wherever that one does not overflow
+  const double mx = dmax(dmax(fabs(m00), fabs(m01)), dmax(fabs(m10), fabs(m11)));
+  int e = 0;
+  if (mx > 0.0 && isfinite(mx)) frexp(mx, &e);
+  m00 = ldexp(m00, -e); m01 = ldexp(m01, -e); m10 = ldexp(m10, -e); m11 = ldexp(m11, -e);
   double tr = 0.5 * (m00 + m11);
   double d = 0.5 * (m00 - m11);
   double disc = d * d + m01 * m10;  // < 0 for a complex pair
   double wr = tr;
   double wi = sqrt(fabs(dmin(disc, 0.0)));
-  ar[0] = wr * b0; ai[0] = wi * b0; be[0] = b0;
-  ar[1] = wr * b1; ai[1] = -wi * b1; be[1] = b1;
+  const double s0 = ldexp(b0, e), s1 = ldexp(b1, e);
+  ar[0] = wr * s0; ai[0] = wi * s0; be[0] = b0;
+  ar[1] = wr * s1; ai[1] = -wi * s1; be[1] = b1;
 }
 
 }  // namespace qz

@@ -209,11 +209,17 @@ def eig_from_schur(S, P):
         if j + 1 < n and S[j + 1, j] != 0.0:
             a = S[j:j + 2, j:j + 2]
             b11, b22 = P[j, j], P[j + 1, j + 1]
-            # eigenvalues of the 2x2 pencil with diagonal B
-            lam = np.linalg.eigvals(np.linalg.solve(np.diag([b11, b22]), a))
+            # eigenvalues of the 2x2 pencil with diagonal B, computed on
+            # diag(B)^-1 A scaled by a power of two (eigenvalues far from 1
+            # in magnitude), the scale folded back into beta's factor
+            m = np.linalg.solve(np.diag([b11, b22]), a)
+            mx = np.abs(m).max()
+            e = int(np.frexp(mx)[1]) if mx > 0 and np.isfinite(mx) else 0
+            lam = np.linalg.eigvals(np.ldexp(m, -e))
             lam = lam[np.argsort(-lam.imag)]
-            ar[j], ai[j], be[j] = lam[0].real * b11, abs(lam[0].imag) * b11, b11
-            ar[j + 1], ai[j + 1], be[j + 1] = lam[0].real * b22, -abs(lam[0].imag) * b22, b22
+            s11, s22 = np.ldexp(b11, e), np.ldexp(b22, e)
+            ar[j], ai[j], be[j] = lam[0].real * s11, abs(lam[0].imag) * s11, b11
+            ar[j + 1], ai[j + 1], be[j + 1] = lam[0].real * s22, -abs(lam[0].imag) * s22, b22
             j += 2
         else:
             ar[j], ai[j], be[j] = S[j, j], 0.0, P[j, j]

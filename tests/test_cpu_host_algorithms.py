@@ -186,6 +186,11 @@ def test_host_solve_edge_cases(pkg, lapack, host, kind):
     assert info == 0
     assert lapack.schur_structure_ok(S, P)
     assert np.all(be >= 0)
+    # the (alpha, beta) convention of the Schur form's blocks, also for
+    # eigenvalues far from 1 in magnitude
+    e = lapack.eig_from_schur(S, P)
+    for x, y in zip(e, (ar, ai, be)):
+        assert np.allclose(x, y, rtol=1e-12, atol=1e-300)
     _check(lapack, H, T, S, P, Q, Z, eig=(ar, ai, be))
 
 
