@@ -1,7 +1,7 @@
 """Benchmark: time-to-Schur of the multishift QZ path on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--n 10000] [--workload c3]
+                    [--n 10000] [--workload c3] [--mode plain|split|learned|split+learned]
 
 One step = one complete reduction of a Hessenberg-triangular pencil to
 generalized real Schur form with Q and Z (JOB='S', COMPQ=COMPZ='I').
@@ -12,28 +12,40 @@ larger than L2, so no flush is needed between steps.
 value      mean device seconds per solve (CUDA events on the solver stream),
            inputs restored from a device-resident copy before each step
            outside the timed events, in --mode (default plain: FP64 DMMA
-           updates, (nw, ns) from the fixed table; split+learned: updates
-           through 8 INT8 Ozaki slices on the tensor cores and (nw, ns) from
-           the trained MLP); the other form is timed on the same pencil
-           after it and reported under "comparison" with the speed-up of
-           split+learned over plain
+           updates, (nw, ns) from the fixed table)
+forms      the other three forms (split: INT8 Ozaki updates; learned: (nw, ns)
+           from the trained MLP; split+learned: both) timed on the same
+           pencil, each with its AED and sweep counts and backward errors;
+           "comparison" keeps the split+learned speed-up over plain
+eigen      the eigenvalues of the timed solve matched as a set against the
+           oracle port's solve of the same pencil (tests/golden fixture),
+           chordal distance in units of 50 n eps ||(H,T)||_F / s_j
 e2e        the same solve through the public C-ABI entry b200qz_solve_host
            with pinned host buffers: H, T copied in, S, P, Q, Z and the
            eigenvalues copied out inside the timed region
-roofline   the kernel with the largest device-time share in a profiled solve
-cpu_baseline / --impl reference
+roofline   the kernel with the largest device-time share in a profiled
+           solve: achieved GB/s from the algorithmic bytes of the windows it
+           actually processed; the updates' FP64 TFLOP/s against a cuBLAS
+           DGEMM measured in the same process
+cpu_baseline
            the oracle's C restatement of the reference path (oracle/qzref.c,
-           OpenBLAS with all host threads) on a bounded sample: a smaller
-           pencil of the same distribution; seconds scaled by (n/n_s)^3
+           OpenBLAS on all host threads) run on the same pencil for its first
+           AEDs only, scaled by the share of the whole solve those AEDs took
+           in the committed full-size profile (bounded to about 20 s)
+--impl reference
+           the same restatement solving the full pencil, as many whole solves
+           as fit the --ref-budget seconds (the true count is reported)
 
-Multi-GPU (torchrun): a single pencil does not shard; every rank solves its
-own replica, value = max over ranks.
+Multi-GPU: a single pencil does not shard; every rank solves its own
+replica, value = max over ranks.  Without torchrun, --gpus N > 1 starts N
+ranks itself (torch.distributed.run on 127.0.0.1).
 
 --workload c5 (batched): 2048 pencils per GPU (seed 4, n ~ U{32..512}, N(0,1),
 2% zero T diagonal) solved in one persistent graph-captured launch after an
 autotuning pass; value = pencils/s over all ranks (each rank solves its
 size-balanced shard of a global batch of 2048 x N pencils), plus the worst
-backward error over the batch.
+backward error over the batch.  --check-ranks joins the ranks on gloo and
+checks the shard partition without solving (launcher test on CPU hosts).
 """
 from __future__ import annotations
 
@@ -41,6 +53,7 @@ import argparse
 import importlib.util
 import json
 import os
+import socket
 import subprocess
 import sys
 import threading
@@ -66,6 +79,8 @@ def load_pkg():
 
 METRIC = "time-to-Schur (s) at n=10k, backward err<=50*n*eps; split+learned vs plain FP64 GPU"
 EPS = np.finfo(np.float64).eps
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+FORMS = ("plain", "split", "learned", "split+learned")
 
 
 def make_pencil(pkg, workload, n):
@@ -79,6 +94,20 @@ def make_pencil(pkg, workload, n):
     if workload == "c4":
         return P.random_ht(n, 3), "N(0,1) seed 3"
     raise ValueError(workload)
+
+
+def workload_config(pkg, workload, n, desc):
+    """The config block both arms print for a single-pencil workload."""
+    return {"workload": "%s: %s n=%d" % (workload, desc, n), "n": n, "job": "S", "compq": "I", "compz": "I",
+            "generator": pkg.pencils.GENERATOR}
+
+
+def port_fixture(workload, n):
+    """The oracle port's eigenvalues of this pencil (tests/golden), or None."""
+    p = os.path.join(GOLDEN, "port_%s_n%d.npz" % (workload, n))
+    if not os.path.exists(p):
+        return None
+    return dict(np.load(p))
 
 
 class ClockSampler:
@@ -142,70 +171,115 @@ def read_peaks():
     return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
 
 
-def read_ncu_traffic(kernel):
-    """Per-launch DRAM bytes of a kernel from the committed ncu summary
-    (profiles/ncu_<kernel>.md, line 'traffic_bytes_per_launch: X')."""
-    p = os.path.join(ROOT, "profiles", "ncu_%s.md" % kernel)
-    if not os.path.exists(p):
-        return None
-    for line in open(p):
-        if line.startswith("traffic_bytes_per_launch:"):
-            try:
-                return float(line.split(":", 1)[1].strip().split()[0])
-            except ValueError:
-                return None
-    return None
+def fp64_gemm_peak(torch, dev, n=8192, reps=3):
+    """FP64 TFLOP/s of a cuBLAS DGEMM (n^3, best of reps) on this GPU: the
+    denominator of the updates' roofline (no FP64 figure is in the measured
+    peaks)."""
+    a = torch.randn(n, n, dtype=torch.float64, device=dev)
+    b = torch.randn(n, n, dtype=torch.float64, device=dev)
+    c = a @ b
+    torch.cuda.synchronize()
+    best = 1e30
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b, out=c)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1) * 1e-3)
+    del a, b, c
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / best / 1e12
 
 
-def cpu_reference_seconds(n_target, n_sample, workload, pkg, steps=1, warmup=0):
-    """The oracle port on a bounded sample; returns (scaled seconds list, sample seconds)."""
+# ---------------------------------------------------------------------------
+# CPU: the oracle port (reference arm and cpu_baseline)
+# ---------------------------------------------------------------------------
+def _port():
     from oracle import lapack as L
     from oracle import qzref as R
     threads = os.cpu_count() or 1
     L.set_threads(threads)
-    (H, T), desc = make_pencil(pkg, workload, n_sample)
     R.lib()
-    for _ in range(warmup):
-        R.pdhgeqz(H, T, nb=60 if n_sample <= 2000 else 130)
-    samples = []
-    for _ in range(steps):
-        t0 = time.perf_counter()
-        out = R.pdhgeqz(H, T, nb=60 if n_sample <= 2000 else 130)
-        samples.append(time.perf_counter() - t0)
-        if out[7] != 0:
-            raise RuntimeError("oracle port did not converge (info=%d)" % out[7])
-    scale = (n_target / n_sample) ** 3
-    return [s * scale for s in samples], samples, threads, desc
+    return R, threads
+
+
+def port_nb(n):
+    return 130 if n > 6000 else 60
+
+
+def cpu_baseline_sample(pkg, workload, n, budget_s=20.0):
+    """The port on the benchmarked pencil itself, stopped after its first K
+    AEDs; the seconds are divided by the share of the whole solve those K
+    AEDs took in the committed full-size profile (``aed_clock``,
+    ``seconds`` of tests/golden/port_<workload>_n<n>.npz).  K is the largest
+    count whose profiled share stays within budget_s of the profiled solve.
+    Returns the baseline dict, or None without a profile."""
+    fx = port_fixture(workload, n)
+    if fx is None or "aed_clock" not in fx:
+        return None
+    clock, total = np.asarray(fx["aed_clock"]), float(fx["seconds"])
+    scale = float(fx["threads"]) / float(os.cpu_count() or 1)
+    k = int(np.searchsorted(clock, budget_s / max(scale, 1e-3), side="right"))
+    k = max(1, min(k, len(clock) - 1))
+    frac = float(clock[k]) / total
+    R, threads = _port()
+    (H, T), desc = make_pencil(pkg, workload, n)
+    t0 = time.perf_counter()
+    out = R.pdhgeqz(H, T, nb=port_nb(n), aed_limit=k)
+    dt = time.perf_counter() - t0
+    if out[7] != -2:
+        raise RuntimeError("bounded port run did not stop at its AED limit (info=%d)" % out[7])
+    return {"value": dt / frac, "unit": "s", "cores": threads, "kind": "port",
+            "sample": "oracle/qzref.c (OpenBLAS, %d threads) on this %s pencil for its first %d AEDs: %.2f s, "
+                      "divided by the %.3f share of the whole solve those AEDs took in the full-size profile "
+                      "(%s, %.1f s on %d threads)" % (threads, desc, k, dt, frac,
+                                                      "tests/golden/port_%s_n%d.npz" % (workload, n), total,
+                                                      int(fx["threads"]))}
 
 
 def run_reference(args, pkg, rank):
+    """Whole solves of the benchmarked pencil by the oracle port, as many as
+    fit the budget (at least one)."""
     if rank != 0:
         return
-    n_s = args.cpu_sample_n
-    scaled, raw, threads, desc = cpu_reference_seconds(args.n, n_s, args.workload, pkg, steps=args.steps,
-                                                       warmup=args.warmup)
-    v = float(np.mean(scaled))
-    sample = ("oracle/qzref.c (C restatement of PDHGEQZ on a 1x1 grid, OpenBLAS %d threads), "
-              "full solve of a %s pencil at n=%d, %.2f s measured, scaled by (n/%d)^3" % (threads, desc, n_s,
-                                                                                          np.mean(raw), n_s))
+    R, threads = _port()
+    (H, T), desc = make_pencil(pkg, args.workload, args.n)
+    # warm-up: one small solve (OpenBLAS thread pool, page-in of the library)
+    Hs, Ts = pkg.pencils.random_ht(300, 0)
+    R.pdhgeqz(Hs, Ts, nb=60)
+    times = []
+    t_all = time.perf_counter()
+    while len(times) < max(1, args.steps):
+        t0 = time.perf_counter()
+        out = R.pdhgeqz(H, T, nb=port_nb(args.n))
+        dt = time.perf_counter() - t0
+        if out[7] != 0:
+            raise RuntimeError("oracle port did not converge (info=%d)" % out[7])
+        times.append(dt)
+        if time.perf_counter() - t_all + dt > args.ref_budget:
+            break
+    v = float(np.mean(times))
+    sample = ("oracle/qzref.c (C restatement of PDHGEQZ on a 1x1 grid, PDHGEQZ0 regime above n=6000, OpenBLAS "
+              "%d threads): %d whole solve(s) of the %s pencil at n=%d; warm-up: one n=300 solve" %
+              (threads, len(times), desc, args.n))
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": v * 1e3, "higher_is_better": False,
+            "steps": len(times), "warmup": 1, "ms_per_step": v * 1e3, "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "%s n=%d" % (args.workload, args.n), "n": args.n, "job": "S", "compq": "I",
-                       "compz": "I", "cpu_sample_n": n_s},
+            "config": workload_config(pkg, args.workload, args.n, desc),
+            "steps_note": "whole solves within --ref-budget %.0f s (requested %d)" % (args.ref_budget, args.steps),
             "cpu_baseline": {"value": v, "unit": "s", "cores": threads, "kind": "port", "sample": sample},
             "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
-DEFAULT_MODE = "plain"
-
-
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
 def configure(pkg, solver, mode):
-    """Set the solver up for a benchmark mode: 'split' routes the
-    off-diagonal updates through 8 INT8 Ozaki slices on the tensor cores,
-    'learned' loads the trained (nw, ns) network (policy/weights.npz).
-    Returns a note on what was used."""
+    """Set the solver up for a form: 'split' routes the off-diagonal updates
+    through 8 INT8 Ozaki slices on the tensor cores, 'learned' loads the
+    trained (nw, ns) network (policy/weights.npz).  Returns a note."""
     solver.set_param("split", 8 if "split" in mode else 0)
     note = "split: 8 INT8 slices" if "split" in mode else "updates: FP64 DMMA"
     if "learned" in mode:
@@ -230,6 +304,77 @@ def errors(torch, dH0, dT0, dH, dT, dQ, dZ, n, dev):
     orth_q = torch.linalg.norm(Q.T @ Q - I).item() / (n * EPS)
     orth_z = torch.linalg.norm(Z.T @ Z - I).item() / (n * EPS)
     return res_h, res_t, orth_q, orth_z
+
+
+def eigen_match(fx, de, n):
+    """Chordal match of the solve's eigenvalues against the port's, in units
+    of 50 n eps ||(H,T)||_F / s_j (s_j: DTGSNA reciprocal condition numbers
+    in the port's Schur form).  <= 1 everywhere is a match."""
+    from oracle import lapack as L
+    e = de.cpu().numpy()
+    ar, ai, be = e[:n], e[n:2 * n], e[2 * n:]
+    tol = np.clip(50.0 * n * EPS * float(fx["norm"]) / np.maximum(fx["rcond"], 1e-300), 50.0 * n * EPS, 2.0)
+    ok, ratio, _ = L.match_eigenvalues((fx["alphar"], fx["alphai"], fx["beta"]), (ar, ai, be), tol)
+    return {"against": "oracle port (oracle/qzref.c) solve of the same pencil", "max_ratio": ratio, "match": ok,
+            "infinite": int(np.sum(be == 0.0)), "infinite_port": int(np.sum(fx["beta"] == 0.0))}
+
+
+def roofline_of(pst, phases, peaks, peak_kind, fp64_peak, split):
+    """Roofline of the dominant kernel of a profiled solve, plus the update
+    kernels' FP64 rate.  Window kernels: achieved = algorithmic bytes of the
+    windows they processed (6*8*w^2 per window of order w) / their device
+    time; launches = windows launched (AED and endgame windows; chase waves)."""
+    dom = max(phases, key=phases.get)
+    upd_ms = phases.get("aed_update", 0.0) + phases.get("chase_update", 0.0)
+    upd = {"kernel": "k_ozaki_update (INT8 tcgen05, 8 slices)" if split else "k_update_persist (DMMA FP64)",
+           "fp64_equivalent_flops": pst["update_flops"], "ms": upd_ms,
+           "achieved_tflops": pst["update_flops"] / max(upd_ms * 1e-3, 1e-12) / 1e12,
+           "peak_tflops": fp64_peak, "peak_source": "cuBLAS DGEMM 8192^3 measured in this process",
+           "frac": pst["update_flops"] / max(upd_ms * 1e-3, 1e-12) / 1e12 / fp64_peak}
+    win = {"aed": ("k_aed_win", pst["aed_bytes"], pst["aed_launches"]),
+           "chase": ("k_chase_win", pst["chase_bytes"], pst["chase_launches"])}
+    if dom in win:
+        kname, byts, launches = win[dom]
+        dur = phases[dom] * 1e-3 / max(1.0, launches)
+        ach = byts / max(launches, 1.0) / dur / 1e9
+        roof = {"kernel": kname, "bound": "hbm", "achieved": ach, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                "frac": ach / peaks["hbm_gbs"], "traffic": None, "launches": int(launches),
+                "avg_launch_ms": dur * 1e3, "bytes_per_launch": byts / max(launches, 1.0),
+                "peak_source": "%s HBM copy bandwidth (of %s)" % (peak_kind, peak_kind),
+                "traffic_note": "ncu DRAM bytes per launch: profiles/ncu_%s.md" % kname}
+    elif dom in ("aed_update", "chase_update"):
+        roof = {"kernel": upd["kernel"], "bound": "tensor", "achieved": upd["achieved_tflops"],
+                "peak": fp64_peak, "unit": "TFLOP/s", "frac": upd["frac"], "traffic": None,
+                "peak_source": upd["peak_source"]}
+    else:
+        roof = {"kernel": dom, "bound": "hbm", "achieved": None, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                "frac": None, "traffic": None}
+    roof["updates"] = upd
+    return roof
+
+
+def maybe_launch_ranks(args):
+    """python bench.py --gpus N (N > 1) outside torchrun: start N ranks with
+    torch.distributed.run on 127.0.0.1 and exit with their status."""
+    if args.gpus <= 1 or "WORLD_SIZE" in os.environ:
+        return
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node=%d" % args.gpus,
+           "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.abspath(__file__)] + sys.argv[1:]
+    sys.exit(subprocess.call(cmd))
+
+
+def init_dist(torch, world, local, backend="nccl"):
+    if world <= 1:
+        return None
+    import datetime
+    import torch.distributed as dist
+    if backend == "nccl":
+        torch.cuda.set_device(local)
+    dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+    return dist
 
 
 C5_METRIC = ("batched pencils/s: 2048 pencils per GPU, n~U{32..512}, seed 4, 2% zero T diagonal, "
@@ -262,12 +407,35 @@ def c5_cpu_pencils_per_s(pkg, sizes_all, idx, sample_every):
     return len(mats) / dt, threads, len(mats), dt
 
 
+def check_ranks(args, pkg, rank, world):
+    """Join the ranks on gloo, take this rank's shard of the batch and
+    gather every rank's shard on rank 0, which checks that the shards
+    partition the batch.  No solve (a launcher test for CPU-only hosts)."""
+    import torch
+    dist = init_dist(torch, world, 0, backend="gloo")
+    sizes_all = pkg.pencils.batch_sizes(args.batch * world, 4)
+    mine = pkg.shard.shard(sizes_all, rank, world)
+    parts = [mine]
+    if dist is not None:
+        parts = [None] * world
+        dist.all_gather_object(parts, mine)
+    if rank == 0:
+        flat = sorted(i for p in parts for i in p)
+        print(json.dumps({"check_ranks": True, "n_ranks": world, "pencils": len(sizes_all),
+                          "partition_ok": flat == list(range(len(sizes_all))),
+                          "per_rank": [len(p) for p in parts]}), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def run_batched(args, pkg, rank, world, local):
     per_rank = args.batch
     sizes_all = pkg.pencils.batch_sizes(per_rank * world, 4)
     idx = pkg.shard.shard(sizes_all, rank, world)
     wl = "c5: %d pencils per GPU (global %d), seed 4, n~U{32..512}, 2%% zero T diagonal" % (per_rank,
                                                                                          per_rank * world)
+    config = {"workload": wl, "job": "S", "compq": "I", "compz": "I", "generator": pkg.pencils.GENERATOR}
     if args.impl == "reference":
         if rank != 0:
             return
@@ -281,7 +449,7 @@ def run_batched(args, pkg, rank, world, local):
         line = {"impl": "reference", "metric": C5_METRIC, "value": v, "unit": "pencils/s", "n_gpus": args.gpus,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * per_rank / v,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-                "data": "synthetic", "config": {"workload": wl, "job": "S", "compq": "I", "compz": "I"},
+                "data": "synthetic", "config": config,
                 "cpu_baseline": {"value": v, "unit": "pencils/s", "cores": threads, "kind": "port",
                                  "sample": sample},
                 "e2e": {"value": v, "unit": "pencils/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -289,13 +457,8 @@ def run_batched(args, pkg, rank, world, local):
         return
 
     import torch
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-    else:
+    dist = init_dist(torch, world, local)
+    if dist is None:
         torch.cuda.set_device(0)
     dev = torch.cuda.current_device()
     sizes = [int(sizes_all[i]) for i in idx]
@@ -393,26 +556,25 @@ def run_batched(args, pkg, rank, world, local):
         alg_bytes = 6.0 * 8.0 * b.elems  # H, T in; H, T, Q, Z out
         peaks, peak_kind = read_peaks()
         ach = alg_bytes / t_mean / 1e9
+        config.update({
+            "parallelism": "size-balanced shards, no collective" if world > 1 else "single-gpu",
+            "l2": "inputs 2 x %.0f MB per GPU > L2; restored from device copy outside timed events"
+                  % (8 * b.elems / 1e6),
+            "autotuned": {"threads": th, "smem_max": smx, "ctas_per_sm": cps, "sample_seconds": best},
+            "worst_backward_error_neps": {"h": worst["h"], "t": worst["t"]},
+            "worst_orthogonality_neps": {"q": worst["q"], "z": worst["z"]}})
         line = {
             "metric": C5_METRIC, "value": total / t_mean, "unit": "pencils/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_mean * 1e3, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": wl, "job": "S", "compq": "I", "compz": "I",
-                       "parallelism": "size-balanced shards, no collective" if world > 1 else "single-gpu",
-                       "l2": "inputs 2 x %.0f MB per GPU > L2; restored from device copy outside timed events"
-                             % (8 * b.elems / 1e6),
-                       "autotuned": {"threads": th, "smem_max": smx, "ctas_per_sm": cps,
-                                     "sample_seconds": best},
-                       "worst_backward_error_neps": {"h": worst["h"], "t": worst["t"]},
-                       "worst_orthogonality_neps": {"q": worst["q"], "z": worst["z"]}},
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config,
             "e2e": {"value": total / e2e, "unit": "pencils/s", "h2d_bytes_per_step": 2 * 8 * b.elems,
                     "d2h_bytes_per_step": 4 * 8 * b.elems + 8 * 3 * b.neig + 4 * b.count},
             "gpu_launches": args.steps,
             "clocks": clk,
             "roofline": {"kernel": "k_batch_qz", "bound": "hbm", "achieved": ach, "peak": peaks["hbm_gbs"],
-                         "unit": "GB/s", "frac": ach / peaks["hbm_gbs"], "traffic": read_ncu_traffic("k_batch_qz"),
+                         "unit": "GB/s", "frac": ach / peaks["hbm_gbs"], "traffic": None,
                          "bytes_per_launch": alg_bytes,
-                         "peak_source": "%s HBM copy bandwidth" % peak_kind},
+                         "peak_source": "%s HBM copy bandwidth (of %s)" % (peak_kind, peak_kind)},
             "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)
@@ -429,20 +591,25 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=10000)
     ap.add_argument("--workload", default="c3")
-    ap.add_argument("--cpu-sample-n", type=int, default=2000)
+    ap.add_argument("--ref-budget", type=float, default=900.0,
+                    help="seconds of whole reference solves (--impl reference)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--param", action="append", default=[], help="solver tunable name=value")
     ap.add_argument("--batch", type=int, default=2048, help="pencils per GPU for --workload c5")
-    ap.add_argument("--mode", default=DEFAULT_MODE, choices=["split+learned", "split", "learned", "plain"],
-                    help="update arithmetic and tuning of the timed solves")
-    ap.add_argument("--no-compare", action="store_true", help="skip the comparison solves of the other form")
+    ap.add_argument("--mode", default="plain", choices=list(FORMS), help="form of the timed solves")
+    ap.add_argument("--form-steps", type=int, default=2, help="timed solves of each other form (0: skip them)")
+    ap.add_argument("--check-ranks", action="store_true", help="join the ranks and check the c5 shards only")
     args = ap.parse_args()
+    maybe_launch_ranks(args)
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     pkg = load_pkg()
 
+    if args.check_ranks:
+        check_ranks(args, pkg, rank, world)
+        return
     if args.workload == "c5":
         run_batched(args, pkg, rank, world, local)
         return
@@ -451,13 +618,8 @@ def main():
         return
 
     import torch
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-    else:
+    dist = init_dist(torch, world, local)
+    if dist is None:
         torch.cuda.set_device(0)
     dev = torch.cuda.current_device()
     n = args.n
@@ -512,78 +674,62 @@ def main():
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         t_mean = float(tt.item())
 
-    # ---- backward errors of the last timed solve (FP64 on the GPU) ----
+    # ---- accuracy of the last timed solve: backward errors (FP64 on the
+    # GPU) and the eigenvalue set against the port's solve of this pencil ----
     res_h, res_t, orth_q, orth_z = errors(torch, dH0, dT0, dH, dT, dQ, dZ, n, dev)
+    fx = port_fixture(args.workload, n)
+    eigen = eigen_match(fx, de, n) if fx is not None else None
 
-    # ---- the other form on the same pencil: split+learned when the plain
-    # FP64 form is benchmarked, plain otherwise ----
-    comparison = None
-    if not args.no_compare:
-        cmode = "split+learned" if args.mode == "plain" else "plain"
-        cnote = configure(pkg, solver, cmode)
-        one_solve()
-        ct = [one_solve()[0] for _ in range(args.steps)]
-        t_c = float(np.mean(ct))
-        if dist is not None:
-            tt = torch.tensor([t_c], dtype=torch.float64, device=dev)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            t_c = float(tt.item())
-        ce = errors(torch, dH0, dT0, dH, dT, dQ, dZ, n, dev)
-        t_plain, t_split = (t_mean, t_c) if args.mode == "plain" else (t_c, t_mean)
-        comparison = {"mode": cmode, "note": cnote, "value": t_c, "unit": "s",
-                      "split_learned_speedup_over_plain": t_plain / t_split,
-                      "backward_error_neps": {"h": ce[0], "t": ce[1]},
-                      "orthogonality_neps": {"q": ce[2], "z": ce[3]}}
+    # ---- the other forms on the same pencil ----
+    forms = {args.mode: {"value": t_mean, "aeds": last_stats["aeds"], "sweeps": last_stats["sweeps"],
+                         "note": mode_note, "backward_error_neps": {"h": res_h, "t": res_t},
+                         "orthogonality_neps": {"q": orth_q, "z": orth_z}}}
+    if args.form_steps > 0:
+        for fm in FORMS:
+            if fm == args.mode:
+                continue
+            note = configure(pkg, solver, fm)
+            one_solve()
+            ts, st = [], None
+            for _ in range(args.form_steps):
+                t, st = one_solve()
+                ts.append(t)
+            t_f = float(np.mean(ts))
+            if dist is not None:
+                tt = torch.tensor([t_f], dtype=torch.float64, device=dev)
+                dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+                t_f = float(tt.item())
+            ce = errors(torch, dH0, dT0, dH, dT, dQ, dZ, n, dev)
+            forms[fm] = {"value": t_f, "aeds": st["aeds"], "sweeps": st["sweeps"], "note": note,
+                         "backward_error_neps": {"h": ce[0], "t": ce[1]},
+                         "orthogonality_neps": {"q": ce[2], "z": ce[3]}}
         configure(pkg, solver, args.mode)
+    comparison = None
+    if "plain" in forms and "split+learned" in forms:
+        comparison = {"split_learned_speedup_over_plain": forms["plain"]["value"] / forms["split+learned"]["value"],
+                      "split_speedup_over_plain": forms["plain"]["value"] / forms["split"]["value"]
+                      if "split" in forms else None,
+                      "learned_speedup_over_plain": forms["plain"]["value"] / forms["learned"]["value"]
+                      if "learned" in forms else None}
 
-    # ---- profiled solve (untimed, in the benchmarked mode) for the phase
-    # breakdown / roofline ----
+    # ---- profiled solve (untimed, in the benchmarked form) for the phase
+    # breakdown and the roofline ----
     os.environ["B200QZ_PROFILE"] = "1"
     _, pst = one_solve()
     os.environ.pop("B200QZ_PROFILE", None)
     peaks, peak_kind = read_peaks()
     sub = ("ms_aed_smallqz", "ms_aed_reorder", "ms_aed_spike", "ms_aed_hessred")
     phases = {k[3:]: v for k, v in pst.items() if k.startswith("ms_") and k not in sub}
-    dom = max(phases, key=phases.get)
-    kernel_of = {"aed": "k_aed_win", "chase": "k_chase_win", "aed_update": "k_update_left/right",
-                 "chase_update": "k_update_left/right", "scan": "k_scan", "inf": "k_inf_win", "final": "k_eigs"}
-    nw = 80
-    split = "split" in args.mode
-    if dom in ("aed_update", "chase_update") and split:
-        # INT8 Ozaki slices: bounded by HBM (each updated entry read and
-        # written once, 16 B; window size taken as the chase window, 80)
-        upd_ms = phases.get("aed_update", 0.0) + phases.get("chase_update", 0.0)
-        bytes_alg = 16.0 * pst["update_flops"] / (2.0 * nw)
-        ach = bytes_alg / (upd_ms * 1e-3) / 1e9
-        roof = {"kernel": "k_ozaki_update (INT8 tcgen05, 8 slices)", "bound": "hbm", "achieved": ach,
-                "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": ach / peaks["hbm_gbs"],
-                "traffic": read_ncu_traffic("k_ozaki_update"),
-                "fp64_equivalent_tflops": pst["update_flops"] / (upd_ms * 1e-3) / 1e12,
-                "peak_source": "%s HBM copy bandwidth" % peak_kind}
-    elif dom in ("aed_update", "chase_update"):
-        upd_ms = phases.get("aed_update", 0.0) + phases.get("chase_update", 0.0)
-        ach = pst["update_flops"] / (upd_ms * 1e-3) / 1e12
-        fp64_peak = 37.0
-        roof = {"kernel": "k_update_left/right (DMMA FP64)", "bound": "tensor", "achieved": ach,
-                "peak": fp64_peak, "unit": "TFLOP/s", "frac": ach / fp64_peak, "traffic": None,
-                "peak_source": "datasheet FP64 tensor (no FP64 peak in MEASURED_PEAKS.json)"}
-    else:
-        launches_dom = {"aed": pst["aeds"] + pst["endgames"], "chase": pst["windows"]}.get(dom, 1)
-        bytes_per = 6.0 * 8.0 * nw * nw  # window in + out, both factors out
-        dur = phases[dom] * 1e-3 / max(1.0, launches_dom)
-        ach = bytes_per / dur / 1e9
-        kname = kernel_of.get(dom, dom)
-        roof = {"kernel": kname, "bound": "hbm", "achieved": ach, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                "frac": ach / peaks["hbm_gbs"], "traffic": read_ncu_traffic(kname),
-                "avg_launch_ms": dur * 1e3, "bytes_per_launch": bytes_per,
-                "peak_source": "%s HBM copy bandwidth" % ("measured" if peak_kind == "measured" else "fallback")}
+    fp64_peak = fp64_gemm_peak(torch, dev)
+    roof = roofline_of(pst, phases, peaks, peak_kind, fp64_peak, "split" in args.mode)
     share = {k: round(v / max(1e-9, sum(phases.values())), 4) for k, v in phases.items()}
+    aed_split = {k[7:]: round(pst[k], 1) for k in sub}
 
     # ---- end to end through the C-ABI with pinned host buffers ----
     e2e_times = []
     pin = lambda a: torch.empty(a.shape[::-1], dtype=torch.float64, pin_memory=True).numpy().T
     Hp, Tp, Qp, Zp = pin(H), pin(T), pin(H), pin(H)
-    for _ in range(max(1, args.steps)):
+    for _ in range(max(1, min(args.steps, 5))):
         np.copyto(Hp, H)
         np.copyto(Tp, T)
         t0 = time.perf_counter()
@@ -599,31 +745,30 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        scaled, raw, threads, cdesc = cpu_reference_seconds(n, args.cpu_sample_n, args.workload, pkg)
-        cpu = {"value": float(scaled[0]), "unit": "s", "cores": threads, "kind": "port",
-               "sample": "oracle/qzref.c on a %s pencil at n=%d: %.2f s measured, scaled by (%d/%d)^3"
-                         % (cdesc, args.cpu_sample_n, raw[0], n, args.cpu_sample_n)}
+        cpu = cpu_baseline_sample(pkg, args.workload, n)
 
     if rank == 0:
-        line = {
-            "metric": METRIC, "value": t_mean, "unit": "s", "n_gpus": world, "steps": args.steps,
-            "mode": args.mode, "mode_note": mode_note, "comparison": comparison,
-            "warmup": args.warmup, "ms_per_step": t_mean * 1e3, "higher_is_better": False, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "%s: %s n=%d" % (args.workload, desc, n), "n": n, "job": "S", "compq": "I",
-                       "compz": "I", "parallelism": "replicas" if world > 1 else "single-gpu",
+        config = workload_config(pkg, args.workload, n, desc)
+        config.update({"parallelism": "replicas" if world > 1 else "single-gpu",
                        "l2": "inputs 4 x %.0f MB > L2; restored from device copy outside timed events"
                              % (8 * n * n / 1e6),
                        "params": args.param,
                        "backward_error_neps": {"h": res_h, "t": res_t},
                        "orthogonality_neps": {"q": orth_q, "z": orth_z},
-                       "stats": {k: v for k, v in last_stats.items() if not k.startswith("ms_")}},
+                       "eigenvalues": eigen,
+                       "stats": {k: v for k, v in last_stats.items() if not k.startswith("ms_")}})
+        line = {
+            "metric": METRIC, "value": t_mean, "unit": "s", "n_gpus": world, "steps": args.steps,
+            "mode": args.mode, "mode_note": mode_note, "forms": forms, "comparison": comparison,
+            "warmup": args.warmup, "ms_per_step": t_mean * 1e3, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config,
             "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": 2 * 8 * n * n,
                     "d2h_bytes_per_step": 4 * 8 * n * n + 3 * 8 * n},
             "gpu_launches": launches,
             "clocks": clk,
             "roofline": roof,
             "phase_share": share,
+            "aed_ms": aed_split,
             "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)

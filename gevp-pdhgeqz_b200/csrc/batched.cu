@@ -156,6 +156,20 @@ void launch_batch(cudaStream_t st, int grid, int threads, int smem_max, int coun
                                                                 status, counter, smem_max);
 }
 
+// The same launch, returning the status of this call's own memset and
+// kernel launch (cudaLaunchKernel reports the launch error directly, so an
+// error left pending by unrelated earlier work is neither reported as ours
+// nor cleared).
+static cudaError_t launch_batch_checked(cudaStream_t st, int grid, int threads, int smem_max, int count,
+                                        const int* order, const int* nsz, const int64_t* moff, const int64_t* eoff,
+                                        double* H, double* T, double* Q, double* Z, double* AR, double* AI,
+                                        double* BE, int* status, int* counter) {
+  cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(int), st);
+  if (e != cudaSuccess) return e;
+  void* args[] = {&count, &order, &nsz, &moff, &eoff, &H, &T, &Q, &Z, &AR, &AI, &BE, &status, &counter, &smem_max};
+  return cudaLaunchKernel((const void*)k_batch_qz, dim3(grid), dim3(threads), args, batch_smem_bytes(smem_max), st);
+}
+
 // ---------------------------------------------------------------------------
 // Batched solve that allocates nothing.
 //
@@ -230,15 +244,20 @@ extern "C" int b200qz_solve_batched_noalloc(int count, const int* n, const long 
   int* d_order = (int*)(d_eoff + kNoAllocMaxPencils);
   int* d_n = d_order + kNoAllocMaxPencils;
   int* d_counter = d_n + kNoAllocMaxPencils;
-  // pageable sources: each copy returns once its source has been staged
+  // Host-to-device copies from pageable memory (the stack array `order`, and
+  // n/moff/eoff when the caller passes ordinary memory) return only after
+  // the source has been copied to a staging buffer, as the CUDA runtime
+  // documents for cudaMemcpyAsync from pageable memory, so `order` may go
+  // out of scope on return.  Page-locked n/moff/eoff are read when the
+  // stream reaches the copy: the caller keeps them unchanged until then.
   if (cudaMemcpyAsync(d_moff, moff, count * sizeof(int64_t), cudaMemcpyHostToDevice, st) != cudaSuccess ||
       cudaMemcpyAsync(d_eoff, eoff, count * sizeof(int64_t), cudaMemcpyHostToDevice, st) != cudaSuccess ||
       cudaMemcpyAsync(d_order, order, count * sizeof(int), cudaMemcpyHostToDevice, st) != cudaSuccess ||
       cudaMemcpyAsync(d_n, n, count * sizeof(int), cudaMemcpyHostToDevice, st) != cudaSuccess)
     return 10001;
-  // launch_batch zeroes the queue counter before the kernel starts
-  launch_batch(st, d->sm_count, 128, kBatchSmemMax, count, d_order, d_n, d_moff, d_eoff, h, t, q, z, alphar, alphai,
-               beta, info, d_counter);
-  return cudaGetLastError() == cudaSuccess ? 0 : 10001;
+  // the queue counter is zeroed on the stream before the kernel starts
+  const cudaError_t e = launch_batch_checked(st, d->sm_count, 128, kBatchSmemMax, count, d_order, d_n, d_moff, d_eoff,
+                                             h, t, q, z, alphar, alphai, beta, info, d_counter);
+  return e == cudaSuccess ? 0 : 10001;
 }
 

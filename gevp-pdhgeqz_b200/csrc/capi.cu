@@ -72,6 +72,20 @@ struct PhaseTimer {
   }
 };
 
+// Everything the captured batched launch depends on: a replay is valid only
+// while every field is unchanged.
+struct BatchKey {
+  // descriptors (order, n, queue counter, moff, eoff), then h, t, q, z,
+  // alphar, alphai, beta, info
+  const void* ptr[13] = {};
+  int count = -1, threads = 0, smem_max = 0, ctas_per_sm = 0;
+  bool operator==(const BatchKey& o) const {
+    for (int i = 0; i < 13; ++i)
+      if (ptr[i] != o.ptr[i]) return false;
+    return count == o.count && threads == o.threads && smem_max == o.smem_max && ctas_per_sm == o.ctas_per_sm;
+  }
+};
+
 struct b200qz_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -111,7 +125,7 @@ struct b200qz_ctx {
   int batch_threads = 128, batch_smem_max = kBatchSmemMax, batch_ctas_per_sm = 1;
   cudaGraph_t bgraph = nullptr;
   cudaGraphExec_t bexec = nullptr;
-  size_t bkey = 0;                     // hash of the captured batch layout
+  BatchKey bkey;                       // operands and configuration of the captured launch
   int sm_count = 148;
   double batch_seconds = 0.0;
   unsigned long long* hts = nullptr;  // pinned mirror
@@ -135,7 +149,22 @@ struct GpuBackend {
   int64_t ld;
   int n;
   bool wantq, wantz;
+  // JOB = 'S': full Schur form.  JOB = 'E' (eigenvalues only): the far
+  // updates of H and T stop at the active block [act_top, act_bot], the
+  // role of ILSCHR = .FALSE. (PDHGEQZ.f:132-150; LAPACK DHGEQZ's
+  // IFRSTM/ILASTM), while Q and Z still accumulate when asked for.
+  bool schur = true;
+  int act_top = 0, act_bot = 0;
   Tol tol;
+
+  void active(int ktop, int kbot) {
+    act_top = ktop;
+    act_bot = kbot;
+  }
+  // columns right of a window (left updates) end at this column + 1, rows
+  // above a window (right updates) start at this row
+  int far_col_end() const { return schur ? n : act_bot + 1; }
+  int far_row_begin() const { return schur ? 0 : act_top; }
 
   void scan(int ifirst, int kbot, int* out) {
     c->timer.begin(kPhScan, c->stream);
@@ -161,8 +190,10 @@ struct GpuBackend {
     c->timer.begin(kPhAed, c->stream);
     launch_aed(c->stream, H, T, ld, ktop, kwtop, nw, tol, c->Ua, c->Va, c->shifts, c->dinfo + 4, c->gscratch,
                c->timer.on ? c->dts : nullptr, (kwtop > ktop) ? aed_early_stop(kbot - ktop + 1) : 0,
-               c->params.aed_threads);
+               c->params.aed_threads, c->params.aed_swap_fail);
     c->stats.launches += 1;
+    c->stats.aed_launches += 1;
+    c->stats.aed_bytes += 6.0 * 8.0 * nw * nw;
     c->timer.end(c->stream);
     QZ_CK(cudaMemcpyAsync(c->hinfo + 4, c->dinfo + 4, 3 * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     QZ_CK(cudaMemcpyAsync(c->hshifts, c->shifts, 3 * nw * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
@@ -186,7 +217,6 @@ struct GpuBackend {
     info3[0] = c->hinfo[4];
     info3[1] = c->hinfo[5];
     info3[2] = c->hinfo[6];
-    if (info3[1] != 0) dump_window(ktop, kwtop, nw);
     int m = std::min(info3[0], nw);
     for (int i = 0; i < m; ++i) {
       sh[i] = c->hshifts[i];
@@ -195,33 +225,6 @@ struct GpuBackend {
     }
     c->stats.win_bytes += 2.0 * 2.0 * 8.0 * nw * nw + 2.0 * 8.0 * nw * nw;
   }
-  // With B200QZ_DUMP_DIR set, a window whose small QZ did not converge is
-  // written to <dir>/aed_fail_<kwtop>.bin (int32 nw, double spike, then the
-  // nw x nw windows of H and T, column-major) for offline study.  The
-  // kernel leaves a failed window untouched, so it is read back as it was.
-  void dump_window(int ktop, int kwtop, int nw) {
-    const char* dir = std::getenv("B200QZ_DUMP_DIR");
-    if (!dir || !*dir) return;
-    std::vector<double> hw((size_t)nw * nw), tw((size_t)nw * nw);
-    double sp = 0.0;
-    for (int j = 0; j < nw; ++j) {
-      QZ_CK(cudaMemcpy(hw.data() + (size_t)j * nw, H + kwtop + (kwtop + j) * ld, nw * sizeof(double),
-                       cudaMemcpyDeviceToHost));
-      QZ_CK(cudaMemcpy(tw.data() + (size_t)j * nw, T + kwtop + (kwtop + j) * ld, nw * sizeof(double),
-                       cudaMemcpyDeviceToHost));
-    }
-    if (kwtop > ktop) QZ_CK(cudaMemcpy(&sp, H + kwtop + (kwtop - 1) * ld, sizeof(double), cudaMemcpyDeviceToHost));
-    std::string path = std::string(dir) + "/aed_fail_" + std::to_string(kwtop) + ".bin";
-    FILE* f = std::fopen(path.c_str(), "wb");
-    if (!f) return;
-    int32_t n32 = nw;
-    std::fwrite(&n32, sizeof(n32), 1, f);
-    std::fwrite(&sp, sizeof(sp), 1, f);
-    std::fwrite(hw.data(), sizeof(double), hw.size(), f);
-    std::fwrite(tw.data(), sizeof(double), tw.size(), f);
-    std::fclose(f);
-  }
-
   // one CTA per window of the wave; window i's factors go to slot i
   void chase_wave(const WinPlan* const* wins, int nw) {
     ChaseWave wave;
@@ -231,7 +234,9 @@ struct GpuBackend {
       J.w0 = p.w; J.wk = p.wk; J.last = p.last; J.nb = p.nb; J.tmax = p.tmax;
       for (int b = 0; b < p.nb; ++b) J.bl[b] = p.bl[b];
       c->stats.win_bytes += 2.0 * 2.0 * 8.0 * p.wk * p.wk + 2.0 * 8.0 * p.wk * p.wk;
+      c->stats.chase_bytes += 6.0 * 8.0 * p.wk * p.wk;
     }
+    c->stats.chase_launches += 1;
     c->timer.begin(kPhChase, c->stream);
     launch_chase_wave(c->stream, H, T, ld, wave, nw, c->Uc, c->Vc, kUslot);
     c->timer.end(c->stream);
@@ -275,16 +280,17 @@ struct GpuBackend {
       P.W[fu] = Ub + i * ustride; P.ldw[fu] = k; P.k[fu] = k;
       P.W[fv] = Vb + i * ustride; P.ldw[fv] = k; P.k[fv] = k;
       P.nfac += 2;
-      const int right_len = n - (w0 + k);
+      const int right_len = far_col_end() - (w0 + k);
       if (right_len > 0) {
         job(L, H, w0, w0 + k, right_len, k, 1, fu);
         job(L, T, w0, w0 + k, right_len, k, 1, fu);
         c->stats.upd_flops += 2.0 * 2.0 * k * k * right_len;
       }
-      if (w0 > 0) {
-        job(R, H, 0, w0, w0, k, 0, fv);
-        job(R, T, 0, w0, w0, k, 0, fv);
-        c->stats.upd_flops += 2.0 * 2.0 * k * k * w0;
+      const int r0 = far_row_begin();
+      if (w0 > r0) {
+        job(R, H, r0, w0, w0 - r0, k, 0, fv);
+        job(R, T, r0, w0, w0 - r0, k, 0, fv);
+        c->stats.upd_flops += 2.0 * 2.0 * k * k * (w0 - r0);
       }
       if (wantq) { job(R, Q, 0, w0, n, k, 0, fu); c->stats.upd_flops += 2.0 * k * k * n; }
       if (wantz) { job(R, Z, 0, w0, n, k, 0, fv); c->stats.upd_flops += 2.0 * k * k * n; }
@@ -357,7 +363,7 @@ struct GpuBackend {
       const double* V = Vb + i * ustride;
       int k = wk[i], w0 = w[i];
       int tile = update_tile(k);
-      int right_len = n - (w0 + k);
+      int right_len = far_col_end() - (w0 + k);
       if (right_len > 0) {
         for (double* M : {H, T}) {
           UpdJob& j = L.job[L.njobs++];
@@ -366,13 +372,14 @@ struct GpuBackend {
         }
         c->stats.upd_flops += 2.0 * 2.0 * k * k * right_len;
       }
-      if (w0 > 0) {
+      const int r0 = far_row_begin();
+      if (w0 > r0) {
         for (double* M : {H, T}) {
           UpdJob& j = R.job[R.njobs++];
-          j.M = M; j.ld = ld; j.r0 = 0; j.c0 = w0; j.len = w0; j.W = V; j.ldw = k; j.k = k;
-          j.tiles = (w0 + tile - 1) / tile;
+          j.M = M; j.ld = ld; j.r0 = r0; j.c0 = w0; j.len = w0 - r0; j.W = V; j.ldw = k; j.k = k;
+          j.tiles = (w0 - r0 + tile - 1) / tile;
         }
-        c->stats.upd_flops += 2.0 * 2.0 * k * k * w0;
+        c->stats.upd_flops += 2.0 * 2.0 * k * k * (w0 - r0);
       }
       if (wantq) {
         UpdJob& j = R.job[R.njobs++];
@@ -467,6 +474,9 @@ int solve_dev_impl(b200qz_ctx* c, char job, char compq, char compz, int n, int i
   bk.n = n;
   bk.wantq = wantq;
   bk.wantz = wantz;
+  bk.schur = is(job, 'S');
+  bk.act_top = ilo - 1;
+  bk.act_bot = ihi - 1;
   Tol& tol = bk.tol;
   tol.safmin = DBL_MIN;
   tol.ulp = DBL_EPSILON;
@@ -495,7 +505,6 @@ int solve_dev_impl(b200qz_ctx* c, char job, char compq, char compz, int n, int i
   float ms = 0.f;
   QZ_CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
   c->seconds = ms * 1e-3;
-  (void)job;
   if (c->err != cudaSuccess) return 10001;
   return info;
 }
@@ -609,6 +618,7 @@ int b200qz_set_param(b200qz_ctx* c, const char* name, double value) {
   else if (k == "upd_persist") { if (v != 0 && v != 1) return -3; P.upd_persist = v; }
   else if (k == "split") { if (v != 0 && v != 7 && v != 8) return -3; P.split = v; }
   else if (k == "aed_threads") { if (v != 32 && v != 64 && v != 128) return -3; P.aed_threads = v; }
+  else if (k == "aed_swap_fail") { if (v != 0 && v != 1) return -3; P.aed_swap_fail = v; }
   else return -2;
   return 0;
 }
@@ -642,9 +652,6 @@ int b200qz_solve_host(b200qz_ctx* c, char job, char compq, char compz, int n, in
   size_t need = 4 * bytes + 3 * (size_t)n * sizeof(double);
   if (c->dbuf_bytes < need) {
     if (c->dbuf) cudaFree(c->dbuf);
-  if (c->bexec) cudaGraphExecDestroy(c->bexec);
-  if (c->bgraph) cudaGraphDestroy(c->bgraph);
-  if (c->bdesc) cudaFree(c->bdesc);
     c->dbuf = nullptr;
     c->dbuf_bytes = 0;
     QZ_CK(cudaMalloc(&c->dbuf, need));
@@ -686,14 +693,15 @@ int b200qz_get_stats(const b200qz_ctx* c, double* out, int nout) {
   if (!c || !out) return 0;
   const SolveStats& s = c->stats;
   const double* ph = c->timer.ms;
-  double v[31] = {c->seconds, (double)s.iters, (double)s.aeds, (double)s.aed_defl, (double)s.sweeps,
+  double v[35] = {c->seconds, (double)s.iters, (double)s.aeds, (double)s.aed_defl, (double)s.sweeps,
                   (double)s.chains, (double)s.windows, (double)s.endgames, (double)s.infs, (double)s.shifts,
                   s.upd_flops, s.win_bytes,
                   ph[kPhScan], ph[kPhAed], ph[kPhAedUpd], ph[kPhChase], ph[kPhChaseUpd], ph[kPhInf], ph[kPhFinal],
                   c->aed_ms[0], c->aed_ms[1], c->aed_ms[2], c->aed_ms[3], (double)s.launches,
                   (double)s.aed_fail, (double)s.exceptional, (double)s.remaining, (double)s.stop_ktop,
-                  (double)s.stop_kbot, s.last_frac, (double)s.policy_calls};
-  int k = std::min(nout, 31);
+                  (double)s.stop_kbot, s.last_frac, (double)s.policy_calls, s.aed_bytes,
+                  (double)s.aed_launches, s.chase_bytes, (double)s.chase_launches};
+  int k = std::min(nout, 35);
   for (int i = 0; i < k; ++i) out[i] = v[i];
   return k;
 }
@@ -846,13 +854,16 @@ extern "C" int b200qz_solve_batched_dev(b200qz_ctx* c, int count, const int* n, 
   int *d_order, *d_n, *d_counter;
   int64_t *d_moff, *d_eoff;
   if (batch_prepare(c, count, n, moff, eoff, &d_order, &d_n, &d_counter, &d_moff, &d_eoff) != 0) return 10001;
-  // one persistent launch, captured in a CUDA graph and replayed while the
-  // batch layout (pointers, count, configuration) stays the same
-  size_t key = std::hash<const void*>()(h) ^ (std::hash<const void*>()(t) << 1) ^ ((size_t)count << 7) ^
-               ((size_t)c->batch_threads << 3) ^ ((size_t)c->batch_smem_max << 11) ^
-               ((size_t)c->batch_ctas_per_sm << 19) ^ std::hash<const void*>()(info) ^
-               std::hash<const void*>()(alphar);
-  if (!c->bexec || key != c->bkey) {
+  // one persistent launch, captured in a CUDA graph and replayed while
+  // every operand pointer, the count and the configuration stay the same
+  BatchKey key;
+  const void* ops[13] = {d_order, d_n, d_counter, d_moff, d_eoff, h, t, q, z, alphar, alphai, beta, info};
+  for (int i = 0; i < 13; ++i) key.ptr[i] = ops[i];
+  key.count = count;
+  key.threads = c->batch_threads;
+  key.smem_max = c->batch_smem_max;
+  key.ctas_per_sm = c->batch_ctas_per_sm;
+  if (!c->bexec || !(key == c->bkey)) {
     if (c->bexec) { cudaGraphExecDestroy(c->bexec); c->bexec = nullptr; }
     if (c->bgraph) { cudaGraphDestroy(c->bgraph); c->bgraph = nullptr; }
     QZ_CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));

@@ -56,7 +56,7 @@ template <int kThreads>
 __global__ void __launch_bounds__(kThreads) k_aed_win(double* H, double* T, int64_t ld, int ktop, int kwtop,
                                                          int nw, Tol tol, double* Qw, double* Zw, double* shifts,
                                                          int* info, double* gscratch, int maxit,
-                                                         unsigned long long* ts, int nskip) {
+                                                         unsigned long long* ts, int nskip, int swapfail) {
   extern __shared__ double smem[];
   const int n = nw;
   const bool in_smem = n <= kWinSmemMax;
@@ -100,7 +100,7 @@ __global__ void __launch_bounds__(kThreads) k_aed_win(double* H, double* T, int6
   w.wantq = true;
   w.wantz = true;
   w.tol = tol;
-  cta_aed(x, w, s, shifts, shifts + n, shifts + 2 * n, maxit, nskip);
+  cta_aed(x, w, s, shifts, shifts + n, shifts + 2 * n, maxit, nskip, swapfail != 0);
   __syncthreads();
   const int m = si[8], st = si[9], tr = si[10];
   if (st == 0 && tr) {
@@ -448,15 +448,17 @@ cudaError_t kernels_init() {
 
 void launch_aed(cudaStream_t st, double* H, double* T, int64_t ld, int ktop, int kwtop, int nw, const Tol& tol,
                 double* Qw, double* Zw, double* shifts, int* info, double* gscratch, unsigned long long* ts, int nskip,
-                int threads) {
+                int threads, int swapfail) {
   const size_t sm = aed_smem_bytes(nw);
   if (threads <= 32)
-    k_aed_win<32><<<1, 32, sm, st>>>(H, T, ld, ktop, kwtop, nw, tol, Qw, Zw, shifts, info, gscratch, 30 * nw, ts, nskip);
+    k_aed_win<32><<<1, 32, sm, st>>>(H, T, ld, ktop, kwtop, nw, tol, Qw, Zw, shifts, info, gscratch, 30 * nw, ts, nskip,
+                                     swapfail);
   else if (threads <= 64)
-    k_aed_win<64><<<1, 64, sm, st>>>(H, T, ld, ktop, kwtop, nw, tol, Qw, Zw, shifts, info, gscratch, 30 * nw, ts, nskip);
+    k_aed_win<64><<<1, 64, sm, st>>>(H, T, ld, ktop, kwtop, nw, tol, Qw, Zw, shifts, info, gscratch, 30 * nw, ts, nskip,
+                                     swapfail);
   else
     k_aed_win<128><<<1, 128, sm, st>>>(H, T, ld, ktop, kwtop, nw, tol, Qw, Zw, shifts, info, gscratch, 30 * nw, ts,
-                                       nskip);
+                                       nskip, swapfail);
 }
 void launch_chase_wave(cudaStream_t st, double* H, double* T, int64_t ld, const ChaseWave& wave, int njob, double* U,
                        double* V, int64_t ustride) {

@@ -303,21 +303,30 @@ __global__ void __launch_bounds__(kOzThreads, 1) k_ozaki_update(const OzBatch B)
                        smem_u32(&mbar))
                    : "memory");
     }
-    // wait for the chunk's MMAs (bounded)
+    // wait for the chunk's MMAs (bounded); the outcome is made uniform
+    // across the CTA, and after a timeout no further MMA is issued: one more
+    // bounded wait lets the chunk in flight drain before the TMEM is freed
     {
-      uint32_t done = 0, spins = 0;
       const uint32_t parity = (uint32_t)(nc & 1);
-      while (!done && spins < kOzSpinLimit) {
-        asm volatile(
-            "{\n\t.reg .pred p;\n\t"
-            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-            "selp.b32 %0, 1, 0, p;\n\t}\n"
-            : "=r"(done)
-            : "r"(smem_u32(&mbar)), "r"(parity)
-            : "memory");
-        ++spins;
+      auto wait = [&]() {
+        uint32_t done = 0, spins = 0;
+        while (!done && spins < kOzSpinLimit) {
+          asm volatile(
+              "{\n\t.reg .pred p;\n\t"
+              "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+              "selp.b32 %0, 1, 0, p;\n\t}\n"
+              : "=r"(done)
+              : "r"(smem_u32(&mbar)), "r"(parity)
+              : "memory");
+          ++spins;
+        }
+        return done != 0;
+      };
+      ok = __syncthreads_and(wait() ? 1 : 0) != 0;
+      if (!ok) {
+        (void)wait();
+        break;
       }
-      if (!done) ok = false;
     }
     tc_fence_after();
     // epilogue in 32-column pieces: thread = row i (TMEM lane); per 8

@@ -80,6 +80,62 @@ QZ_HD void par_house_cols(X& x, MatV M, int c, const House3& h, int r_lo, int r_
     M(i, c) = a0; M(i, c + 1) = a1; M(i, c + 2) = a2;
   }
 }
+
+// One transformation applied to several vector sets at once, the items of
+// all sets spread over every thread (instead of one loop per set, which
+// leaves most threads idle when the sets are short).  Item i of a set is
+// the vector p + i*step, p + i*step + stride (+ 2*stride for a reflector).
+struct Seg {
+  double* p;
+  int64_t step;
+  int64_t stride;
+  int count;
+};
+QZ_HD Seg seg_rows(MatV M, int r, int c_lo, int c_hi) {  // rows r.. of columns c_lo..c_hi-1
+  return Seg{&M(r, c_lo), (int64_t)M.ld, 1, c_hi - c_lo};
+}
+QZ_HD Seg seg_cols(MatV M, int c, int r_lo, int r_hi) {  // columns c.. of rows r_lo..r_hi-1
+  return Seg{&M(r_lo, c), 1, (int64_t)M.ld, r_hi - r_lo};
+}
+// item idx of the sets a, b, c (a's items first): its first element and stride
+QZ_HD bool seg_item(const Seg& a, const Seg& b, const Seg& c, int idx, double*& q, int64_t& st) {
+  const int na = a.count > 0 ? a.count : 0, nb = b.count > 0 ? b.count : 0, nc = c.count > 0 ? c.count : 0;
+  if (idx < na) { q = a.p + (int64_t)idx * a.step; st = a.stride; return true; }
+  idx -= na;
+  if (idx < nb) { q = b.p + (int64_t)idx * b.step; st = b.stride; return true; }
+  idx -= nb;
+  if (idx < nc) { q = c.p + (int64_t)idx * c.step; st = c.stride; return true; }
+  return false;
+}
+QZ_HD int seg_total(const Seg& a, const Seg& b, const Seg& c) {
+  return (a.count > 0 ? a.count : 0) + (b.count > 0 ? b.count : 0) + (c.count > 0 ? c.count : 0);
+}
+template <class X>
+QZ_HD void par_house_segs(X& x, const House3& h, const Seg& a, const Seg& b, const Seg& c) {
+  const int total = seg_total(a, b, c);
+  for (int idx = x.tid; idx < total; idx += x.nt) {
+    double* q;
+    int64_t st;
+    if (!seg_item(a, b, c, idx, q, st)) break;
+    double a0 = q[0], a1 = q[st], a2 = q[2 * st];
+    house3_apply(h, a0, a1, a2);
+    q[0] = a0; q[st] = a1; q[2 * st] = a2;
+  }
+}
+template <class X>
+QZ_HD void par_rot_segs(X& x, double c, double s, const Seg& a, const Seg& b, const Seg& d) {
+  const int total = seg_total(a, b, d);
+  for (int idx = x.tid; idx < total; idx += x.nt) {
+    double* q;
+    int64_t st;
+    if (!seg_item(a, b, d, idx, q, st)) break;
+    const double u = q[0], v = q[st];
+    q[0] = c * u + s * v;
+    q[st] = -s * u + c * v;
+  }
+}
+constexpr Seg kNoSeg = Seg{nullptr, 0, 0, 0};
+
 template <class X>
 QZ_HD void par_neg_row(X& x, MatV M, int r, int c_lo, int c_hi) {
   for (int j = c_lo + x.tid; j < c_hi; j += x.nt) M(r, j) = -M(r, j);
@@ -118,14 +174,18 @@ QZ_HD void cta_std2x2(X& x, WinState& w, int j) {
   std2x2(A, B, o);
   x.sync();  // all reads of the block done before anyone writes
   int n = w.n;
-  // rows: columns j+2..n-1 (the block itself is written from o.a/o.b)
-  par_rot_rows(x, w.H, j, j + 1, o.csl, o.snl, j + 2, n);
-  par_rot_rows(x, w.T, j, j + 1, o.csl, o.snl, j + 2, n);
-  if (w.wantq) par_rot_cols(x, w.Q, j, j + 1, o.csl, o.snl, 0, n);
-  // cols: rows 0..j-1
-  par_rot_cols(x, w.H, j, j + 1, o.csr, o.snr, 0, j);
-  par_rot_cols(x, w.T, j, j + 1, o.csr, o.snr, 0, j);
-  if (w.wantz) par_rot_cols(x, w.Z, j, j + 1, o.csr, o.snr, 0, n);
+  {
+    // rows: columns j+2..n-1 (the block itself is written from o.a/o.b);
+    // cols: rows 0..j-1 (disjoint entries, so one pass)
+    const Seg sl0 = seg_rows(w.H, j, j + 2, n);
+    const Seg sl1 = seg_rows(w.T, j, j + 2, n);
+    const Seg sl2 = w.wantq ? seg_cols(w.Q, j, 0, n) : kNoSeg;
+    par_rot_segs(x, o.csl, o.snl, sl0, sl1, sl2);
+    const Seg sr0 = seg_cols(w.H, j, 0, j);
+    const Seg sr1 = seg_cols(w.T, j, 0, j);
+    const Seg sr2 = w.wantz ? seg_cols(w.Z, j, 0, n) : kNoSeg;
+    par_rot_segs(x, o.csr, o.snr, sr0, sr1, sr2);
+  }
   x.sync();
   if (o.negrow0) {
     par_neg_row(x, w.H, j, j + 2, n);
@@ -140,6 +200,90 @@ QZ_HD void cta_std2x2(X& x, WinState& w, int j) {
   if (x.tid == 0) {
     w.H(j, j) = o.a[0]; w.H(j + 1, j) = o.a[1]; w.H(j, j + 1) = o.a[2]; w.H(j + 1, j + 1) = o.a[3];
     w.T(j, j) = o.b[0]; w.T(j + 1, j) = 0.0;    w.T(j, j + 1) = o.b[2]; w.T(j + 1, j + 1) = o.b[3];
+  }
+  x.sync();
+}
+
+// ---------------------------------------------------------------------------
+// Standardise every 2x2 block of the window at once.  A block's rotations
+// touch rows j, j+1 right of the block and columns j, j+1 above it, never
+// another block's diagonal entries, so all blocks are computed in one
+// phase (one thread per block, which also writes its own 2x2 entries), all
+// row rotations (and sign changes) applied in a second and all column
+// rotations in a third.  Scratch: 6 doubles per slot, 3n in sd.
+// ---------------------------------------------------------------------------
+template <class X>
+QZ_HD void cta_std_all(X& x, WinState& w, double* sd) {
+  const int n = w.n;
+  const int nslot = n / 2;  // block starts are >= 2 apart: slot j/2 is unique
+  for (int k = x.tid; k < nslot; k += x.nt) sd[6 * k] = 0.0;
+  x.sync();
+  // phase A: block j (H(j+1, j) != 0) -> rotations, signs, new block
+  for (int j = x.tid; j + 1 < n; j += x.nt) {
+    if (w.H(j + 1, j) == 0.0 || (j > 0 && w.H(j, j - 1) != 0.0)) continue;
+    double A[4] = {w.H(j, j), w.H(j + 1, j), w.H(j, j + 1), w.H(j + 1, j + 1)};
+    double B[4] = {w.T(j, j), w.T(j + 1, j), w.T(j, j + 1), w.T(j + 1, j + 1)};
+    Std2 o;
+    std2x2(A, B, o);
+    double* r = sd + 6 * (j / 2);
+    r[0] = (double)(j + 1);
+    r[1] = o.csl; r[2] = o.snl; r[3] = o.csr; r[4] = o.snr;
+    r[5] = (double)(o.negrow0 + 2 * o.negrow1);
+    w.H(j, j) = o.a[0]; w.H(j + 1, j) = o.a[1]; w.H(j, j + 1) = o.a[2]; w.H(j + 1, j + 1) = o.a[3];
+    w.T(j, j) = o.b[0]; w.T(j + 1, j) = 0.0; w.T(j, j + 1) = o.b[2]; w.T(j + 1, j + 1) = o.b[3];
+  }
+  x.sync();
+  // phase B: row rotation then sign changes of every block; items =
+  // (block, column of H or T right of it, or row of Q)
+  const int per = 3 * n;
+  for (int idx = x.tid; idx < nslot * per; idx += x.nt) {
+    const double* r = sd + 6 * (idx / per);
+    if (r[0] == 0.0) continue;
+    const int j = (int)r[0] - 1, it = idx % per;
+    const int neg = (int)r[5];
+    double* p0;
+    double* p1;
+    if (it < n) {
+      if (it < j + 2) continue;
+      p0 = &w.H(j, it); p1 = &w.H(j + 1, it);
+    } else if (it < 2 * n) {
+      const int c = it - n;
+      if (c < j + 2) continue;
+      p0 = &w.T(j, c); p1 = &w.T(j + 1, c);
+    } else {
+      if (!w.wantq) continue;
+      const int rr = it - 2 * n;
+      p0 = &w.Q(rr, j); p1 = &w.Q(rr, j + 1);
+    }
+    const double a = *p0, b = *p1;
+    double u = r[1] * a + r[2] * b, v = -r[2] * a + r[1] * b;
+    if (neg & 1) u = -u;
+    if (neg & 2) v = -v;
+    *p0 = u; *p1 = v;
+  }
+  x.sync();
+  // phase C: column rotation of every block (H, T rows above it, Z rows)
+  for (int idx = x.tid; idx < nslot * per; idx += x.nt) {
+    const double* r = sd + 6 * (idx / per);
+    if (r[0] == 0.0) continue;
+    const int j = (int)r[0] - 1, it = idx % per;
+    double* p0;
+    double* p1;
+    if (it < n) {
+      if (it >= j) continue;
+      p0 = &w.H(it, j); p1 = &w.H(it, j + 1);
+    } else if (it < 2 * n) {
+      const int rr = it - n;
+      if (rr >= j) continue;
+      p0 = &w.T(rr, j); p1 = &w.T(rr, j + 1);
+    } else {
+      if (!w.wantz) continue;
+      const int rr = it - 2 * n;
+      p0 = &w.Z(rr, j); p1 = &w.Z(rr, j + 1);
+    }
+    const double a = *p0, b = *p1;
+    *p0 = r[3] * a + r[4] * b;
+    *p1 = -r[4] * a + r[3] * b;
   }
   x.sync();
 }
@@ -228,14 +372,20 @@ QZ_HD void cta_ds_sweep(X& x, WinState& w, int f, int l, double c2, double c1, d
       for (int rr = 0; rr < 3; ++rr) house3_apply(PR, tb[rr], tb[rr + 3], tb[rr + 6]);
       tb[1] = 0.0; tb[2] = 0.0;
       x.sync();  // everyone has read H(.,j-1) and the T block
-      par_house_rows(x, w.H, j, PL, j, n);
-      par_house_rows(x, w.T, j, PL, j + 3, n);
-      if (w.wantq) par_house_cols(x, w.Q, j, PL, 0, n);
+      {
+        const Seg sl0 = seg_rows(w.H, j, j, n);
+        const Seg sl1 = seg_rows(w.T, j, j + 3, n);
+        const Seg sl2 = w.wantq ? seg_cols(w.Q, j, 0, n) : kNoSeg;
+        par_house_segs(x, PL, sl0, sl1, sl2);
+      }
       x.sync();
-      int hr = (j + 4 < l + 1) ? j + 4 : l + 1;
-      par_house_cols(x, w.H, j, PR, 0, hr);
-      par_house_cols(x, w.T, j, PR, 0, j);
-      if (w.wantz) par_house_cols(x, w.Z, j, PR, 0, n);
+      {
+        int hr = (j + 4 < l + 1) ? j + 4 : l + 1;
+        const Seg sr0 = seg_cols(w.H, j, 0, hr);
+        const Seg sr1 = seg_cols(w.T, j, 0, j);
+        const Seg sr2 = w.wantz ? seg_cols(w.Z, j, 0, n) : kNoSeg;
+        par_house_segs(x, PR, sr0, sr1, sr2);
+      }
       if (x.tid == 0) {
         for (int cc = 0; cc < 3; ++cc)
           for (int rr = 0; rr < 3; ++rr) w.T(j + rr, j + cc) = tb[rr + 3 * cc];
@@ -255,13 +405,19 @@ QZ_HD void cta_ds_sweep(X& x, WinState& w, int f, int l, double c2, double c1, d
       rot2(cr, sr, t10, t11);
       t10 = 0.0;
       x.sync();
-      par_rot_rows(x, w.H, j, j + 1, c, s, j, n);
-      par_rot_rows(x, w.T, j, j + 1, c, s, j + 2, n);
-      if (w.wantq) par_rot_cols(x, w.Q, j, j + 1, c, s, 0, n);
+      {
+        const Seg sl0 = seg_rows(w.H, j, j, n);
+        const Seg sl1 = seg_rows(w.T, j, j + 2, n);
+        const Seg sl2 = w.wantq ? seg_cols(w.Q, j, 0, n) : kNoSeg;
+        par_rot_segs(x, c, s, sl0, sl1, sl2);
+      }
       x.sync();
-      par_rot_cols(x, w.H, j, j + 1, cr, sr, 0, l + 1);
-      par_rot_cols(x, w.T, j, j + 1, cr, sr, 0, j);
-      if (w.wantz) par_rot_cols(x, w.Z, j, j + 1, cr, sr, 0, n);
+      {
+        const Seg sr20 = seg_cols(w.H, j, 0, l + 1);
+        const Seg sr21 = seg_cols(w.T, j, 0, j);
+        const Seg sr22 = w.wantz ? seg_cols(w.Z, j, 0, n) : kNoSeg;
+        par_rot_segs(x, cr, sr, sr20, sr21, sr22);
+      }
       if (x.tid == 0) {
         w.T(j, j) = t00; w.T(j + 1, j) = 0.0; w.T(j, j + 1) = t01; w.T(j + 1, j + 1) = t11;
         w.H(j, j - 1) = r; w.H(j + 1, j - 1) = 0.0;
@@ -577,7 +733,7 @@ QZ_HD bool swap_compute(MatV Hb, MatV Tb, double* S2, double* T2, double* Qs, do
 // Thread 0 computes, everyone applies.  Returns false (nothing changed)
 // if the swap was rejected.
 template <int N1, int N2, class X>
-QZ_HD bool cta_swap_t(X& x, WinState& w, int j1) {
+QZ_HD bool cta_swap_t(X& x, WinState& w, int j1, bool restd) {
   constexpr int M = N1 + N2;
   double* sQ = x.sd;       // 16
   double* sZ = x.sd + 16;  // 16
@@ -658,30 +814,34 @@ QZ_HD bool cta_swap_t(X& x, WinState& w, int j1) {
     w.T(j1 + i % M, j1 + i / M) = sT[i];
   }
   x.sync();
-  // re-standardise the new diagonal blocks (moved block first, size N2)
-  if (N2 == 2) cta_std2x2(x, w, j1);
-  if (N1 == 2) cta_std2x2(x, w, j1 + N2);
+  // re-standardise the new diagonal blocks (moved block first, size N2);
+  // without restd they stay general 2x2 blocks (T's block not triangular)
+  // until a later cta_std_all
+  if (restd && N2 == 2) cta_std2x2(x, w, j1);
+  if (restd && N1 == 2) cta_std2x2(x, w, j1 + N2);
   return true;
 }
 
 template <class X>
-QZ_HD bool cta_swap(X& x, WinState& w, int j1, int n1, int n2) {
-  if (n1 == 1 && n2 == 1) return cta_swap_t<1, 1>(x, w, j1);
-  if (n1 == 1) return cta_swap_t<1, 2>(x, w, j1);
-  if (n2 == 1) return cta_swap_t<2, 1>(x, w, j1);
-  return cta_swap_t<2, 2>(x, w, j1);
+QZ_HD bool cta_swap(X& x, WinState& w, int j1, int n1, int n2, bool restd = true) {
+  if (n1 == 1 && n2 == 1) return cta_swap_t<1, 1>(x, w, j1, restd);
+  if (n1 == 1) return cta_swap_t<1, 2>(x, w, j1, restd);
+  if (n2 == 1) return cta_swap_t<2, 1>(x, w, j1, restd);
+  return cta_swap_t<2, 2>(x, w, j1, restd);
 }
 
 // Move the block starting at ifst (size nb) up to position ilst
 // (DTGEXC semantics for ifst > ilst).  Returns false on a rejected swap.
+// restd = false leaves the 2x2 blocks it touches unstandardised (the
+// caller standardises the window afterwards, cta_std_all).
 template <class X>
-QZ_HD bool cta_move_block(X& x, WinState& w, int ifst, int nb, int ilst) {
+QZ_HD bool cta_move_block(X& x, WinState& w, int ifst, int nb, int ilst, bool restd = true) {
   int here = ifst;
   while (here > ilst) {
     int nbn = 1;
     if (here - 2 >= ilst && w.H(here - 1, here - 2) != 0.0) nbn = 2;
     x.sync();
-    if (!cta_swap(x, w, here - nbn, nbn, nb)) return false;
+    if (!cta_swap(x, w, here - nbn, nbn, nb, restd)) return false;
     here -= nbn;
     // the moved block must keep its size (a complex pair stays 2x2)
     int nbnow = (nb == 2 && w.H(here + 1, here) != 0.0) ? 2 : 1;
@@ -694,7 +854,8 @@ QZ_HD bool cta_move_block(X& x, WinState& w, int ifst, int nb, int ilst) {
 // ---------------------------------------------------------------------------
 // Aggressive early deflation on a window (already copied into w, with
 // w.Q = w.Z = I).  s is the spike H(kwtop, kwtop-1) (0 at the top of the
-// active block).  On return:
+// active block).  swapfail makes every block swap report failure (a test
+// hook for the failure branch).  On return:
 //   si[8]  = number of undeflated eigenvalues m (positions 0..m-1)
 //   si[9]  = status (0 ok, >0 small QZ failed)
 //   si[10] = 1 if the window was transformed (nd > 0 or full solve)
@@ -705,7 +866,8 @@ QZ_HD bool cta_move_block(X& x, WinState& w, int ifst, int nb, int ilst) {
 // caller discards it (the pencil is unchanged).
 // ---------------------------------------------------------------------------
 template <class X>
-QZ_HD void cta_aed(X& x, WinState& w, double s, double* sr, double* si_, double* sb, int maxit, int nskip = 0) {
+QZ_HD void cta_aed(X& x, WinState& w, double s, double* sr, double* si_, double* sb, int maxit, int nskip = 0,
+                   bool swapfail = false) {
   int n = w.n;
   x.stamp(0);
   int info = cta_small_qz(x, w, maxit);
@@ -749,12 +911,18 @@ QZ_HD void cta_aed(X& x, WinState& w, double s, double* sr, double* si_, double*
       kb -= nb;
       fails = 0;
     } else {
-      if (!cta_move_block(x, w, kb - nb + 1, nb, ilst)) { failed = true; break; }
+      // a rejected swap ends the test: the window is re-reduced with the
+      // deflations found so far (qzearly.f:321-326); swapfail forces it
+      if (swapfail || !cta_move_block(x, w, kb - nb + 1, nb, ilst, false)) { failed = true; break; }
       ilst += nb;
       ++fails;
     }
   }
   (void)failed;
+  // the swaps left the 2x2 blocks they touched general: standardise every
+  // block of the window at once (T upper triangular again, complex pairs
+  // with a positive diagonal block of T)
+  cta_std_all(x, w, x.sd + 64);
   x.stamp(2);
   int m = kb + 1;  // undeflated eigenvalues at 0..m-1
   // ---- shifts: eigenvalues of the undeflated Schur blocks ----
@@ -925,17 +1093,24 @@ QZ_HD void cta_aed(X& x, WinState& w, double s, double* sr, double* si_, double*
       double c, sn, r;
       lartg(w.H(jr - 1, jc), w.H(jr, jc), c, sn, r);
       x.sync();
-      par_rot_rows(x, w.H, jr - 1, jr, c, sn, jc + 1, n);
-      par_rot_rows(x, w.T, jr - 1, jr, c, sn, jr - 1, n);
-      if (w.wantq) par_rot_cols(x, w.Q, jr - 1, jr, c, sn, 0, n);
+      {
+        const Seg sl0 = seg_rows(w.H, jr - 1, jc + 1, n);
+        const Seg sl1 = seg_rows(w.T, jr - 1, jr - 1, n);
+        const Seg sl2 = w.wantq ? seg_cols(w.Q, jr - 1, 0, n) : kNoSeg;
+        par_rot_segs(x, c, sn, sl0, sl1, sl2);
+      }
       if (x.tid == 0) { w.H(jr - 1, jc) = r; w.H(jr, jc) = 0.0; }
       x.sync();
       // pair (col jr, col jr-1): zero T(jr, jr-1)
       lartg(w.T(jr, jr), w.T(jr, jr - 1), c, sn, r);
       x.sync();
-      par_rot_cols(x, w.H, jr, jr - 1, c, sn, 0, m);
-      par_rot_cols(x, w.T, jr, jr - 1, c, sn, 0, jr);
-      if (w.wantz) par_rot_cols(x, w.Z, jr, jr - 1, c, sn, 0, n);
+      {
+        // columns (jr, jr-1): the pair's first member is column jr
+        const Seg sr0 = Seg{&w.H(0, jr), 1, -(int64_t)w.H.ld, m};
+        const Seg sr1 = Seg{&w.T(0, jr), 1, -(int64_t)w.T.ld, jr};
+        const Seg sr2 = w.wantz ? Seg{&w.Z(0, jr), 1, -(int64_t)w.Z.ld, n} : kNoSeg;
+        par_rot_segs(x, c, sn, sr0, sr1, sr2);
+      }
       if (x.tid == 0) { w.T(jr, jr) = r; w.T(jr, jr - 1) = 0.0; }
       x.sync();
     }

@@ -41,6 +41,8 @@ struct SolveParams {
   int upd_persist = 1;   // 1: persistent, prefetching DMMA update kernels
   int aed_limit = -1;    // >= 0: stop before the AED after this many AEDs
                          // (tuning traces; the solve then returns -2)
+  int aed_swap_fail = 0; // 1: every block swap inside the AED reports failure
+                         // (exercises the swap-failure branch, qzearly.f:321-326)
 };
 
 struct SolveStats {
@@ -55,6 +57,11 @@ struct SolveStats {
   int stop_ktop = -1, stop_kbot = -1;  // active block where an AED limit stopped the solve
   double last_frac = 0.0;  // deflated fraction of the last AED window
   int64_t policy_calls = 0;  // AED decisions taken by the learned policy
+  // algorithmic bytes and launches per window kernel (roofline accounting):
+  // a window of order w moves 6*8*w^2 bytes (H, T in; H, T, and both
+  // factors out)
+  double aed_bytes = 0.0, chase_bytes = 0.0;
+  int64_t aed_launches = 0, chase_launches = 0;
 };
 
 // reference shift-count table (piparmq.f:504-533)
@@ -198,6 +205,9 @@ inline void plan_chain(int ktop, int kbot, int W, int nb, const ShiftPair* sp, i
 //   void inf_top(int ktop)
 //   bool policy(int ktop, int kbot, double lastfrac, int* nw, int* ns)
 //                                                       // learned (nw, ns); false: use the table
+//   void active(int ktop, int kbot)                     // the active block of the next steps
+//                                                       // (bounds the far updates when only
+//                                                       // eigenvalues are wanted)
 template <class BK>
 int qz_iterate(BK& bk, int n, int ilo, int ihi, const SolveParams& P, SolveStats& S) {
   int ifirst = ilo, kbot = ihi;
@@ -227,6 +237,7 @@ int qz_iterate(BK& bk, int n, int ilo, int ihi, const SolveParams& P, SolveStats
     if (stall > P.stall_limit) return done(kbot + 1);
     if (P.verbose)
       std::fprintf(stderr, "[b200qz] it=%lld ktop=%d kbot=%d ninf=%d\n", (long long)it, ktop, kbot, ninf);
+    bk.active(ktop, kbot);
     if (ktop == kbot) {
       // a 1x1 block has converged (finite or infinite eigenvalue)
       kbot -= 1;

@@ -94,7 +94,12 @@ int b200qz_solve_host(b200qz_ctx* ctx, char job, char compq, char compz, int n, 
  * 23 kernel launches issued by the solve, 24 AED windows whose small QZ
  * did not converge (they deflate nothing and supply diagonal shifts),
  * 25 sweeps run with exceptional shifts (after 40 iterations without
- * deflation).
+ * deflation), 26 rows left unconverged, 27/28 active block where an
+ * "aed_limit" stopped the solve, 29 deflated fraction of the last AED
+ * window, 30 AED decisions taken by the learned policy, 31 algorithmic
+ * bytes of the AED/endgame window kernels (6*8*w^2 per window of order w),
+ * 32 their launches, 33 algorithmic bytes of the chase windows, 34 chase
+ * launches (one per wave of concurrent windows).
  * Returns the number of values written. */
 int b200qz_get_stats(const b200qz_ctx* ctx, double* out, int nout);
 
@@ -108,7 +113,12 @@ int b200qz_set_params(b200qz_ctx* ctx, int nw_max, int w_chase, int nmin, int ni
  * "ns_max", "maxit_factor", "chain_max" (bulges per chain), "aed_nskip"
  * (AED spike test stops after this many consecutive undeflatable blocks,
  * 0 = whole window), "max_wave" (chains chased concurrently, 1..8),
- * "stall_limit" (iterations without deflation before INFO > 0).
+ * "stall_limit" (iterations without deflation before INFO > 0),
+ * "split" (0, 7 or 8 INT8 Ozaki slices for the off-diagonal updates),
+ * "aed_threads" (32, 64 or 128), "upd_persist" (0 or 1), "aed_limit"
+ * (stop before that AED, INFO 10003), "aed_swap_fail" (1: every block swap
+ * inside the AED reports failure, which exercises the swap-failure branch
+ * of the reference, qzearly.f:321-326).
  * Returns 0, -2 for an unknown name, -3 for a value out of range. */
 int b200qz_set_param(b200qz_ctx* ctx, const char* name, double value);
 
@@ -189,19 +199,22 @@ int b200qz_batched_config(const b200qz_ctx* ctx, int* threads, int* smem_max, in
  * allocator, hosts that reserve the device heap up front, and loops where
  * an allocation could block.  Same arguments and results as
  * b200qz_solve_batched_dev (device buffers h, t, q, z, alphar, alphai,
- * beta, info; host arrays n, moff, eoff), but no context: it runs on the
- * current device and on `stream` (a cudaStream_t, NULL for the default
- * stream) and returns without waiting for the GPU.  The batch descriptors
- * and the work-queue counter live in one fixed array in the library's
- * device memory (about 96 KB, held by every GPU that loads the library
- * until the process exits), so at most 4096 pencils per call: a larger
- * count returns -2.  The first call on a device sets that device up (it
- * looks up the array's device address and raises the kernel's shared-
+ * beta, info; host arrays n, moff, eoff), but no context and its own return
+ * codes (below): it runs on the current device and on `stream` (a
+ * cudaStream_t, NULL for the default stream) and returns without waiting
+ * for the GPU.  n, moff and eoff in ordinary (pageable) memory may be
+ * reused as soon as the call returns; page-locked ones are read when the
+ * stream reaches the copy and must stay unchanged until then.  The batch
+ * descriptors and the work-queue counter live in one fixed array in the
+ * library's device memory (about 96 KB, held by every GPU that loads the
+ * library until the process exits), so at most 4096 pencils per call: a
+ * larger count returns -2.  The first call on a device sets that device up
+ * (it looks up the array's device address and raises the kernel's shared-
  * memory limit), so make it before any stream capture.  All calls share
  * the array: calls whose work overlaps on the GPU (different streams, or
  * host threads racing) corrupt each other's batches.  Returns 0, -1 bad
  * count, -2 count above 4096, -3 a size outside 1..46340, or 10001 on a
- * CUDA error.  No counterpart in the reference. */
+ * CUDA error of this call.  No counterpart in the reference. */
 int b200qz_solve_batched_noalloc(int count, const int* n, const long long* moff, const long long* eoff,
                                  double* h, double* t, double* q, double* z, double* alphar, double* alphai,
                                  double* beta, int* info, void* stream);

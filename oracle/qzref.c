@@ -23,11 +23,19 @@
  *    unwindowed Givens sequence instead of PDHGEQZ8/9's windows.
  * Column-major storage, 1-based comments, 0-based code.
  */
+#define _POSIX_C_SOURCE 199309L
 #include <math.h>
 #include <stdint.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <time.h>
+
+static double wall_seconds(void) {
+  struct timespec ts;
+  clock_gettime(CLOCK_MONOTONIC, &ts);
+  return (double)ts.tv_sec + 1e-9 * (double)ts.tv_nsec;
+}
 
 /* ---- LAPACK / BLAS through scipy's OpenBLAS ------------------------------ */
 typedef size_t flen;
@@ -73,6 +81,13 @@ typedef struct {
   /* counters */
   long iters, aeds, sweeps, smallsub, infs;
   double upd_flops;
+  /* bounded runs (CPU-baseline samples): stop before AED number aed_limit
+     (-1: never); aed_clock[k] receives the wall-clock seconds since the
+     start of the solve at which AED k began (up to aed_cap entries) */
+  long aed_limit;
+  double* aed_clock;
+  long aed_cap;
+  double t_start;
 } Ctx;
 
 /* ---- QZFCOL (src/kkqz/qzfcol.f:1-116) -----------------------------------
@@ -763,6 +778,8 @@ static int iterate(Ctx* C, int ilo, int ihi) {
       if (dblk > 1000) dblk = 1000;
       nib = imin(100, (int)ceil(335.0 * pow((double)nh, -0.44)));
     }
+    if (C->aed_limit >= 0 && C->aeds >= C->aed_limit) { free(sh); return -2; }
+    if (C->aed_clock && C->aeds < C->aed_cap) C->aed_clock[C->aeds] = wall_seconds() - C->t_start;
     C->aeds++;
     int nshift = 0;
     int nd = aed(C, ktop, kbot, dblk, sh, sh + 1024, sh + 2048, &nshift);
@@ -857,12 +874,17 @@ static void finalize(Ctx* C, double* ar, double* ai, double* be) {
  * 1x1 grid (job 'S'/'E', compq/compz 'N'/'I'/'V', 1-based ilo/ihi).
  * stats (may be NULL): iters, aeds, sweeps, small subproblems, infinite
  * eigenvalues, update flops. */
-int qzref_pdhgeqz(char job, char compq, char compz, int n, int ilo, int ihi, double* H, double* T, double* Q,
-                  double* Z, int ld, int nb, double* ar, double* ai, double* be, double* stats) {
+int qzref_pdhgeqz_ex(char job, char compq, char compz, int n, int ilo, int ihi, double* H, double* T, double* Q,
+                     double* Z, int ld, int nb, double* ar, double* ai, double* be, double* stats, long aed_limit,
+                     double* aed_clock, long aed_cap) {
   (void)job;
   if (n <= 0) return 0;
   Ctx C;
   memset(&C, 0, sizeof(C));
+  C.aed_limit = aed_limit;
+  C.aed_clock = aed_clock;
+  C.aed_cap = aed_cap;
+  C.t_start = wall_seconds();
   C.n = n; C.ld = ld; C.H = H; C.T = T; C.Q = Q; C.Z = Z;
   C.wantq = (compq != 'N' && compq != 'n');
   C.wantz = (compz != 'N' && compz != 'n');
@@ -881,12 +903,19 @@ int qzref_pdhgeqz(char job, char compq, char compz, int n, int ilo, int ihi, dou
   C.ttol = dmax(unfl, C.ulp * sqrt(tn));
   for (int i = ilo - 1; i < ihi; ++i) { ar[i] = -1.0; ai[i] = -1.0; be[i] = -1.0; }
   int info = iterate(&C, ilo - 1, ihi - 1);
-  finalize(&C, ar, ai, be);
+  if (info != -2) finalize(&C, ar, ai, be);
   if (stats) {
     stats[0] = C.iters; stats[1] = C.aeds; stats[2] = C.sweeps; stats[3] = C.smallsub; stats[4] = C.infs;
     stats[5] = C.upd_flops;
   }
   return info;
+}
+
+/* The restatement without the bounded-run options; returns INFO, or -2
+ * when an AED limit stopped it (only through qzref_pdhgeqz_ex). */
+int qzref_pdhgeqz(char job, char compq, char compz, int n, int ilo, int ihi, double* H, double* T, double* Q,
+                  double* Z, int ld, int nb, double* ar, double* ai, double* be, double* stats) {
+  return qzref_pdhgeqz_ex(job, compq, compz, n, ilo, ihi, H, T, Q, Z, ld, nb, ar, ai, be, stats, -1, NULL, 0);
 }
 
 /* ---- kernel-level restatements exported for parity tests --------------- */

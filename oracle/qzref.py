@@ -22,6 +22,8 @@ def lib():
         L.qzref_pdhgeqz.restype = ctypes.c_int
         L.qzref_pdhgeqz.argtypes = [ctypes.c_char, ctypes.c_char, ctypes.c_char, ctypes.c_int, ctypes.c_int,
                                     ctypes.c_int, _pd, _pd, _pd, _pd, ctypes.c_int, ctypes.c_int, _pd, _pd, _pd, _pd]
+        L.qzref_pdhgeqz_ex.restype = ctypes.c_int
+        L.qzref_pdhgeqz_ex.argtypes = L.qzref_pdhgeqz.argtypes + [ctypes.c_long, _pd, ctypes.c_long]
         L.qzref_dhgeqz5.restype = None
         L.qzref_dhgeqz5.argtypes = [ctypes.c_int, _pd, ctypes.c_int, _pd, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                     ctypes.c_int, _pd, _pd, _pd, _pd, _pd, ctypes.c_int]
@@ -45,8 +47,13 @@ def _p(a):
 STAT_NAMES = ("iters", "aeds", "sweeps", "small_subproblems", "infinite", "update_flops")
 
 
-def pdhgeqz(H, T, job="S", compq="I", compz="I", ilo=1, ihi=None, nb=130, Q=None, Z=None):
-    """Run the restatement.  Returns (S, P, Q, Z, alphar, alphai, beta, info, stats)."""
+def pdhgeqz(H, T, job="S", compq="I", compz="I", ilo=1, ihi=None, nb=130, Q=None, Z=None, aed_limit=-1,
+            aed_clock=None):
+    """Run the restatement.  Returns (S, P, Q, Z, alphar, alphai, beta, info, stats).
+
+    aed_limit >= 0 stops the run before that AED (info -2, for bounded
+    CPU-baseline samples); aed_clock (float64 array) receives the seconds
+    since the start at which each AED began."""
     n = H.shape[0]
     if ihi is None:
         ihi = n
@@ -56,8 +63,11 @@ def pdhgeqz(H, T, job="S", compq="I", compz="I", ilo=1, ihi=None, nb=130, Q=None
     Zm = np.array(Z if Z is not None else np.eye(n), dtype=np.float64, order="F", copy=True)
     ar, ai, be = np.zeros(n), np.zeros(n), np.zeros(n)
     st = np.zeros(8)
-    info = lib().qzref_pdhgeqz(job.encode(), compq.encode(), compz.encode(), n, ilo, ihi, _p(S), _p(P), _p(Qm),
-                               _p(Zm), max(1, n), nb, _p(ar), _p(ai), _p(be), _p(st))
+    clk = aed_clock if aed_clock is not None else np.zeros(1)
+    info = lib().qzref_pdhgeqz_ex(job.encode(), compq.encode(), compz.encode(), n, ilo, ihi, _p(S), _p(P), _p(Qm),
+                                  _p(Zm), max(1, n), nb, _p(ar), _p(ai), _p(be), _p(st), int(aed_limit),
+                                  _p(clk) if aed_clock is not None else None,
+                                  len(clk) if aed_clock is not None else 0)
     return S, P, Qm, Zm, ar, ai, be, info, dict(zip(STAT_NAMES, st[:6].tolist()))
 
 

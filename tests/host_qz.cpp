@@ -63,6 +63,13 @@ struct HostBK {
   double *H, *T, *Q, *Z;
   bool wantq = true, wantz = true;
   int nskip = 4;
+  int swapfail = 0;
+  // JOB = 'E': far updates of H and T stop at the active block (as in the
+  // device backend)
+  bool schur = true;
+  int act_top = 0, act_bot = 0;
+  int far_col_end() const { return schur ? n : act_bot + 1; }
+  int far_row_begin() const { return schur ? 0 : act_top; }
   Tol tol;
   HostExec x;
   std::vector<double> Ua, Va;                 // last AED window factors
@@ -113,7 +120,8 @@ struct HostBK {
     WinState w;
     w.n = nw; w.H = MatV{Hs.data(), nw}; w.T = MatV{Ts.data(), nw}; w.Q = MatV{Us.data(), nw};
     w.Z = MatV{Vs.data(), nw}; w.wantq = true; w.wantz = true; w.tol = tol;
-    cta_aed(x, w, s, s3.data(), s3.data() + nw, s3.data() + 2 * nw, 30 * nw, (kwtop > ktop) ? nskip : 0);
+    cta_aed(x, w, s, s3.data(), s3.data() + nw, s3.data() + 2 * nw, 30 * nw, (kwtop > ktop) ? nskip : 0,
+            swapfail != 0);
     const int m = x.si[8], st = x.si[9], tr = x.si[10];
     if (st == 0 && tr) {
       store(kwtop, nw, Hs, Ts);
@@ -130,7 +138,7 @@ struct HostBK {
   void apply_left(int w, int wk, const std::vector<double>& U) {
     std::vector<double> col(wk);
     for (double* M : {H, T})
-      for (int c = w + wk; c < n; ++c) {
+      for (int c = w + wk; c < far_col_end(); ++c) {
         for (int i = 0; i < wk; ++i) {
           double a = 0.0;
           for (int k = 0; k < wk; ++k) a += U[k + (size_t)i * wk] * M[(w + k) + (size_t)c * ld];
@@ -141,8 +149,8 @@ struct HostBK {
   }
   void apply_right(int w, int wk, const std::vector<double>& U, const std::vector<double>& V) {
     std::vector<double> row(wk);
-    auto right = [&](double* M, int rows, const std::vector<double>& W) {
-      for (int r = 0; r < rows; ++r) {
+    auto right = [&](double* M, int r0, int rows, const std::vector<double>& W) {
+      for (int r = r0; r < rows; ++r) {
         for (int j = 0; j < wk; ++j) {
           double a = 0.0;
           for (int k = 0; k < wk; ++k) a += M[r + (size_t)(w + k) * ld] * W[k + (size_t)j * wk];
@@ -151,10 +159,10 @@ struct HostBK {
         for (int j = 0; j < wk; ++j) M[r + (size_t)(w + j) * ld] = row[j];
       }
     };
-    right(H, w, V);
-    right(T, w, V);
-    if (wantq) right(Q, n, U);
-    if (wantz) right(Z, n, V);
+    right(H, far_row_begin(), w, V);
+    right(T, far_row_begin(), w, V);
+    if (wantq) right(Q, 0, n, U);
+    if (wantz) right(Z, 0, n, V);
   }
   void update(int w, int wk, int which) {
     const std::vector<double>& U = which == 0 ? Ua : Uc[0];
@@ -210,6 +218,10 @@ struct HostBK {
     h(f + 1, f) = 0.0;
   }
   bool policy(int, int, double, int*, int*) { return false; }
+  void active(int ktop, int kbot) {
+    act_top = ktop;
+    act_bot = kbot;
+  }
 };
 
 }  // namespace
@@ -275,6 +287,39 @@ int host_solve(int n, double* H, double* T, double* Q, double* Z, int nw_max, in
   int info = (n > 0) ? qz_iterate(bk, n, 0, n - 1, P, S) : 0;
   if (e != 0)
     for (size_t i = 0; i < (size_t)n * n; ++i) T[i] = ldexp(T[i], -e);
+  if (info == 0) {
+    WinState w;
+    w.n = n; w.H = MatV{H, n}; w.T = MatV{T, n}; w.Q = MatV{Q, n}; w.Z = MatV{Z, n};
+    w.wantq = w.wantz = true;
+    w.tol = bk.tol;
+    cta_finalize(bk.x, w, ar, ai, be);
+  }
+  stats[0] = (int)S.iters; stats[1] = (int)S.aeds; stats[2] = (int)S.sweeps; stats[3] = (int)S.windows;
+  stats[4] = (int)S.infs;
+  return info;
+}
+
+// The same with more controls: ip = {nw_max, w_chase, nmin, nskip,
+// stall_limit, aed_swap_fail, schur (1: JOB='S', 0: JOB='E')}.  Returns
+// INFO (0, or the 1-based unconverged row).  The eigenvalues are read from
+// the diagonal blocks also for JOB='E'.
+int host_solve_p(int n, double* H, double* T, double* Q, double* Z, const int* ip, double* ar, double* ai, double* be,
+                 int* stats) {
+  HostBK bk;
+  bk.n = n; bk.ld = n; bk.H = H; bk.T = T; bk.Q = Q; bk.Z = Z; bk.nskip = ip[3];
+  bk.swapfail = ip[5];
+  bk.schur = ip[6] != 0;
+  bk.act_top = 0;
+  bk.act_bot = n - 1;
+  bk.tol = make_tol(H, T, n, 0, n);
+  for (int j = 0; j < n; ++j)
+    for (int i = 0; i < n; ++i) { Q[i + (size_t)j * n] = (i == j); Z[i + (size_t)j * n] = (i == j); }
+  SolveParams P;
+  P.nw_max = ip[0]; P.w_chase = ip[1]; P.nmin = ip[2];
+  P.stall_limit = ip[4];
+  P.aed_swap_fail = ip[5];
+  SolveStats S;
+  int info = (n > 0) ? qz_iterate(bk, n, 0, n - 1, P, S) : 0;
   if (info == 0) {
     WinState w;
     w.n = n; w.H = MatV{H, n}; w.T = MatV{T, n}; w.Q = MatV{Q, n}; w.Z = MatV{Z, n};

@@ -31,6 +31,8 @@ def host(tmp_path_factory):
     L.host_solve.restype = ctypes.c_int
     L.host_chase.argtypes = [ctypes.c_int] + [_pd] * 4 + [_pi, _pd] + [ctypes.c_int] * 3
     L.host_chase.restype = None
+    L.host_solve_p.argtypes = [ctypes.c_int] + [_pd] * 4 + [_pi] + [_pd] * 3 + [_pi]
+    L.host_solve_p.restype = ctypes.c_int
     return L
 
 
@@ -207,3 +209,59 @@ def test_host_solve_default_windows(pkg, lapack, host):
     assert info == 0 and st[2] > 0
     assert lapack.schur_structure_ok(S, P)
     _check(lapack, H, T, S, P, Q, Z, eig=(ar, ai, be))
+
+
+def _solve_p(host, H, T, nw=32, wc=40, nmin=40, nskip=4, stall=300, swapfail=0, schur=1):
+    n = H.shape[0]
+    S, P, Q, Z = (np.array(M, order="F", copy=True) for M in (H, T, np.zeros((n, n)), np.zeros((n, n))))
+    ar, ai, be = np.zeros(n), np.zeros(n), np.zeros(n)
+    st = np.zeros(5, dtype=np.int32)
+    ip = np.array([nw, wc, nmin, nskip, stall, swapfail, schur], dtype=np.int32)
+    info = host.host_solve_p(n, _p(S), _p(P), _p(Q), _p(Z), ip.ctypes.data_as(_pi), _p(ar), _p(ai), _p(be),
+                             st.ctypes.data_as(_pi))
+    return info, (S, P, Q, Z), (ar, ai, be), st
+
+
+def test_host_swap_failure_branch(pkg, lapack, host):
+    """Every AED block swap reports failure: each AED keeps the deflations
+    found before its first undeflatable block and re-reduces the window
+    (the reference's branch at qzearly.f:321-326); the solve converges."""
+    H, T = pkg.pencils.random_ht(220, 51)
+    info, (S, P, Q, Z), eig, st = _solve_p(host, H, T, swapfail=1)
+    assert info == 0 and st[1] > 0
+    assert lapack.schur_structure_ok(S, P)
+    _check(lapack, H, T, S, P, Q, Z, eig=eig)
+
+
+def test_host_no_convergence_info(pkg, lapack, host):
+    """Cyclic pencil (H a cyclic shift, T = I) with a stall limit of two
+    iterations: INFO is the 1-based row where the iteration stopped
+    (PDHGEQZ0.f:1207) and the pencil is still an orthogonal equivalence of
+    the input."""
+    n = 120
+    H = np.zeros((n, n), order="F")
+    H[np.arange(1, n), np.arange(n - 1)] = 1.0
+    H[0, n - 1] = 1.0
+    T = np.eye(n, order="F")
+    info, (S, P, Q, Z), _, st = _solve_p(host, H, T, nw=48, wc=80, nmin=4, stall=2)
+    assert 0 < info <= n, info
+    r = lapack.residuals(H, T, S, P, Q, Z)
+    for key in ("h", "t", "q", "z"):
+        assert r[key] <= 50 * r["neps"], (key, r[key] / r["neps"])
+
+
+@pytest.mark.parametrize("kind", ["r", "z"])
+def test_host_job_e(pkg, lapack, host, kind):
+    """JOB='E': far updates of H and T stop at the active block; the
+    eigenvalues read from the diagonal blocks still match LAPACK, and Q, Z
+    stay orthogonal."""
+    n = 260
+    H, T = pkg.pencils.random_ht(n, 52, 0.05 if kind == "z" else 0.0)
+    info, (S, P, Q, Z), (ar, ai, be), st = _solve_p(host, H, T, schur=0)
+    assert info == 0 and st[2] > 0
+    So, Po, lar, lai, lbe, _, _, _ = lapack.dhgeqz(H, T)
+    ok, ratio, _ = lapack.match_eigenvalues((lar, lai, lbe), (ar, ai, be), lapack.eig_tolerance(So, Po, H, T))
+    assert ok, ratio
+    eps = np.finfo(float).eps
+    assert np.linalg.norm(Q.T @ Q - np.eye(n)) <= 50 * n * eps
+    assert np.linalg.norm(Z.T @ Z - np.eye(n)) <= 50 * n * eps

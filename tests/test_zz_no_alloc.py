@@ -61,9 +61,18 @@ def test_noalloc_matches_batched_entry(pkg):
     tol = 50 * int(b.n.max()) * EPS
     for call in range(2):
         out = _buffers(torch, b, h0, t0)
+        torch.cuda.synchronize()
+        free0 = torch.cuda.mem_get_info()[0]
+        stats0 = torch.cuda.memory_stats().get("allocation.all.allocated", 0)
         rc = _noalloc(pkg, b, *out, stream=torch.cuda.current_stream().cuda_stream)
         assert rc == 0, (call, rc)
         torch.cuda.synchronize()
+        if call == 1:
+            # the call itself took no device memory: neither the driver's free
+            # count nor torch's allocator moved (the first call may load the
+            # kernel module, so only the second one is checked)
+            assert torch.cuda.mem_get_info()[0] == free0
+            assert torch.cuda.memory_stats().get("allocation.all.allocated", 0) == stats0
         assert torch.equal(out[5], ref[5]), call
         for a, r in zip(out[:4], ref[:4]):
             assert float(torch.max(torch.abs(a - r))) <= tol * max(1.0, nrm), call
