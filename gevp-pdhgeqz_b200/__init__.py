@@ -68,7 +68,8 @@ STAT_NAMES = ("seconds", "iters", "aeds", "aed_deflations", "sweeps", "chains", 
               "ms_scan", "ms_aed", "ms_aed_update", "ms_chase", "ms_chase_update", "ms_inf", "ms_final",
               "ms_aed_smallqz", "ms_aed_reorder", "ms_aed_spike", "ms_aed_hessred", "launches",
               "aed_failures", "exceptional_sweeps", "remaining", "stop_ktop", "stop_kbot", "last_aed_fraction",
-              "policy_calls", "aed_bytes", "aed_launches", "chase_bytes", "chase_launches")
+              "policy_calls", "aed_bytes", "aed_launches", "chase_bytes", "chase_launches",
+              "aed_qz_steps", "aed_swaps", "aed_rotations")
 
 
 def lib() -> ctypes.CDLL:

@@ -31,6 +31,7 @@ struct BExec {
   double* sd;
   __device__ void sync() { __syncthreads(); }
   __device__ void stamp(int) {}
+  __device__ void count(int) {}
 };
 
 __device__ __forceinline__ double block_sum(double v, double* red) {

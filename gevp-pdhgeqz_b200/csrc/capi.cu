@@ -130,6 +130,7 @@ struct b200qz_ctx {
   double batch_seconds = 0.0;
   unsigned long long* hts = nullptr;  // pinned mirror
   double aed_ms[4] = {0, 0, 0, 0};   // small QZ, reorder, spike+RQ, HT re-reduction
+  double aed_counts[3] = {0, 0, 0};  // small-QZ steps, block swaps, re-reduction rotation pairs
 };
 
 namespace {
@@ -190,7 +191,7 @@ struct GpuBackend {
     c->timer.begin(kPhAed, c->stream);
     launch_aed(c->stream, H, T, ld, ktop, kwtop, nw, tol, c->Ua, c->Va, c->shifts, c->dinfo + 4, c->gscratch,
                c->timer.on ? c->dts : nullptr, (kwtop > ktop) ? aed_early_stop(kbot - ktop + 1) : 0,
-               c->params.aed_threads, c->params.aed_swap_fail);
+               c->params.aed_threads, c->params.aed_swap_fail, c->params.aed_ms);
     c->stats.launches += 1;
     c->stats.aed_launches += 1;
     c->stats.aed_bytes += 6.0 * 8.0 * nw * nw;
@@ -210,6 +211,9 @@ struct GpuBackend {
         c->aed_ms[2] += (t[3] - t[2]) * 1e-6;
         c->aed_ms[3] += (t[4] - t[3]) * 1e-6;
       }
+      c->aed_counts[0] += (double)t[5];
+      c->aed_counts[1] += (double)t[6];
+      c->aed_counts[2] += (double)t[7];
       for (int i = 0; i < 8; ++i) t[i] = 0;
       QZ_CK(cudaMemsetAsync(c->dts, 0, 8 * sizeof(unsigned long long), c->stream));
     }
@@ -425,6 +429,7 @@ int solve_dev_impl(b200qz_ctx* c, char job, char compq, char compz, int n, int i
     c->timer.on = (p && *p && *p != '0');
     c->timer.reset();
     for (double& a : c->aed_ms) a = 0.0;
+    for (double& a : c->aed_counts) a = 0.0;
   }
   QZ_CK(cudaSetDevice(c->device));
   bool wantq = !is(compq, 'N'), wantz = !is(compz, 'N');
@@ -619,6 +624,7 @@ int b200qz_set_param(b200qz_ctx* c, const char* name, double value) {
   else if (k == "split") { if (v != 0 && v != 7 && v != 8) return -3; P.split = v; }
   else if (k == "aed_threads") { if (v != 32 && v != 64 && v != 128) return -3; P.aed_threads = v; }
   else if (k == "aed_swap_fail") { if (v != 0 && v != 1) return -3; P.aed_swap_fail = v; }
+  else if (k == "aed_ms") { if (v != 0 && v != 1) return -3; P.aed_ms = v; }
   else return -2;
   return 0;
 }
@@ -693,15 +699,16 @@ int b200qz_get_stats(const b200qz_ctx* c, double* out, int nout) {
   if (!c || !out) return 0;
   const SolveStats& s = c->stats;
   const double* ph = c->timer.ms;
-  double v[35] = {c->seconds, (double)s.iters, (double)s.aeds, (double)s.aed_defl, (double)s.sweeps,
+  double v[38] = {c->seconds, (double)s.iters, (double)s.aeds, (double)s.aed_defl, (double)s.sweeps,
                   (double)s.chains, (double)s.windows, (double)s.endgames, (double)s.infs, (double)s.shifts,
                   s.upd_flops, s.win_bytes,
                   ph[kPhScan], ph[kPhAed], ph[kPhAedUpd], ph[kPhChase], ph[kPhChaseUpd], ph[kPhInf], ph[kPhFinal],
                   c->aed_ms[0], c->aed_ms[1], c->aed_ms[2], c->aed_ms[3], (double)s.launches,
                   (double)s.aed_fail, (double)s.exceptional, (double)s.remaining, (double)s.stop_ktop,
                   (double)s.stop_kbot, s.last_frac, (double)s.policy_calls, s.aed_bytes,
-                  (double)s.aed_launches, s.chase_bytes, (double)s.chase_launches};
-  int k = std::min(nout, 35);
+                  (double)s.aed_launches, s.chase_bytes, (double)s.chase_launches, c->aed_counts[0],
+                  c->aed_counts[1], c->aed_counts[2]};
+  int k = std::min(nout, 38);
   for (int i = 0; i < k; ++i) out[i] = v[i];
   return k;
 }

@@ -15,7 +15,7 @@
 #include <stdint.h>
 
 #define QZ_DEFINE_UPDATE_KERNELS
-#include "qz_chase.cuh"
+#include "qz_window.cuh"
 #include "update.cuh"
 #include "kernels.h"
 
@@ -40,6 +40,11 @@ struct DevExecT {
       ts[k] = t;
     }
   }
+  // event counters (profiling): 0 small-QZ steps, 1 block swaps, 2
+  // re-reduction rotation pairs
+  __device__ void count(int k) {
+    if (ts && tid == 0) ts[5 + k] += 1;
+  }
 };
 
 using DevExec = DevExecT<false>;
@@ -56,7 +61,7 @@ template <int kThreads>
 __global__ void __launch_bounds__(kThreads) k_aed_win(double* H, double* T, int64_t ld, int ktop, int kwtop,
                                                          int nw, Tol tol, double* Qw, double* Zw, double* shifts,
                                                          int* info, double* gscratch, int maxit,
-                                                         unsigned long long* ts, int nskip, int swapfail) {
+                                                         unsigned long long* ts, int nskip, int swapfail, int ms) {
   extern __shared__ double smem[];
   const int n = nw;
   const bool in_smem = n <= kWinSmemMax;
@@ -80,7 +85,9 @@ __global__ void __launch_bounds__(kThreads) k_aed_win(double* H, double* T, int6
     Zs = Zw;
     sd = smem;
   }
-  int* si = (int*)(sd + 64 + 4 * n);
+  // sd: 64 doubles of swap/spike scalars, 4n of spike vectors, then the
+  // multishift window QZ's scratch
+  int* si = (int*)(sd + 64 + 4 * n + kMsScratch);
   DevExecT<kThreads == 32> x{(int)threadIdx.x, kThreads, si, sd, ts};
   for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
     int i = idx % n, j = idx / n;
@@ -100,7 +107,7 @@ __global__ void __launch_bounds__(kThreads) k_aed_win(double* H, double* T, int6
   w.wantq = true;
   w.wantz = true;
   w.tol = tol;
-  cta_aed(x, w, s, shifts, shifts + n, shifts + 2 * n, maxit, nskip, swapfail != 0);
+  cta_aed(x, w, s, shifts, shifts + n, shifts + 2 * n, maxit, nskip, swapfail != 0, ms ? sd + 64 + 4 * n : nullptr);
   __syncthreads();
   const int m = si[8], st = si[9], tr = si[10];
   if (st == 0 && tr) {
@@ -387,7 +394,7 @@ __global__ void k_scale_pow2(double* A, int64_t ld, int n, int e) {
 // ---------------------------------------------------------------------------
 size_t aed_smem_bytes(int nw) {
   size_t d = (nw <= kWinSmemMax) ? (size_t)4 * nw * smem_ld(nw) : 0;
-  d += 64 + 4 * (size_t)nw;
+  d += 64 + 4 * (size_t)nw + kMsScratch;
   return d * sizeof(double) + kSi * sizeof(int);
 }
 size_t chase_smem_bytes(int wk) {
@@ -448,17 +455,17 @@ cudaError_t kernels_init() {
 
 void launch_aed(cudaStream_t st, double* H, double* T, int64_t ld, int ktop, int kwtop, int nw, const Tol& tol,
                 double* Qw, double* Zw, double* shifts, int* info, double* gscratch, unsigned long long* ts, int nskip,
-                int threads, int swapfail) {
+                int threads, int swapfail, int ms) {
   const size_t sm = aed_smem_bytes(nw);
   if (threads <= 32)
     k_aed_win<32><<<1, 32, sm, st>>>(H, T, ld, ktop, kwtop, nw, tol, Qw, Zw, shifts, info, gscratch, 30 * nw, ts, nskip,
-                                     swapfail);
+                                     swapfail, ms);
   else if (threads <= 64)
     k_aed_win<64><<<1, 64, sm, st>>>(H, T, ld, ktop, kwtop, nw, tol, Qw, Zw, shifts, info, gscratch, 30 * nw, ts, nskip,
-                                     swapfail);
+                                     swapfail, ms);
   else
     k_aed_win<128><<<1, 128, sm, st>>>(H, T, ld, ktop, kwtop, nw, tol, Qw, Zw, shifts, info, gscratch, 30 * nw, ts,
-                                       nskip, swapfail);
+                                       nskip, swapfail, ms);
 }
 void launch_chase_wave(cudaStream_t st, double* H, double* T, int64_t ld, const ChaseWave& wave, int njob, double* U,
                        double* V, int64_t ustride) {

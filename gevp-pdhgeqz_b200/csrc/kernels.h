@@ -3,7 +3,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
-#include "qz_chase.cuh"
+#include "qz_window.cuh"
 #include "update.cuh"
 
 namespace qz {
@@ -46,7 +46,8 @@ cudaError_t kernels_init();
 
 void launch_aed(cudaStream_t st, double* H, double* T, int64_t ld, int ktop, int kwtop, int nw, const Tol& tol,
                 double* Qw, double* Zw, double* shifts, int* info, double* gscratch,
-                unsigned long long* ts = nullptr, int nskip = 0, int threads = kWinThreads, int swapfail = 0);
+                unsigned long long* ts = nullptr, int nskip = 0, int threads = kWinThreads, int swapfail = 0,
+                int ms = 1);
 // one CTA per job; job i writes its factors to U + i*ustride, V + i*ustride
 void launch_chase_wave(cudaStream_t st, double* H, double* T, int64_t ld, const ChaseWave& wave, int njob, double* U,
                        double* V, int64_t ustride);

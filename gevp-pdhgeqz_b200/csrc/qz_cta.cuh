@@ -4,6 +4,7 @@
 //   int tid, nt;   thread index / count inside the block
 //   void sync();   block barrier
 //   void stamp(int k);  optional phase timestamp k (profiling)
+//   void count(int k);  optional event counter k (profiling)
 //   int* si; double* sd;  small shared scratch (>= 64 ints, >= 256 doubles)
 // On the device X is a thin wrapper over threadIdx/__syncthreads and shared
 // memory.  Data-parallel loops are written "for (i = tid; i < n; i += nt)"
@@ -21,9 +22,7 @@
 //    generalized real Schur form by direct swapping (generalized Sylvester
 //    equation, Kagstrom-Poromaa), the role of DTGEXC/DTGEX2
 //    (src/reorder/dtgexc.f, dtgex2.f) called at qzearly.f:315.
-//  * cta_aed: aggressive early deflation on a window: Schur form, spike
-//    test, reordering, spike reflector, RQ-update of T and Givens
-//    Hessenberg-triangular re-reduction (qzearly.f:229-449).
+// The AED routine built on these (cta_aed) is in qz_window.cuh.
 #pragma once
 #include "qz_prims.cuh"
 
@@ -134,7 +133,7 @@ QZ_HD void par_rot_segs(X& x, double c, double s, const Seg& a, const Seg& b, co
     q[st] = -s * u + c * v;
   }
 }
-constexpr Seg kNoSeg = Seg{nullptr, 0, 0, 0};
+QZ_HD Seg no_seg() { return Seg{nullptr, 0, 0, 0}; }
 
 template <class X>
 QZ_HD void par_neg_row(X& x, MatV M, int r, int c_lo, int c_hi) {
@@ -179,11 +178,11 @@ QZ_HD void cta_std2x2(X& x, WinState& w, int j) {
     // cols: rows 0..j-1 (disjoint entries, so one pass)
     const Seg sl0 = seg_rows(w.H, j, j + 2, n);
     const Seg sl1 = seg_rows(w.T, j, j + 2, n);
-    const Seg sl2 = w.wantq ? seg_cols(w.Q, j, 0, n) : kNoSeg;
+    const Seg sl2 = w.wantq ? seg_cols(w.Q, j, 0, n) : no_seg();
     par_rot_segs(x, o.csl, o.snl, sl0, sl1, sl2);
     const Seg sr0 = seg_cols(w.H, j, 0, j);
     const Seg sr1 = seg_cols(w.T, j, 0, j);
-    const Seg sr2 = w.wantz ? seg_cols(w.Z, j, 0, n) : kNoSeg;
+    const Seg sr2 = w.wantz ? seg_cols(w.Z, j, 0, n) : no_seg();
     par_rot_segs(x, o.csr, o.snr, sr0, sr1, sr2);
   }
   x.sync();
@@ -347,11 +346,20 @@ QZ_HD void cta_inf_chase_down(X& x, WinState& w, int f, int jz, int l) {
 // ---------------------------------------------------------------------------
 // One implicit double-shift QZ sweep over the active block [f, l]
 // (l - f + 1 >= 3) with shift polynomial c2*M^2 - c1*M + c0.
+//
+// Two barriers per step.  Every thread computes the step's reflectors from
+// the bulge column and the T block; thread 0 also forms the small block
+// that both reflectors touch (H rows j..j+3 x columns j..j+2, the T block)
+// in registers.  After the first barrier (all inputs read) the far parts
+// (rows j..j+2 right of the block, columns j..j+2 above it, Q and Z), which
+// are disjoint, are transformed in one pass over all threads while thread 0
+// stores its block; the second barrier publishes the step.
 // ---------------------------------------------------------------------------
 template <class X>
 QZ_HD void cta_ds_sweep(X& x, WinState& w, int f, int l, double c2, double c1, double c0) {
   int n = w.n;
   for (int j = f; j < l; ++j) {
+    x.count(0);
     if (j < l - 1) {
       // ---- 3x3 step at rows/cols j..j+2 ----
       double a0, a1, a2;
@@ -371,24 +379,38 @@ QZ_HD void cta_ds_sweep(X& x, WinState& w, int f, int l, double c2, double c1, d
       opposite_house3(tb, PR);
       for (int rr = 0; rr < 3; ++rr) house3_apply(PR, tb[rr], tb[rr + 3], tb[rr + 6]);
       tb[1] = 0.0; tb[2] = 0.0;
-      x.sync();  // everyone has read H(.,j-1) and the T block
-      {
-        const Seg sl0 = seg_rows(w.H, j, j, n);
-        const Seg sl1 = seg_rows(w.T, j, j + 3, n);
-        const Seg sl2 = w.wantq ? seg_cols(w.Q, j, 0, n) : kNoSeg;
-        par_house_segs(x, PL, sl0, sl1, sl2);
-      }
-      x.sync();
-      {
-        int hr = (j + 4 < l + 1) ? j + 4 : l + 1;
-        const Seg sr0 = seg_cols(w.H, j, 0, hr);
-        const Seg sr1 = seg_cols(w.T, j, 0, j);
-        const Seg sr2 = w.wantz ? seg_cols(w.Z, j, 0, n) : kNoSeg;
-        par_house_segs(x, PR, sr0, sr1, sr2);
-      }
+      // rows of the block touched by PR: up to j+3 while j+3 <= l
+      const int nr = (j + 3 <= l) ? 4 : 3;
+      double hb[12];
       if (x.tid == 0) {
         for (int cc = 0; cc < 3; ++cc)
+          for (int rr = 0; rr < 4; ++rr) hb[rr + 4 * cc] = (rr < nr) ? w.H(j + rr, j + cc) : 0.0;
+        for (int cc = 0; cc < 3; ++cc) house3_apply(PL, hb[4 * cc], hb[4 * cc + 1], hb[4 * cc + 2]);
+        for (int rr = 0; rr < 4; ++rr) house3_apply(PR, hb[rr], hb[rr + 4], hb[rr + 8]);
+      }
+      x.sync();  // everyone has read H(.,j-1), the T block and the block
+      {
+        const Seg a = seg_rows(w.H, j, j + 3, n), b = seg_rows(w.T, j, j + 3, n);
+        const Seg c = w.wantq ? seg_cols(w.Q, j, 0, n) : no_seg();
+        const Seg d = seg_cols(w.H, j, 0, j), e = seg_cols(w.T, j, 0, j);
+        const Seg g = w.wantz ? seg_cols(w.Z, j, 0, n) : no_seg();
+        const int n1 = seg_total(a, b, c), total = n1 + seg_total(d, e, g);
+        for (int idx = x.tid; idx < total; idx += x.nt) {
+          double* q;
+          int64_t st;
+          const bool left = idx < n1;
+          if (left) seg_item(a, b, c, idx, q, st);
+          else seg_item(d, e, g, idx - n1, q, st);
+          double v0 = q[0], v1 = q[st], v2 = q[2 * st];
+          house3_apply(left ? PL : PR, v0, v1, v2);
+          q[0] = v0; q[st] = v1; q[2 * st] = v2;
+        }
+      }
+      if (x.tid == 0) {
+        for (int cc = 0; cc < 3; ++cc) {
           for (int rr = 0; rr < 3; ++rr) w.T(j + rr, j + cc) = tb[rr + 3 * cc];
+          for (int rr = 0; rr < nr; ++rr) w.H(j + rr, j + cc) = hb[rr + 4 * cc];
+        }
         if (j > f) { w.H(j, j - 1) = beta; w.H(j + 1, j - 1) = 0.0; w.H(j + 2, j - 1) = 0.0; }
       }
       x.sync();
@@ -404,22 +426,36 @@ QZ_HD void cta_ds_sweep(X& x, WinState& w, int f, int l, double c2, double c1, d
       rot2(cr, sr, t00, t01);
       rot2(cr, sr, t10, t11);
       t10 = 0.0;
-      x.sync();
-      {
-        const Seg sl0 = seg_rows(w.H, j, j, n);
-        const Seg sl1 = seg_rows(w.T, j, j + 2, n);
-        const Seg sl2 = w.wantq ? seg_cols(w.Q, j, 0, n) : kNoSeg;
-        par_rot_segs(x, c, s, sl0, sl1, sl2);
+      double hb[4];
+      if (x.tid == 0) {
+        hb[0] = w.H(j, j); hb[1] = w.H(j + 1, j); hb[2] = w.H(j, j + 1); hb[3] = w.H(j + 1, j + 1);
+        rot2(c, s, hb[0], hb[1]);
+        rot2(c, s, hb[2], hb[3]);
+        rot2(cr, sr, hb[0], hb[2]);
+        rot2(cr, sr, hb[1], hb[3]);
       }
       x.sync();
       {
-        const Seg sr20 = seg_cols(w.H, j, 0, l + 1);
-        const Seg sr21 = seg_cols(w.T, j, 0, j);
-        const Seg sr22 = w.wantz ? seg_cols(w.Z, j, 0, n) : kNoSeg;
-        par_rot_segs(x, cr, sr, sr20, sr21, sr22);
+        const Seg a = seg_rows(w.H, j, j + 2, n), b = seg_rows(w.T, j, j + 2, n);
+        const Seg cq = w.wantq ? seg_cols(w.Q, j, 0, n) : no_seg();
+        const Seg d = seg_cols(w.H, j, 0, j), e = seg_cols(w.T, j, 0, j);
+        const Seg g = w.wantz ? seg_cols(w.Z, j, 0, n) : no_seg();
+        const int n1 = seg_total(a, b, cq), total = n1 + seg_total(d, e, g);
+        for (int idx = x.tid; idx < total; idx += x.nt) {
+          double* q;
+          int64_t st;
+          const bool left = idx < n1;
+          if (left) seg_item(a, b, cq, idx, q, st);
+          else seg_item(d, e, g, idx - n1, q, st);
+          const double u = q[0], v = q[st];
+          const double cc = left ? c : cr, ss = left ? s : sr;
+          q[0] = cc * u + ss * v;
+          q[st] = -ss * u + cc * v;
+        }
       }
       if (x.tid == 0) {
         w.T(j, j) = t00; w.T(j + 1, j) = 0.0; w.T(j, j + 1) = t01; w.T(j + 1, j + 1) = t11;
+        w.H(j, j) = hb[0]; w.H(j + 1, j) = hb[1]; w.H(j, j + 1) = hb[2]; w.H(j + 1, j + 1) = hb[3];
         w.H(j, j - 1) = r; w.H(j + 1, j - 1) = 0.0;
       }
       x.sync();
@@ -572,41 +608,32 @@ QZ_HD void small_qr_q(double* X, double* Q) {
   }
 }
 
-// Gaussian elimination with complete pivoting on an S x S system (S <= 8,
-// column-major, ld S).  Row and column exchanges are predicated moves so
-// the matrix stays in registers.  Tiny pivots are replaced by smin (the
-// DGETC2 device); returns false if that happened (the swap then relies on
-// the stability test).
+// Gaussian elimination with row pivoting on an S x S system (S <= 8,
+// column-major, ld S): the pivot of column k is the largest entry of that
+// column at or below the diagonal, so the search is S - k compares (complete
+// pivoting searches (S - k)^2 entries, which made the serial solve the
+// longest part of a block swap).  Row exchanges are predicated moves so the
+// matrix stays in registers.  Tiny pivots are replaced by smin (the DGETC2
+// device); returns false if that happened.  An inaccurate solution is caught
+// by the swap's stability test, which then rejects the swap.
 template <int S>
 QZ_HD bool small_solve_cp(double* A, double* rhs, double smin) {
-  int perm[S];
-#pragma unroll
-  for (int i = 0; i < S; ++i) perm[i] = i;
   bool exact = true;
 #pragma unroll
   for (int k = 0; k < S; ++k) {
-    int pi = k, pj = k;
-    double best = -1.0;
+    int pi = k;
+    double best = fabs(A[k + S * k]);
 #pragma unroll
-    for (int i = k; i < S; ++i)
-#pragma unroll
-      for (int j = k; j < S; ++j) {
-        double v = fabs(A[i + S * j]);
-        if (v > best) { best = v; pi = i; pj = j; }
-      }
+    for (int i = k + 1; i < S; ++i) {
+      const double v = fabs(A[i + S * k]);
+      if (v > best) { best = v; pi = i; }
+    }
 #pragma unroll
     for (int i = k + 1; i < S; ++i)
       if (pi == i) {
 #pragma unroll
-        for (int j = 0; j < S; ++j) { double t = A[k + S * j]; A[k + S * j] = A[i + S * j]; A[i + S * j] = t; }
+        for (int j = k; j < S; ++j) { double t = A[k + S * j]; A[k + S * j] = A[i + S * j]; A[i + S * j] = t; }
         double t = rhs[k]; rhs[k] = rhs[i]; rhs[i] = t;
-      }
-#pragma unroll
-    for (int j = k + 1; j < S; ++j)
-      if (pj == j) {
-#pragma unroll
-        for (int i = 0; i < S; ++i) { double t = A[i + S * k]; A[i + S * k] = A[i + S * j]; A[i + S * j] = t; }
-        int t = perm[k]; perm[k] = perm[j]; perm[j] = t;
       }
     if (fabs(A[k + S * k]) < smin) { A[k + S * k] = smin; exact = false; }
     const double rpiv = 1.0 / A[k + S * k];
@@ -619,22 +646,12 @@ QZ_HD bool small_solve_cp(double* A, double* rhs, double smin) {
       A[i + S * k] = 0.0;
     }
   }
-  double y[S];
 #pragma unroll
   for (int k = S - 1; k >= 0; --k) {
     double acc = rhs[k];
 #pragma unroll
-    for (int j = k + 1; j < S; ++j) acc -= A[k + S * j] * y[j];
-    y[k] = acc / A[k + S * k];
-  }
-  // undo the column exchanges: x(perm[k]) = y(k)
-#pragma unroll
-  for (int t = 0; t < S; ++t) {
-    double v = 0.0;
-#pragma unroll
-    for (int k = 0; k < S; ++k)
-      if (perm[k] == t) v = y[k];
-    rhs[t] = v;
+    for (int j = k + 1; j < S; ++j) acc -= A[k + S * j] * rhs[j];
+    rhs[k] = acc / A[k + S * k];
   }
   return exact;
 }
@@ -739,6 +756,7 @@ QZ_HD bool cta_swap_t(X& x, WinState& w, int j1, bool restd) {
   double* sZ = x.sd + 16;  // 16
   double* sS = x.sd + 32;  // 16
   double* sT = x.sd + 48;  // 16
+  x.count(1);
   if (x.tid == 0) {
     double S2[M * M], T2[M * M], Qs[M * M], Zs[M * M];
     bool ok = swap_compute<N1, N2>(MatV{&w.H(j1, j1), w.H.ld}, MatV{&w.T(j1, j1), w.T.ld}, S2, T2, Qs, Zs,
@@ -836,286 +854,19 @@ QZ_HD bool cta_swap(X& x, WinState& w, int j1, int n1, int n2, bool restd = true
 // caller standardises the window afterwards, cta_std_all).
 template <class X>
 QZ_HD bool cta_move_block(X& x, WinState& w, int ifst, int nb, int ilst, bool restd = true) {
+  // reads of the block structure need no barrier of their own: every swap
+  // starts (after these reads) and ends with one
   int here = ifst;
   while (here > ilst) {
     int nbn = 1;
     if (here - 2 >= ilst && w.H(here - 1, here - 2) != 0.0) nbn = 2;
-    x.sync();
     if (!cta_swap(x, w, here - nbn, nbn, nb, restd)) return false;
     here -= nbn;
     // the moved block must keep its size (a complex pair stays 2x2)
     int nbnow = (nb == 2 && w.H(here + 1, here) != 0.0) ? 2 : 1;
-    x.sync();
     if (nbnow != nb) return false;
   }
   return true;
-}
-
-// ---------------------------------------------------------------------------
-// Aggressive early deflation on a window (already copied into w, with
-// w.Q = w.Z = I).  s is the spike H(kwtop, kwtop-1) (0 at the top of the
-// active block).  swapfail makes every block swap report failure (a test
-// hook for the failure branch).  On return:
-//   si[8]  = number of undeflated eigenvalues m (positions 0..m-1)
-//   si[9]  = status (0 ok, >0 small QZ failed)
-//   si[10] = 1 if the window was transformed (nd > 0 or full solve)
-//   sd[128..] unused
-// shifts (alphar, alphai, beta) of the undeflated eigenvalues are written
-// to sr/si_/sb (length >= m) by thread 0 before the spike reflector is
-// applied.  When nothing deflates the window is left in Schur form but the
-// caller discards it (the pencil is unchanged).
-// ---------------------------------------------------------------------------
-template <class X>
-QZ_HD void cta_aed(X& x, WinState& w, double s, double* sr, double* si_, double* sb, int maxit, int nskip = 0,
-                   bool swapfail = false) {
-  int n = w.n;
-  x.stamp(0);
-  int info = cta_small_qz(x, w, maxit);
-  x.stamp(1);
-  if (info != 0) {
-    // window QZ did not converge: deflate nothing, hand the diagonal
-    // ratios of the (equivalent) partly reduced window over as shifts
-    // (qzearly.f:237-248); the caller discards the window itself
-    if (x.tid == 0) {
-      for (int i = 0; i < n; ++i) { sr[i] = w.H(i, i); si_[i] = 0.0; sb[i] = w.T(i, i); }
-      x.si[8] = n; x.si[9] = info; x.si[10] = 0;
-    }
-    x.sync();
-    return;
-  }
-  // ---- spike test with reordering (qzearly.f:253-365) ----
-  int kb = n - 1, ilst = 0;
-  bool failed = false;
-  int fails = 0;  // consecutive undeflatable blocks
-  while (kb >= ilst) {
-    // optional early stop: after nskip consecutive undeflatable blocks the
-    // rest of the window is left undeflated (bounds the O(n^2) swaps)
-    if (nskip > 0 && fails >= nskip) break;
-    bool bulge = (kb > ilst) && (w.H(kb, kb - 1) != 0.0);
-    bool dfl;
-    if (!bulge) {
-      double temp = fabs(s) + fabs(w.H(kb, kb));
-      dfl = fabs(s * w.Q(0, kb)) <= dmax(w.tol.ulp * temp, w.tol.smlnum);
-    } else {
-      double h11 = w.H(kb - 1, kb - 1), h21 = w.H(kb, kb - 1), h12 = w.H(kb - 1, kb), h22 = w.H(kb, kb);
-      double rtdet;
-      if (h11 == 0.0 && h21 == 0.0) rtdet = 0.0;
-      else if (fabs(h11) >= fabs(h21)) rtdet = sqrt(fabs(h11)) * sqrt(fabs(h22 - (h21 / h11) * h12));
-      else rtdet = sqrt(fabs(h21)) * sqrt(fabs(h12 - (h11 / h21) * h22));
-      double temp = fabs(s) + rtdet;
-      dfl = dmax(fabs(s * w.Q(0, kb)), fabs(s * w.Q(0, kb - 1))) <= dmax(w.tol.ulp * temp, w.tol.smlnum);
-    }
-    x.sync();
-    int nb = bulge ? 2 : 1;
-    if (dfl) {
-      kb -= nb;
-      fails = 0;
-    } else {
-      // a rejected swap ends the test: the window is re-reduced with the
-      // deflations found so far (qzearly.f:321-326); swapfail forces it
-      if (swapfail || !cta_move_block(x, w, kb - nb + 1, nb, ilst, false)) { failed = true; break; }
-      ilst += nb;
-      ++fails;
-    }
-  }
-  (void)failed;
-  // the swaps left the 2x2 blocks they touched general: standardise every
-  // block of the window at once (T upper triangular again, complex pairs
-  // with a positive diagonal block of T)
-  cta_std_all(x, w, x.sd + 64);
-  x.stamp(2);
-  int m = kb + 1;  // undeflated eigenvalues at 0..m-1
-  // ---- shifts: eigenvalues of the undeflated Schur blocks ----
-  if (x.tid == 0) {
-    int j = 0;
-    while (j < m) {
-      if (j + 1 < m && w.H(j + 1, j) != 0.0) {
-        double c2, c1, c0;
-        pencil2_poly(w.H(j, j), w.H(j + 1, j), w.H(j, j + 1), w.H(j + 1, j + 1),
-                     w.T(j, j), w.T(j, j + 1), w.T(j + 1, j + 1), c2, c1, c0);
-        // complex pair (or real pair if rounding says so): store as
-        // lambda = (c1 +- sqrt(disc)) / (2 c2)
-        double disc = c1 * c1 - 4.0 * c2 * c0;
-        if (disc < 0.0) {
-          sr[j] = c1; si_[j] = sqrt(-disc); sb[j] = 2.0 * c2;
-          sr[j + 1] = c1; si_[j + 1] = -sqrt(-disc); sb[j + 1] = 2.0 * c2;
-        } else {
-          double sq = sqrt(disc);
-          sr[j] = c1 + sq; si_[j] = 0.0; sb[j] = 2.0 * c2;
-          sr[j + 1] = c1 - sq; si_[j + 1] = 0.0; sb[j + 1] = 2.0 * c2;
-        }
-        j += 2;
-      } else {
-        sr[j] = w.H(j, j); si_[j] = 0.0; sb[j] = w.T(j, j);
-        j += 1;
-      }
-    }
-    x.si[8] = m;
-    x.si[9] = 0;
-    x.si[10] = (m < n) ? 1 : 0;
-  }
-  x.sync();
-  if (m == n || m <= 1 || s == 0.0) {
-    // nothing deflated (caller discards), or nothing left to re-reduce
-    x.sync();
-    return;
-  }
-  // ---- spike reflector from Q(0, 0:m-1) (qzearly.f:371-381) ----
-  double* v = x.sd + 64;  // length m (<= n); caller guarantees room
-  if (x.tid == 0) {
-    double alpha = w.Q(0, 0);
-    double mx = 0.0;
-    for (int i = 1; i < m; ++i) mx = dmax(mx, fabs(w.Q(0, i)));
-    double tau = 0.0;
-    v[0] = 1.0;
-    if (mx > 0.0) {
-      double ma = dmax(mx, fabs(alpha));
-      double nrm = 0.0;
-      nrm += (alpha / ma) * (alpha / ma);
-      for (int i = 1; i < m; ++i) { double t = w.Q(0, i) / ma; nrm += t * t; }
-      nrm = sqrt(nrm) * ma;
-      double beta = -dsign(nrm, alpha);
-      tau = (beta - alpha) / beta;
-      double sc = 1.0 / (alpha - beta);
-      for (int i = 1; i < m; ++i) v[i] = w.Q(0, i) * sc;
-    } else {
-      for (int i = 1; i < m; ++i) v[i] = 0.0;
-    }
-    x.sd[63] = tau;
-  }
-  x.sync();
-  double tau = x.sd[63];
-  if (tau != 0.0) {
-    // H(0:m, :) <- P H ; T(0:m, m:n) <- P T ; Q(:, 0:m) <- Q P
-    for (int j = x.tid; j < n; j += x.nt) {
-      double t = 0.0;
-      for (int i = 0; i < m; ++i) t += v[i] * w.H(i, j);
-      t *= tau;
-      for (int i = 0; i < m; ++i) w.H(i, j) -= t * v[i];
-      if (j >= m) {
-        double u = 0.0;
-        for (int i = 0; i < m; ++i) u += v[i] * w.T(i, j);
-        u *= tau;
-        for (int i = 0; i < m; ++i) w.T(i, j) -= u * v[i];
-      }
-    }
-    if (w.wantq)
-      for (int r = x.tid; r < n; r += x.nt) {
-        double t = 0.0;
-        for (int i = 0; i < m; ++i) t += w.Q(r, i) * v[i];
-        t *= tau;
-        for (int i = 0; i < m; ++i) w.Q(r, i) -= t * v[i];
-      }
-    // RQ update of the leading m x m block of T:  T' = T + v*wv^T with
-    // wv = -tau T^T v  (qzearly.f:396-446)
-    double* wv = x.sd + 64 + n;  // length m
-    for (int j = x.tid; j < m; j += x.nt) {
-      double t = 0.0;
-      for (int i = 0; i <= j; ++i) t += w.T(i, j) * v[i];
-      wv[j] = -tau * t;
-    }
-    x.sync();
-    // pass 1 rotations (depend on wv only): zero wv(i) into wv(i+1)
-    double* rc = x.sd + 64 + 2 * n;      // length m
-    double* rs = x.sd + 64 + 3 * n;      // length m
-    if (x.tid == 0) {
-      double wl = wv[0];
-      for (int i = 0; i < m - 1; ++i) {
-        double c, sn, r;
-        lartg(wv[i + 1], wl, c, sn, r);
-        // column op on (col i, col i+1): col_i' = c col_i - sn col_{i+1}
-        //                                col_{i+1}' = sn col_i + c col_{i+1}
-        rc[i] = c; rs[i] = sn;
-        wl = r;
-      }
-      x.sd[62] = wl;  // final wv(m-1)
-    }
-    x.sync();
-    // apply pass 1 row by row to T (rows 0..m-1), H (rows 0..m-1), Z (all rows)
-    for (int r = x.tid; r < n; r += x.nt) {
-      if (r < m) {
-        for (int i = (r > 0 ? r - 1 : 0); i < m - 1; ++i) {
-          double a = w.T(r, i), b = w.T(r, i + 1);
-          w.T(r, i) = rc[i] * a - rs[i] * b;
-          w.T(r, i + 1) = rs[i] * a + rc[i] * b;
-        }
-        for (int i = 0; i < m - 1; ++i) {
-          double a = w.H(r, i), b = w.H(r, i + 1);
-          w.H(r, i) = rc[i] * a - rs[i] * b;
-          w.H(r, i + 1) = rs[i] * a + rc[i] * b;
-        }
-      }
-      if (w.wantz)
-        for (int i = 0; i < m - 1; ++i) {
-          double a = w.Z(r, i), b = w.Z(r, i + 1);
-          w.Z(r, i) = rc[i] * a - rs[i] * b;
-          w.Z(r, i + 1) = rs[i] * a + rc[i] * b;
-        }
-    }
-    x.sync();
-    double wl = x.sd[62];
-    for (int i = x.tid; i < m; i += x.nt) w.T(i, m - 1) += wl * v[i];
-    x.sync();
-    // pass 2: zero the subdiagonal of T from the bottom
-    for (int i = m - 2; i >= 0; --i) {
-      double c, sn, r;
-      lartg(w.T(i + 1, i + 1), w.T(i + 1, i), c, sn, r);
-      x.sync();
-      for (int rr = x.tid; rr <= i; rr += x.nt) {
-        double a = w.T(rr, i), b = w.T(rr, i + 1);
-        w.T(rr, i) = c * a - sn * b;
-        w.T(rr, i + 1) = sn * a + c * b;
-      }
-      if (x.tid == 0) { w.T(i + 1, i + 1) = r; w.T(i + 1, i) = 0.0; rc[i] = c; rs[i] = sn; }
-      x.sync();
-    }
-    for (int r = x.tid; r < n; r += x.nt) {
-      if (r < m)
-        for (int i = m - 2; i >= 0; --i) {
-          double a = w.H(r, i), b = w.H(r, i + 1);
-          w.H(r, i) = rc[i] * a - rs[i] * b;
-          w.H(r, i + 1) = rs[i] * a + rc[i] * b;
-        }
-      if (w.wantz)
-        for (int i = m - 2; i >= 0; --i) {
-          double a = w.Z(r, i), b = w.Z(r, i + 1);
-          w.Z(r, i) = rc[i] * a - rs[i] * b;
-          w.Z(r, i + 1) = rs[i] * a + rc[i] * b;
-        }
-    }
-    x.sync();
-  }
-  x.stamp(3);
-  // ---- Hessenberg-triangular re-reduction of the leading m x m block
-  //      by Givens rotations (the job of DGGHRD at qzearly.f:449) ----
-  for (int jc = 0; jc < m - 2; ++jc) {
-    for (int jr = m - 1; jr >= jc + 2; --jr) {
-      double c, sn, r;
-      lartg(w.H(jr - 1, jc), w.H(jr, jc), c, sn, r);
-      x.sync();
-      {
-        const Seg sl0 = seg_rows(w.H, jr - 1, jc + 1, n);
-        const Seg sl1 = seg_rows(w.T, jr - 1, jr - 1, n);
-        const Seg sl2 = w.wantq ? seg_cols(w.Q, jr - 1, 0, n) : kNoSeg;
-        par_rot_segs(x, c, sn, sl0, sl1, sl2);
-      }
-      if (x.tid == 0) { w.H(jr - 1, jc) = r; w.H(jr, jc) = 0.0; }
-      x.sync();
-      // pair (col jr, col jr-1): zero T(jr, jr-1)
-      lartg(w.T(jr, jr), w.T(jr, jr - 1), c, sn, r);
-      x.sync();
-      {
-        // columns (jr, jr-1): the pair's first member is column jr
-        const Seg sr0 = Seg{&w.H(0, jr), 1, -(int64_t)w.H.ld, m};
-        const Seg sr1 = Seg{&w.T(0, jr), 1, -(int64_t)w.T.ld, jr};
-        const Seg sr2 = w.wantz ? Seg{&w.Z(0, jr), 1, -(int64_t)w.Z.ld, n} : kNoSeg;
-        par_rot_segs(x, c, sn, sr0, sr1, sr2);
-      }
-      if (x.tid == 0) { w.T(jr, jr) = r; w.T(jr, jr - 1) = 0.0; }
-      x.sync();
-    }
-  }
-  x.stamp(4);
 }
 
 }  // namespace qz

@@ -429,7 +429,12 @@ QZ_HD void eig2_complex(const double* a, double b0, double b1, double* ar, doubl
   m00 = ldexp(m00, -e); m01 = ldexp(m01, -e); m10 = ldexp(m10, -e); m11 = ldexp(m11, -e);
   double tr = 0.5 * (m00 + m11);
   double d = 0.5 * (m00 - m11);
-  double disc = d * d + m01 * m10;  // < 0 for a complex pair
+  // disc = d^2 + m01 m10 (< 0 for a complex pair) with the rounding error of
+  // the product added back (fma), so a nearly real pair, where the two terms
+  // almost cancel, keeps its imaginary part accurate
+  const double p = m01 * m10;
+  const double perr = fma(m01, m10, -p);
+  double disc = fma(d, d, p) + perr;
   double wr = tr;
   double wi = sqrt(fabs(dmin(disc, 0.0)));
   const double s0 = ldexp(b0, e), s1 = ldexp(b1, e);

@@ -1,0 +1,489 @@
+// AED on a window held by one CTA: window Schur form, spike test,
+// reordering, spike reflector, RQ update of T and Givens Hessenberg-
+// triangular re-reduction -- the role of QZEARLY (qzearly.f:229-449) inside
+// PDHGEQZ2 (PDHGEQZ2.f:315-389), and with the window equal to the whole
+// small block the role of PDHGEQZ4 -> KKQZ (PDHGEQZ4.f:329-372).
+//
+// The window's Schur form comes from cta_small_qz_ms: a small-bulge
+// multishift QZ inside the window.  Each sweep chases a chain of up to
+// kMsMaxBulges bulges through the active block in lockstep
+// (cta_chase_window, the same code as the sweeps of the whole pencil), with
+// shifts from the eigenvalues of the active block's trailing 2*nb x 2*nb
+// part, which one thread computes alone (a small double-shift QZ on a copy,
+// eigenvalues only).  Blocks too short for a chain, and every tenth
+// iteration without deflation (exceptional shift), take one double-shift
+// sweep instead.  The lockstep chain advances every bulge one row per step,
+// so a sweep of 2*nb shifts costs (L + 3 nb) steps instead of nb*L.
+#pragma once
+#include "qz_chase.cuh"
+
+namespace qz {
+
+constexpr int kMsMaxBulges = 6;       // bulges per sweep of the window QZ
+constexpr int kMsMinBlock = 28;       // shorter active blocks use double shifts
+// shared scratch of cta_small_qz_ms: bulge records, bulge descriptions and
+// two (2*kMsMaxBulges)^2 copies of the trailing block, in doubles
+constexpr int kMsScratch = kMsMaxBulges * ((int)(sizeof(BulgeRec) + sizeof(Bulge)) / 8 + 2) +
+                           2 * (2 * kMsMaxBulges) * (2 * kMsMaxBulges) + 16;
+
+// Executor for code one thread runs alone while the others wait at a
+// barrier of the enclosing executor.
+struct SoloExec {
+  int tid, nt;
+  int* si;
+  double* sd;
+  QZ_HD void sync() {}
+  QZ_HD void stamp(int) {}
+  QZ_HD void count(int) {}
+};
+
+// Shift polynomials of a chain from the Schur form (Hs, Ts) of a k x k
+// block: a 2x2 block gives its own real quadratic, real eigenvalues pair in
+// order.  Returns the number of polynomials written (at most nbmax).
+QZ_HD int shifts_from_schur(MatV Hs, MatV Ts, int k, Bulge* bl, int nbmax) {
+  int nbu = 0;
+  int j = k - 1;
+  double ra = 0.0, rb = 0.0;
+  bool have = false;
+  while (j >= 0 && nbu < nbmax) {
+    double c2, c1, c0;
+    if (j > 0 && Hs(j, j - 1) != 0.0) {
+      pencil2_poly(Hs(j - 1, j - 1), Hs(j, j - 1), Hs(j - 1, j), Hs(j, j), Ts(j - 1, j - 1), Ts(j - 1, j), Ts(j, j),
+                   c2, c1, c0);
+      j -= 2;
+    } else {
+      const double a = Hs(j, j), b = Ts(j, j);
+      j -= 1;
+      if (!have) { ra = a; rb = b; have = true; continue; }
+      have = false;
+      c2 = rb * b; c1 = ra * b + a * rb; c0 = ra * a;
+    }
+    const double mx = dmax(fabs(c2), dmax(fabs(c1), fabs(c0)));
+    if (!(mx > 0.0) || !isfinite(mx)) continue;
+    bl[nbu].c2 = c2 / mx; bl[nbu].c1 = c1 / mx; bl[nbu].c0 = c0 / mx;
+    ++nbu;
+  }
+  return nbu;
+}
+
+// ---------------------------------------------------------------------------
+// Small QZ by small-bulge multishift sweeps: reduce the whole window to
+// generalized real Schur form.  Returns 0, or ilast+1 if maxit iterations
+// did not suffice.  scr: kMsScratch doubles of shared scratch.
+// ---------------------------------------------------------------------------
+template <class X>
+QZ_HD int cta_small_qz_ms(X& x, WinState& w, int maxit, double* scr) {
+  const int n = w.n;
+  BulgeRec* rec = (BulgeRec*)scr;
+  Bulge* bl = (Bulge*)(rec + kMsMaxBulges);
+  double* tcopy = scr + kMsMaxBulges * ((int)(sizeof(BulgeRec) + sizeof(Bulge)) / 8 + 2);
+  int ilast = n - 1;
+  int iiter = 0, jiter = 0;
+  while (ilast >= 0) {
+    if (x.tid == 0) {
+      int ifirst = 0;
+      for (int j = ilast; j >= 1; --j) {
+        double tst = fabs(w.H(j - 1, j - 1)) + fabs(w.H(j, j));
+        if (tst == 0.0) tst = fabs(w.H(j - 1, j)) + fabs(w.H(j, j - 1));
+        if (fabs(w.H(j, j - 1)) <= dmax(w.tol.smlnum, w.tol.ulp * tst)) {
+          w.H(j, j - 1) = 0.0;
+          ifirst = j;
+          break;
+        }
+      }
+      int jz = -1;
+      for (int j = ilast; j >= ifirst; --j) {
+        if (fabs(w.T(j, j)) <= w.tol.ttol) { w.T(j, j) = 0.0; jz = j; break; }
+      }
+      x.si[0] = ifirst;
+      x.si[1] = jz;
+    }
+    x.sync();
+    const int ifirst = x.si[0], jz = x.si[1];
+    x.sync();
+    if (ifirst == ilast) { ilast -= 1; iiter = 0; continue; }
+    if (jz >= 0) {
+      if (jz == ifirst) {
+        cta_inf_top(x, w, ifirst);
+      } else {
+        if (jz < ilast) cta_inf_chase_down(x, w, ifirst, jz, ilast);
+        cta_inf_bottom(x, w, ilast);
+        ilast -= 1;
+      }
+      iiter = 0;
+      continue;
+    }
+    if (ifirst + 1 == ilast) {
+      cta_std2x2(x, w, ifirst);
+      ilast -= 2;
+      iiter = 0;
+      continue;
+    }
+    ++iiter;
+    ++jiter;
+    if (jiter > maxit) return ilast + 1;
+    const int L = ilast - ifirst + 1;
+    int nb = (L - 4) / 6;
+    nb = nb < kMsMaxBulges ? nb : kMsMaxBulges;
+    int nbu = 0;
+    if (L >= kMsMinBlock && nb >= 2 && iiter % 10 != 0) {
+      // shifts: eigenvalues of the trailing 2nb x 2nb block, one thread
+      if (x.tid == 0) {
+        const int k = 2 * nb, a = ilast - k + 1;
+        MatV Hc{tcopy, k}, Tc{tcopy + k * k, k};
+        for (int c = 0; c < k; ++c)
+          for (int r = 0; r < k; ++r) {
+            Hc(r, c) = (r <= c + 1) ? w.H(a + r, a + c) : 0.0;
+            Tc(r, c) = (r <= c) ? w.T(a + r, a + c) : 0.0;
+          }
+        WinState ws;
+        ws.n = k; ws.H = Hc; ws.T = Tc; ws.Q = Hc; ws.Z = Hc;
+        ws.wantq = false; ws.wantz = false;
+        ws.tol = w.tol;
+        int sis[4];
+        SoloExec solo{0, 1, sis, nullptr};
+        const int inf = cta_small_qz(solo, ws, 30 * k);
+        int got = (inf == 0) ? shifts_from_schur(Hc, Tc, k, bl, nb) : 0;
+        for (int b = 0; b < got; ++b) {
+          bl[b].base = ifirst - 3 * b;
+          bl[b].tlo = 3 * b;
+          bl[b].thi = ilast - bl[b].base;
+          bl[b].intro = 1;
+        }
+        x.si[2] = got;
+      }
+      x.sync();
+      nbu = x.si[2];
+    }
+    if (nbu >= 1) {
+      x.count(3);
+      const int tmax = ilast - (ifirst - 3 * (nbu - 1));
+      cta_chase_window(x, n, ilast, w.H, w.T, w.Q, w.Z, bl, nbu, tmax, rec);
+      continue;
+    }
+    double c2, c1, c0;
+    const int l = ilast;
+    if (iiter % 10 == 0) {
+      // exceptional shift from the bottom subdiagonals
+      double sc = fabs(w.H(l, l - 1) / w.T(l - 1, l - 1)) + fabs(w.H(l - 1, l - 2) / w.T(l - 2, l - 2));
+      double h11 = 0.75 * sc + w.H(l, l) / w.T(l, l);
+      c2 = 1.0;
+      c1 = 2.0 * h11;
+      c0 = h11 * h11 + 0.4375 * sc * sc;
+    } else {
+      pencil2_poly(w.H(l - 1, l - 1), w.H(l, l - 1), w.H(l - 1, l), w.H(l, l),
+                   w.T(l - 1, l - 1), w.T(l - 1, l), w.T(l, l), c2, c1, c0);
+    }
+    cta_ds_sweep(x, w, ifirst, ilast, c2, c1, c0);
+  }
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// Aggressive early deflation on a window (already copied into w, with
+// w.Q = w.Z = I).  s is the spike H(kwtop, kwtop-1) (0 at the top of the
+// active block).  swapfail makes every block swap report failure (a test
+// hook for the failure branch).  On return:
+//   si[8]  = number of undeflated eigenvalues m (positions 0..m-1)
+//   si[9]  = status (0 ok, >0 small QZ failed)
+//   si[10] = 1 if the window was transformed (nd > 0 or full solve)
+//   sd[128..] unused
+// shifts (alphar, alphai, beta) of the undeflated eigenvalues are written
+// to sr/si_/sb (length >= m) by thread 0 before the spike reflector is
+// applied.  When nothing deflates the window is left in Schur form but the
+// caller discards it (the pencil is unchanged).
+// ---------------------------------------------------------------------------
+template <class X>
+QZ_HD void cta_aed(X& x, WinState& w, double s, double* sr, double* si_, double* sb, int maxit, int nskip = 0,
+                   bool swapfail = false, double* msscr = nullptr) {
+  const bool ms = msscr != nullptr;
+  int n = w.n;
+  x.stamp(0);
+  int info = ms ? cta_small_qz_ms(x, w, maxit, msscr) : cta_small_qz(x, w, maxit);
+  x.stamp(1);
+  if (info != 0) {
+    // window QZ did not converge: deflate nothing, hand the diagonal
+    // ratios of the (equivalent) partly reduced window over as shifts
+    // (qzearly.f:237-248); the caller discards the window itself
+    if (x.tid == 0) {
+      for (int i = 0; i < n; ++i) { sr[i] = w.H(i, i); si_[i] = 0.0; sb[i] = w.T(i, i); }
+      x.si[8] = n; x.si[9] = info; x.si[10] = 0;
+    }
+    x.sync();
+    return;
+  }
+  // ---- spike test with reordering (qzearly.f:253-365) ----
+  int kb = n - 1, ilst = 0;
+  bool failed = false;
+  int fails = 0;  // consecutive undeflatable blocks
+  while (kb >= ilst) {
+    // optional early stop: after nskip consecutive undeflatable blocks the
+    // rest of the window is left undeflated (bounds the O(n^2) swaps)
+    if (nskip > 0 && fails >= nskip) break;
+    bool bulge = (kb > ilst) && (w.H(kb, kb - 1) != 0.0);
+    bool dfl;
+    if (!bulge) {
+      double temp = fabs(s) + fabs(w.H(kb, kb));
+      dfl = fabs(s * w.Q(0, kb)) <= dmax(w.tol.ulp * temp, w.tol.smlnum);
+    } else {
+      double h11 = w.H(kb - 1, kb - 1), h21 = w.H(kb, kb - 1), h12 = w.H(kb - 1, kb), h22 = w.H(kb, kb);
+      double rtdet;
+      if (h11 == 0.0 && h21 == 0.0) rtdet = 0.0;
+      else if (fabs(h11) >= fabs(h21)) rtdet = sqrt(fabs(h11)) * sqrt(fabs(h22 - (h21 / h11) * h12));
+      else rtdet = sqrt(fabs(h21)) * sqrt(fabs(h12 - (h11 / h21) * h22));
+      double temp = fabs(s) + rtdet;
+      dfl = dmax(fabs(s * w.Q(0, kb)), fabs(s * w.Q(0, kb - 1))) <= dmax(w.tol.ulp * temp, w.tol.smlnum);
+    }
+    int nb = bulge ? 2 : 1;
+    if (dfl) {
+      kb -= nb;
+      fails = 0;
+    } else {
+      // a rejected swap ends the test: the window is re-reduced with the
+      // deflations found so far (qzearly.f:321-326); swapfail forces it
+      if (swapfail || !cta_move_block(x, w, kb - nb + 1, nb, ilst, false)) { failed = true; break; }
+      ilst += nb;
+      ++fails;
+    }
+  }
+  (void)failed;
+  // the swaps left the 2x2 blocks they touched general: standardise every
+  // block of the window at once (T upper triangular again, complex pairs
+  // with a positive diagonal block of T)
+  cta_std_all(x, w, x.sd + 64);
+  x.stamp(2);
+  int m = kb + 1;  // undeflated eigenvalues at 0..m-1
+  // ---- shifts: eigenvalues of the undeflated Schur blocks ----
+  if (x.tid == 0) {
+    int j = 0;
+    while (j < m) {
+      if (j + 1 < m && w.H(j + 1, j) != 0.0) {
+        double c2, c1, c0;
+        pencil2_poly(w.H(j, j), w.H(j + 1, j), w.H(j, j + 1), w.H(j + 1, j + 1),
+                     w.T(j, j), w.T(j, j + 1), w.T(j + 1, j + 1), c2, c1, c0);
+        // complex pair (or real pair if rounding says so): store as
+        // lambda = (c1 +- sqrt(disc)) / (2 c2)
+        double disc = c1 * c1 - 4.0 * c2 * c0;
+        if (disc < 0.0) {
+          sr[j] = c1; si_[j] = sqrt(-disc); sb[j] = 2.0 * c2;
+          sr[j + 1] = c1; si_[j + 1] = -sqrt(-disc); sb[j + 1] = 2.0 * c2;
+        } else {
+          double sq = sqrt(disc);
+          sr[j] = c1 + sq; si_[j] = 0.0; sb[j] = 2.0 * c2;
+          sr[j + 1] = c1 - sq; si_[j + 1] = 0.0; sb[j + 1] = 2.0 * c2;
+        }
+        j += 2;
+      } else {
+        sr[j] = w.H(j, j); si_[j] = 0.0; sb[j] = w.T(j, j);
+        j += 1;
+      }
+    }
+    x.si[8] = m;
+    x.si[9] = 0;
+    x.si[10] = (m < n) ? 1 : 0;
+  }
+  x.sync();
+  if (m == n || m <= 1 || s == 0.0) {
+    // nothing deflated (caller discards), or nothing left to re-reduce
+    x.sync();
+    return;
+  }
+  // ---- spike reflector from Q(0, 0:m-1) (qzearly.f:371-381) ----
+  double* v = x.sd + 64;  // length m (<= n); caller guarantees room
+  if (x.tid == 0) {
+    double alpha = w.Q(0, 0);
+    double mx = 0.0;
+    for (int i = 1; i < m; ++i) mx = dmax(mx, fabs(w.Q(0, i)));
+    double tau = 0.0;
+    v[0] = 1.0;
+    if (mx > 0.0) {
+      double ma = dmax(mx, fabs(alpha));
+      double nrm = 0.0;
+      nrm += (alpha / ma) * (alpha / ma);
+      for (int i = 1; i < m; ++i) { double t = w.Q(0, i) / ma; nrm += t * t; }
+      nrm = sqrt(nrm) * ma;
+      double beta = -dsign(nrm, alpha);
+      tau = (beta - alpha) / beta;
+      double sc = 1.0 / (alpha - beta);
+      for (int i = 1; i < m; ++i) v[i] = w.Q(0, i) * sc;
+    } else {
+      for (int i = 1; i < m; ++i) v[i] = 0.0;
+    }
+    x.sd[63] = tau;
+  }
+  x.sync();
+  double tau = x.sd[63];
+  if (tau != 0.0) {
+    // H(0:m, :) <- P H ; T(0:m, m:n) <- P T ; Q(:, 0:m) <- Q P
+    for (int j = x.tid; j < n; j += x.nt) {
+      double t = 0.0;
+      for (int i = 0; i < m; ++i) t += v[i] * w.H(i, j);
+      t *= tau;
+      for (int i = 0; i < m; ++i) w.H(i, j) -= t * v[i];
+      if (j >= m) {
+        double u = 0.0;
+        for (int i = 0; i < m; ++i) u += v[i] * w.T(i, j);
+        u *= tau;
+        for (int i = 0; i < m; ++i) w.T(i, j) -= u * v[i];
+      }
+    }
+    if (w.wantq)
+      for (int r = x.tid; r < n; r += x.nt) {
+        double t = 0.0;
+        for (int i = 0; i < m; ++i) t += w.Q(r, i) * v[i];
+        t *= tau;
+        for (int i = 0; i < m; ++i) w.Q(r, i) -= t * v[i];
+      }
+    // RQ update of the leading m x m block of T:  T' = T + v*wv^T with
+    // wv = -tau T^T v  (qzearly.f:396-446)
+    double* wv = x.sd + 64 + n;  // length m
+    for (int j = x.tid; j < m; j += x.nt) {
+      double t = 0.0;
+      for (int i = 0; i <= j; ++i) t += w.T(i, j) * v[i];
+      wv[j] = -tau * t;
+    }
+    x.sync();
+    // pass 1 rotations (depend on wv only): zero wv(i) into wv(i+1)
+    double* rc = x.sd + 64 + 2 * n;      // length m
+    double* rs = x.sd + 64 + 3 * n;      // length m
+    if (x.tid == 0) {
+      double wl = wv[0];
+      for (int i = 0; i < m - 1; ++i) {
+        double c, sn, r;
+        lartg(wv[i + 1], wl, c, sn, r);
+        // column op on (col i, col i+1): col_i' = c col_i - sn col_{i+1}
+        //                                col_{i+1}' = sn col_i + c col_{i+1}
+        rc[i] = c; rs[i] = sn;
+        wl = r;
+      }
+      x.sd[62] = wl;  // final wv(m-1)
+    }
+    x.sync();
+    // apply pass 1 row by row to T (rows 0..m-1), H (rows 0..m-1), Z (all rows)
+    for (int r = x.tid; r < n; r += x.nt) {
+      if (r < m) {
+        for (int i = (r > 0 ? r - 1 : 0); i < m - 1; ++i) {
+          double a = w.T(r, i), b = w.T(r, i + 1);
+          w.T(r, i) = rc[i] * a - rs[i] * b;
+          w.T(r, i + 1) = rs[i] * a + rc[i] * b;
+        }
+        for (int i = 0; i < m - 1; ++i) {
+          double a = w.H(r, i), b = w.H(r, i + 1);
+          w.H(r, i) = rc[i] * a - rs[i] * b;
+          w.H(r, i + 1) = rs[i] * a + rc[i] * b;
+        }
+      }
+      if (w.wantz)
+        for (int i = 0; i < m - 1; ++i) {
+          double a = w.Z(r, i), b = w.Z(r, i + 1);
+          w.Z(r, i) = rc[i] * a - rs[i] * b;
+          w.Z(r, i + 1) = rs[i] * a + rc[i] * b;
+        }
+    }
+    x.sync();
+    double wl = x.sd[62];
+    for (int i = x.tid; i < m; i += x.nt) w.T(i, m - 1) += wl * v[i];
+    x.sync();
+    // pass 2: zero the subdiagonal of T from the bottom
+    for (int i = m - 2; i >= 0; --i) {
+      double c, sn, r;
+      lartg(w.T(i + 1, i + 1), w.T(i + 1, i), c, sn, r);
+      x.sync();
+      for (int rr = x.tid; rr <= i; rr += x.nt) {
+        double a = w.T(rr, i), b = w.T(rr, i + 1);
+        w.T(rr, i) = c * a - sn * b;
+        w.T(rr, i + 1) = sn * a + c * b;
+      }
+      if (x.tid == 0) { w.T(i + 1, i + 1) = r; w.T(i + 1, i) = 0.0; rc[i] = c; rs[i] = sn; }
+      x.sync();
+    }
+    for (int r = x.tid; r < n; r += x.nt) {
+      if (r < m)
+        for (int i = m - 2; i >= 0; --i) {
+          double a = w.H(r, i), b = w.H(r, i + 1);
+          w.H(r, i) = rc[i] * a - rs[i] * b;
+          w.H(r, i + 1) = rs[i] * a + rc[i] * b;
+        }
+      if (w.wantz)
+        for (int i = m - 2; i >= 0; --i) {
+          double a = w.Z(r, i), b = w.Z(r, i + 1);
+          w.Z(r, i) = rc[i] * a - rs[i] * b;
+          w.Z(r, i + 1) = rs[i] * a + rc[i] * b;
+        }
+    }
+    x.sync();
+  }
+  x.stamp(3);
+  // ---- Hessenberg-triangular re-reduction of the leading m x m block
+  //      by Givens rotations (the job of DGGHRD at qzearly.f:449).  Each
+  //      pair (row rotation zeroing H(jr, jc), column rotation removing the
+  //      T(jr, jr-1) it creates) is computed by every thread from the 2x2
+  //      block of T; thread 0 transforms the 2x2 blocks of H and T that both
+  //      rotations touch, everyone else the disjoint rest: two barriers per
+  //      pair ----
+  for (int jc = 0; jc < m - 2; ++jc) {
+    for (int jr = m - 1; jr >= jc + 2; --jr) {
+      x.count(2);
+      double c, sn, r;
+      lartg(w.H(jr - 1, jc), w.H(jr, jc), c, sn, r);
+      // T after the row rotation: (jr, jr-1) fill, (jr, jr) updated
+      const double t00 = w.T(jr - 1, jr - 1), t01 = w.T(jr - 1, jr), t11 = w.T(jr, jr);
+      const double u10 = -sn * t00, u11 = -sn * t01 + c * t11;
+      double cz, sz, rz;
+      lartg(u11, u10, cz, sz, rz);  // pair (col jr, col jr-1): zero T(jr, jr-1)
+      double hb[4], tb2[2];
+      if (x.tid == 0) {
+        // H(jr-1..jr, jr-1..jr): row rotation, then column rotation
+        double h00 = w.H(jr - 1, jr - 1), h10 = w.H(jr, jr - 1), h01 = w.H(jr - 1, jr), h11 = w.H(jr, jr);
+        rot2(c, sn, h00, h10);
+        rot2(c, sn, h01, h11);
+        rot2(cz, sz, h01, h00);
+        rot2(cz, sz, h11, h10);
+        hb[0] = h00; hb[1] = h10; hb[2] = h01; hb[3] = h11;
+        // T(jr-1, jr-1..jr) after both (row jr of the block is (0, rz))
+        double u00 = c * t00, u01 = c * t01 + sn * t11;
+        rot2(cz, sz, u01, u00);
+        tb2[0] = u00; tb2[1] = u01;
+      }
+      x.sync();
+      {
+        // row rotation: H rows jr-1, jr, columns jc+1..jr-2 and jr+1..n-1;
+        // T rows jr-1, jr, columns jr+1..n-1; Q columns jr-1, jr
+        const Seg a = seg_rows(w.H, jr - 1, jc + 1, jr - 1), b = seg_rows(w.H, jr - 1, jr + 1, n);
+        const Seg t = seg_rows(w.T, jr - 1, jr + 1, n);
+        const Seg q = w.wantq ? seg_cols(w.Q, jr - 1, 0, n) : no_seg();
+        // column rotation (col jr, col jr-1): H rows 0..jr-2 and jr+1..m-1;
+        // T rows 0..jr-2; Z columns
+        const Seg d = Seg{&w.H(0, jr), 1, -(int64_t)w.H.ld, jr - 1};
+        const Seg e = Seg{&w.H(jr + 1, jr), 1, -(int64_t)w.H.ld, m - jr - 1};
+        const Seg g = Seg{&w.T(0, jr), 1, -(int64_t)w.T.ld, jr - 1};
+        const Seg z = w.wantz ? Seg{&w.Z(0, jr), 1, -(int64_t)w.Z.ld, n} : no_seg();
+        const int n1 = seg_total(a, b, t), n2 = n1 + seg_total(q, no_seg(), no_seg());
+        const int n3 = n2 + seg_total(d, e, g), total = n3 + seg_total(z, no_seg(), no_seg());
+        for (int idx = x.tid; idx < total; idx += x.nt) {
+          double* p;
+          int64_t st;
+          bool row;
+          if (idx < n1) { seg_item(a, b, t, idx, p, st); row = true; }
+          else if (idx < n2) { seg_item(q, no_seg(), no_seg(), idx - n1, p, st); row = true; }
+          else if (idx < n3) { seg_item(d, e, g, idx - n2, p, st); row = false; }
+          else { seg_item(z, no_seg(), no_seg(), idx - n3, p, st); row = false; }
+          const double u = p[0], v = p[st];
+          const double cc = row ? c : cz, ss = row ? sn : sz;
+          p[0] = cc * u + ss * v;
+          p[st] = -ss * u + cc * v;
+        }
+      }
+      if (x.tid == 0) {
+        w.H(jr - 1, jc) = r; w.H(jr, jc) = 0.0;
+        w.H(jr - 1, jr - 1) = hb[0]; w.H(jr, jr - 1) = hb[1]; w.H(jr - 1, jr) = hb[2]; w.H(jr, jr) = hb[3];
+        w.T(jr - 1, jr - 1) = tb2[0]; w.T(jr - 1, jr) = tb2[1];
+        w.T(jr, jr - 1) = 0.0; w.T(jr, jr) = rz;
+      }
+      x.sync();
+    }
+  }
+  x.stamp(4);
+}
+
+}  // namespace qz

@@ -29,6 +29,7 @@ struct HostExec {
   HostExec() : sdv(16384, 0.0) { sd = sdv.data(); }
   void sync() {}
   void stamp(int) {}
+  void count(int) {}
 };
 
 Tol make_tol(const double* H, const double* T, int ld, int o, int nh) {
@@ -64,6 +65,7 @@ struct HostBK {
   bool wantq = true, wantz = true;
   int nskip = 4;
   int swapfail = 0;
+  int ms = 1;  // multishift window QZ
   // JOB = 'E': far updates of H and T stop at the active block (as in the
   // device backend)
   bool schur = true;
@@ -121,7 +123,7 @@ struct HostBK {
     w.n = nw; w.H = MatV{Hs.data(), nw}; w.T = MatV{Ts.data(), nw}; w.Q = MatV{Us.data(), nw};
     w.Z = MatV{Vs.data(), nw}; w.wantq = true; w.wantz = true; w.tol = tol;
     cta_aed(x, w, s, s3.data(), s3.data() + nw, s3.data() + 2 * nw, 30 * nw, (kwtop > ktop) ? nskip : 0,
-            swapfail != 0);
+            swapfail != 0, ms ? x.sd + 64 + 4 * nw : nullptr);
     const int m = x.si[8], st = x.si[9], tr = x.si[10];
     if (st == 0 && tr) {
       store(kwtop, nw, Hs, Ts);
@@ -238,6 +240,16 @@ int host_small_qz(int n, double* H, double* T, double* Q, double* Z) {
   return cta_small_qz(x, w, 30 * n);
 }
 
+// The same with the multishift window QZ (lockstep chains of bulges).
+int host_small_qz_ms(int n, double* H, double* T, double* Q, double* Z) {
+  static HostExec x;
+  WinState w;
+  w.n = n; w.H = MatV{H, n}; w.T = MatV{T, n}; w.Q = MatV{Q, n}; w.Z = MatV{Z, n};
+  w.wantq = w.wantz = true;
+  w.tol = make_tol(H, T, n, 0, n);
+  return cta_small_qz_ms(x, w, 30 * n, x.sd + 1024);
+}
+
 // AED on a whole window with spike s (Q, Z identity on entry); out3 =
 // {undeflated m, status, transformed}; shifts: alphar, alphai, beta (n each).
 void host_aed(int n, double* H, double* T, double* Q, double* Z, double s, int nskip, double* shifts, int* out3) {
@@ -300,7 +312,8 @@ int host_solve(int n, double* H, double* T, double* Q, double* Z, int nw_max, in
 }
 
 // The same with more controls: ip = {nw_max, w_chase, nmin, nskip,
-// stall_limit, aed_swap_fail, schur (1: JOB='S', 0: JOB='E')}.  Returns
+// stall_limit, aed_swap_fail, schur (1: JOB='S', 0: JOB='E'), window QZ
+// (1: multishift, 0: double shift)}.  Returns
 // INFO (0, or the 1-based unconverged row).  The eigenvalues are read from
 // the diagonal blocks also for JOB='E'.
 int host_solve_p(int n, double* H, double* T, double* Q, double* Z, const int* ip, double* ar, double* ai, double* be,
@@ -309,6 +322,7 @@ int host_solve_p(int n, double* H, double* T, double* Q, double* Z, const int* i
   bk.n = n; bk.ld = n; bk.H = H; bk.T = T; bk.Q = Q; bk.Z = Z; bk.nskip = ip[3];
   bk.swapfail = ip[5];
   bk.schur = ip[6] != 0;
+  bk.ms = ip[7];
   bk.act_top = 0;
   bk.act_bot = n - 1;
   bk.tol = make_tol(H, T, n, 0, n);

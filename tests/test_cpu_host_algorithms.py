@@ -25,6 +25,8 @@ def host(tmp_path_factory):
     L = ctypes.CDLL(out)
     L.host_small_qz.argtypes = [ctypes.c_int] + [_pd] * 4
     L.host_small_qz.restype = ctypes.c_int
+    L.host_small_qz_ms.argtypes = [ctypes.c_int] + [_pd] * 4
+    L.host_small_qz_ms.restype = ctypes.c_int
     L.host_aed.argtypes = [ctypes.c_int] + [_pd] * 4 + [ctypes.c_double, ctypes.c_int, _pd, _pi]
     L.host_aed.restype = None
     L.host_solve.argtypes = [ctypes.c_int] + [_pd] * 4 + [ctypes.c_int] * 4 + [_pd] * 3 + [_pi]
@@ -56,6 +58,21 @@ def test_host_window_qz(pkg, lapack, host, n, seed, zf):
     H, T = pkg.pencils.random_ht(n, seed, zf)
     S, P, Q, Z = (np.array(M, order="F", copy=True) for M in (H, T, np.eye(n), np.eye(n)))
     assert host.host_small_qz(n, _p(S), _p(P), _p(Q), _p(Z)) == 0
+    _check(lapack, H, T, S, P, Q, Z)
+
+
+@pytest.mark.parametrize("n,seed,kind", [(30, 1, "r"), (48, 2, "z"), (64, 3, "g"), (80, 4, "r"), (80, 5, "c"),
+                                         (160, 6, "r")])
+def test_host_window_qz_multishift(pkg, lapack, host, n, seed, kind):
+    """Window QZ by small-bulge multishift sweeps (lockstep chains, shifts
+    from the trailing block's eigenvalues): generalized Schur form, backward
+    errors within 50 n eps and the eigenvalues of LAPACK DHGEQZ."""
+    P_ = pkg.pencils
+    H, T = {"r": lambda: P_.random_ht(n, seed), "z": lambda: P_.random_ht(n, seed, 0.05),
+            "g": lambda: P_.graded_ht(n, seed), "c": lambda: P_.clustered_ht(n, seed, every=11, scale=1e-9)}[kind]()
+    S, P, Q, Z = (np.array(M, order="F", copy=True) for M in (H, T, np.eye(n), np.eye(n)))
+    assert host.host_small_qz_ms(n, _p(S), _p(P), _p(Q), _p(Z)) == 0
+    assert lapack.schur_structure_ok(S, P)
     _check(lapack, H, T, S, P, Q, Z)
 
 
@@ -191,8 +208,11 @@ def test_host_solve_edge_cases(pkg, lapack, host, kind):
     # the (alpha, beta) convention of the Schur form's blocks, also for
     # eigenvalues far from 1 in magnitude
     e = lapack.eig_from_schur(S, P)
-    for x, y in zip(e, (ar, ai, be)):
-        assert np.allclose(x, y, rtol=1e-12, atol=1e-300)
+    assert np.allclose(e[2], be, rtol=1e-12, atol=1e-300)
+    # alpha as a complex number, relative to its modulus (the imaginary part
+    # of a nearly real pair is ill-conditioned on its own)
+    a_ref, a = e[0] + 1j * e[1], ar + 1j * ai
+    assert np.all(np.abs(a - a_ref) <= 1e-12 * np.maximum(np.abs(a_ref), 1e-300))
     _check(lapack, H, T, S, P, Q, Z, eig=(ar, ai, be))
 
 
@@ -211,12 +231,12 @@ def test_host_solve_default_windows(pkg, lapack, host):
     _check(lapack, H, T, S, P, Q, Z, eig=(ar, ai, be))
 
 
-def _solve_p(host, H, T, nw=32, wc=40, nmin=40, nskip=4, stall=300, swapfail=0, schur=1):
+def _solve_p(host, H, T, nw=32, wc=40, nmin=40, nskip=4, stall=300, swapfail=0, schur=1, ms=1):
     n = H.shape[0]
     S, P, Q, Z = (np.array(M, order="F", copy=True) for M in (H, T, np.zeros((n, n)), np.zeros((n, n))))
     ar, ai, be = np.zeros(n), np.zeros(n), np.zeros(n)
     st = np.zeros(5, dtype=np.int32)
-    ip = np.array([nw, wc, nmin, nskip, stall, swapfail, schur], dtype=np.int32)
+    ip = np.array([nw, wc, nmin, nskip, stall, swapfail, schur, ms], dtype=np.int32)
     info = host.host_solve_p(n, _p(S), _p(P), _p(Q), _p(Z), ip.ctypes.data_as(_pi), _p(ar), _p(ai), _p(be),
                              st.ctypes.data_as(_pi))
     return info, (S, P, Q, Z), (ar, ai, be), st
