@@ -9,7 +9,10 @@
 // decreasing size (longest-first scheduling), solve a pencil in shared
 // memory when n <= kBatchSmemMax (H, T, Q, Z with an odd leading
 // dimension), in place in global memory otherwise, normalise beta >= 0 and
-// write the eigenvalues.  Per-pencil status words; no host round trip.
+// write the eigenvalues.  Pencils long enough for chains of bulges are
+// reduced by small-bulge multishift sweeps (cta_small_qz_ms), shorter
+// ones by double-shift sweeps.  Per-pencil status words; no host round
+// trip.
 #include <cuda_runtime.h>
 #include <float.h>
 #include <stdint.h>
@@ -19,7 +22,7 @@
 
 #include "../../include/b200qz.h"
 #include "kernels.h"
-#include "qz_cta.cuh"
+#include "qz_window.cuh"
 
 namespace qz {
 
@@ -62,6 +65,7 @@ __global__ void __launch_bounds__(kBatchThreads) k_batch_qz(int count, const int
   __shared__ double red[32];
   __shared__ int si[64];
   __shared__ double sd_small[64];
+  __shared__ double ms_scr[kMsScratch];  // multishift window QZ scratch
   for (;;) {
     if (threadIdx.x == 0) s_next = atomicAdd(counter, 1);
     __syncthreads();
@@ -125,7 +129,8 @@ __global__ void __launch_bounds__(kBatchThreads) k_batch_qz(int count, const int
     w.wantq = true;
     w.wantz = true;
     w.tol = tol;
-    int info = cta_small_qz(x, w, 30 * n);
+    // pencils long enough for chains of bulges take multishift sweeps
+    int info = cta_small_qz_ms(x, w, 30 * n, ms_scr);
     __syncthreads();
     if (info == 0) cta_finalize(x, w, AR + eoff[p], AI + eoff[p], BE + eoff[p]);
     if (in_smem) {

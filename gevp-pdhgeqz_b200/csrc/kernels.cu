@@ -307,9 +307,9 @@ __global__ void k_eigs(const double* H, const double* T, int64_t ld, int n, doub
   double o_ar[2], o_ai[2], o_be[2];
   eig2_complex(a, G((double*)T, ld, f, f), G((double*)T, ld, f + 1, f + 1), o_ar, o_ai, o_be);
   int e = j - f;
-  ar[j] = o_ar[e];
-  ai[j] = o_ai[e];
-  be[j] = o_be[e];
+  ar[j] = e ? o_ar[1] : o_ar[0];  // selects keep the pair in registers
+  ai[j] = e ? o_ai[1] : o_ai[0];
+  be[j] = e ? o_be[1] : o_be[0];
 }
 
 __global__ void k_set_identity(double* Q, int64_t ld, int n) {

@@ -612,40 +612,52 @@ QZ_HD void small_qr_q(double* X, double* Q) {
 // column-major, ld S): the pivot of column k is the largest entry of that
 // column at or below the diagonal, so the search is S - k compares (complete
 // pivoting searches (S - k)^2 entries, which made the serial solve the
-// longest part of a block swap).  Row exchanges are predicated moves so the
-// matrix stays in registers.  Tiny pivots are replaced by smin (the DGETC2
-// device); returns false if that happened.  An inaccurate solution is caught
-// by the swap's stability test, which then rejects the swap.
+// longest part of a block swap).  The elimination steps are unrolled by
+// template recursion and row exchanges are selects, so every index is a
+// compile-time constant and the system stays in registers.  Tiny pivots are
+// replaced by smin (the DGETC2 device); an inaccurate solution is caught by
+// the swap's stability test, which then rejects the swap.
+template <int S, int K>
+struct SmallElim {
+  static QZ_HD void run(double* A, double* rhs, double smin, bool& exact) {
+    if constexpr (K < S) {
+      int pi = K;
+      double best = fabs(A[K + S * K]);
+#pragma unroll
+      for (int i = K + 1; i < S; ++i) {
+        const double v = fabs(A[i + S * K]);
+        if (v > best) { best = v; pi = i; }
+      }
+#pragma unroll
+      for (int i = K + 1; i < S; ++i) {
+        const bool sw = (pi == i);
+#pragma unroll
+        for (int j = K; j < S; ++j) {
+          const double a = A[K + S * j], b = A[i + S * j];
+          A[K + S * j] = sw ? b : a;
+          A[i + S * j] = sw ? a : b;
+        }
+        const double a = rhs[K], b = rhs[i];
+        rhs[K] = sw ? b : a;
+        rhs[i] = sw ? a : b;
+      }
+      if (fabs(A[K + S * K]) < smin) { A[K + S * K] = smin; exact = false; }
+      const double rpiv = 1.0 / A[K + S * K];
+#pragma unroll
+      for (int i = K + 1; i < S; ++i) {
+        const double f = A[i + S * K] * rpiv;
+#pragma unroll
+        for (int j = K + 1; j < S; ++j) A[i + S * j] -= f * A[K + S * j];
+        rhs[i] -= f * rhs[K];
+      }
+      SmallElim<S, K + 1>::run(A, rhs, smin, exact);
+    }
+  }
+};
 template <int S>
 QZ_HD bool small_solve_cp(double* A, double* rhs, double smin) {
   bool exact = true;
-#pragma unroll
-  for (int k = 0; k < S; ++k) {
-    int pi = k;
-    double best = fabs(A[k + S * k]);
-#pragma unroll
-    for (int i = k + 1; i < S; ++i) {
-      const double v = fabs(A[i + S * k]);
-      if (v > best) { best = v; pi = i; }
-    }
-#pragma unroll
-    for (int i = k + 1; i < S; ++i)
-      if (pi == i) {
-#pragma unroll
-        for (int j = k; j < S; ++j) { double t = A[k + S * j]; A[k + S * j] = A[i + S * j]; A[i + S * j] = t; }
-        double t = rhs[k]; rhs[k] = rhs[i]; rhs[i] = t;
-      }
-    if (fabs(A[k + S * k]) < smin) { A[k + S * k] = smin; exact = false; }
-    const double rpiv = 1.0 / A[k + S * k];
-#pragma unroll
-    for (int i = k + 1; i < S; ++i) {
-      double f = A[i + S * k] * rpiv;
-#pragma unroll
-      for (int j = k + 1; j < S; ++j) A[i + S * j] -= f * A[k + S * j];
-      rhs[i] -= f * rhs[k];
-      A[i + S * k] = 0.0;
-    }
-  }
+  SmallElim<S, 0>::run(A, rhs, smin, exact);
 #pragma unroll
   for (int k = S - 1; k >= 0; --k) {
     double acc = rhs[k];
@@ -910,9 +922,10 @@ QZ_HD void cta_finalize(X& x, WinState& w, double* ar, double* ai, double* be) {
     double a[4] = {w.H(f, f), w.H(f + 1, f), w.H(f, f + 1), w.H(f + 1, f + 1)};
     double o_ar[2], o_ai[2], o_be[2];
     eig2_complex(a, w.T(f, f), w.T(f + 1, f + 1), o_ar, o_ai, o_be);
-    ar[j] = o_ar[j - f];
-    ai[j] = o_ai[j - f];
-    be[j] = o_be[j - f];
+    const bool second = j > f;  // selects keep the pair in registers
+    ar[j] = second ? o_ar[1] : o_ar[0];
+    ai[j] = second ? o_ai[1] : o_ai[0];
+    be[j] = second ? o_be[1] : o_be[0];
   }
   x.sync();
 }

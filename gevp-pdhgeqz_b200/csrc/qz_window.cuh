@@ -140,8 +140,7 @@ QZ_HD int cta_small_qz_ms(X& x, WinState& w, int maxit, double* scr) {
         ws.n = k; ws.H = Hc; ws.T = Tc; ws.Q = Hc; ws.Z = Hc;
         ws.wantq = false; ws.wantz = false;
         ws.tol = w.tol;
-        int sis[4];
-        SoloExec solo{0, 1, sis, nullptr};
+        SoloExec solo{0, 1, x.si + 16, nullptr};  // si[16..17]: free during the window QZ
         const int inf = cta_small_qz(solo, ws, 30 * k);
         int got = (inf == 0) ? shifts_from_schur(Hc, Tc, k, bl, nb) : 0;
         for (int b = 0; b < got; ++b) {
