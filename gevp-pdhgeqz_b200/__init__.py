@@ -69,7 +69,7 @@ STAT_NAMES = ("seconds", "iters", "aeds", "aed_deflations", "sweeps", "chains", 
               "ms_aed_smallqz", "ms_aed_reorder", "ms_aed_spike", "ms_aed_hessred", "launches",
               "aed_failures", "exceptional_sweeps", "remaining", "stop_ktop", "stop_kbot", "last_aed_fraction",
               "policy_calls", "aed_bytes", "aed_launches", "chase_bytes", "chase_launches",
-              "aed_qz_steps", "aed_swaps", "aed_rotations")
+              "aed_qz_steps", "aed_swaps", "aed_rotations", "aed_ms_sweeps")
 
 
 def lib() -> ctypes.CDLL:

@@ -25,6 +25,7 @@ using namespace qz;
 namespace {
 constexpr int kAedMax = 512;  // largest AED / small-solve window supported
 constexpr int64_t kUslot = (int64_t)kWinSmemMax * kWinSmemMax;  // one window's factor in Uc/Vc
+constexpr int kTsSlots = 16;  // AED kernel profiling: stamps 0..4, counters 5..8
 }
 
 // Phase timer: CUDA event pairs recorded around each group of launches on
@@ -130,7 +131,8 @@ struct b200qz_ctx {
   double batch_seconds = 0.0;
   unsigned long long* hts = nullptr;  // pinned mirror
   double aed_ms[4] = {0, 0, 0, 0};   // small QZ, reorder, spike+RQ, HT re-reduction
-  double aed_counts[3] = {0, 0, 0};  // small-QZ steps, block swaps, re-reduction rotation pairs
+  double aed_counts[4] = {0, 0, 0, 0};  // small-QZ steps, block swaps, re-reduction rotation pairs,
+                                        // multishift window sweeps
 };
 
 namespace {
@@ -199,7 +201,7 @@ struct GpuBackend {
     QZ_CK(cudaMemcpyAsync(c->hinfo + 4, c->dinfo + 4, 3 * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     QZ_CK(cudaMemcpyAsync(c->hshifts, c->shifts, 3 * nw * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     if (c->timer.on)
-      QZ_CK(cudaMemcpyAsync(c->hts, c->dts, 8 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream));
+      QZ_CK(cudaMemcpyAsync(c->hts, c->dts, kTsSlots * sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream));
     QZ_CK(cudaStreamSynchronize(c->stream));
     c->ka = nw;
     if (c->timer.on) {
@@ -214,8 +216,9 @@ struct GpuBackend {
       c->aed_counts[0] += (double)t[5];
       c->aed_counts[1] += (double)t[6];
       c->aed_counts[2] += (double)t[7];
-      for (int i = 0; i < 8; ++i) t[i] = 0;
-      QZ_CK(cudaMemsetAsync(c->dts, 0, 8 * sizeof(unsigned long long), c->stream));
+      c->aed_counts[3] += (double)t[8];
+      for (int i = 0; i < kTsSlots; ++i) t[i] = 0;
+      QZ_CK(cudaMemsetAsync(c->dts, 0, kTsSlots * sizeof(unsigned long long), c->stream));
     }
     if (c->err != cudaSuccess) { info3[0] = nw; info3[1] = 1; info3[2] = 0; return; }
     info3[0] = c->hinfo[4];
@@ -549,9 +552,9 @@ int b200qz_create(b200qz_ctx** out, int device) {
   if (e == cudaSuccess) e = cudaMallocHost(&c->hinfo, 16 * sizeof(int));
   if (e == cudaSuccess) e = cudaMallocHost(&c->hshifts, 3 * kAedMax * sizeof(double));
   if (e == cudaSuccess) e = cudaMallocHost(&c->hnorms, 2 * sizeof(double));
-  if (e == cudaSuccess) e = cudaMalloc(&c->dts, 8 * sizeof(unsigned long long));
-  if (e == cudaSuccess) e = cudaMemset(c->dts, 0, 8 * sizeof(unsigned long long));
-  if (e == cudaSuccess) e = cudaMallocHost(&c->hts, 8 * sizeof(unsigned long long));
+  if (e == cudaSuccess) e = cudaMalloc(&c->dts, kTsSlots * sizeof(unsigned long long));
+  if (e == cudaSuccess) e = cudaMemset(c->dts, 0, kTsSlots * sizeof(unsigned long long));
+  if (e == cudaSuccess) e = cudaMallocHost(&c->hts, kTsSlots * sizeof(unsigned long long));
   if (e == cudaSuccess) e = cudaEventCreate(&c->ev0);
   if (e == cudaSuccess) e = cudaEventCreate(&c->ev1);
   if (e != cudaSuccess) {
@@ -699,7 +702,7 @@ int b200qz_get_stats(const b200qz_ctx* c, double* out, int nout) {
   if (!c || !out) return 0;
   const SolveStats& s = c->stats;
   const double* ph = c->timer.ms;
-  double v[38] = {c->seconds, (double)s.iters, (double)s.aeds, (double)s.aed_defl, (double)s.sweeps,
+  double v[39] = {c->seconds, (double)s.iters, (double)s.aeds, (double)s.aed_defl, (double)s.sweeps,
                   (double)s.chains, (double)s.windows, (double)s.endgames, (double)s.infs, (double)s.shifts,
                   s.upd_flops, s.win_bytes,
                   ph[kPhScan], ph[kPhAed], ph[kPhAedUpd], ph[kPhChase], ph[kPhChaseUpd], ph[kPhInf], ph[kPhFinal],
@@ -707,8 +710,8 @@ int b200qz_get_stats(const b200qz_ctx* c, double* out, int nout) {
                   (double)s.aed_fail, (double)s.exceptional, (double)s.remaining, (double)s.stop_ktop,
                   (double)s.stop_kbot, s.last_frac, (double)s.policy_calls, s.aed_bytes,
                   (double)s.aed_launches, s.chase_bytes, (double)s.chase_launches, c->aed_counts[0],
-                  c->aed_counts[1], c->aed_counts[2]};
-  int k = std::min(nout, 38);
+                  c->aed_counts[1], c->aed_counts[2], c->aed_counts[3]};
+  int k = std::min(nout, 39);
   for (int i = 0; i < k; ++i) out[i] = v[i];
   return k;
 }

@@ -40,8 +40,8 @@ struct DevExecT {
       ts[k] = t;
     }
   }
-  // event counters (profiling): 0 small-QZ steps, 1 block swaps, 2
-  // re-reduction rotation pairs
+  // event counters (profiling, ts has 16 slots): 0 double-shift steps, 1
+  // block swaps, 2 re-reduction rotation pairs, 3 multishift window sweeps
   __device__ void count(int k) {
     if (ts && tid == 0) ts[5 + k] += 1;
   }

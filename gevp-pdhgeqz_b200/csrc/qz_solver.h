@@ -41,7 +41,7 @@ struct SolveParams {
   int upd_persist = 1;   // 1: persistent, prefetching DMMA update kernels
   int aed_limit = -1;    // >= 0: stop before the AED after this many AEDs
                          // (tuning traces; the solve then returns -2)
-  int aed_ms = 1;        // window QZ of the AED kernel: 1 small-bulge multishift
+  int aed_ms = 0;        // window QZ of the AED kernel: 1 small-bulge multishift
                          // (lockstep chains), 0 double shift
   int aed_swap_fail = 0; // 1: every block swap inside the AED reports failure
                          // (exercises the swap-failure branch, qzearly.f:321-326)

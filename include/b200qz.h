@@ -100,8 +100,8 @@ int b200qz_solve_host(b200qz_ctx* ctx, char job, char compq, char compz, int n, 
  * bytes of the AED/endgame window kernels (6*8*w^2 per window of order w),
  * 32 their launches, 33 algorithmic bytes of the chase windows, 34 chase
  * launches (one per wave of concurrent windows); with B200QZ_PROFILE=1
- * also 35 small-QZ steps, 36 block swaps and 37 re-reduction rotation
- * pairs executed inside the AED kernels.
+ * also 35 double-shift steps, 36 block swaps, 37 re-reduction rotation
+ * pairs and 38 multishift window sweeps executed inside the AED kernels.
  * Returns the number of values written. */
 int b200qz_get_stats(const b200qz_ctx* ctx, double* out, int nout);
 

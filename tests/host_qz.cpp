@@ -21,14 +21,24 @@ using namespace qz;
 
 namespace {
 
+// Barrier counts by AED phase (the latency model of the device kernels:
+// each barrier separates two dependent steps): [0] outside the AED kernel
+// routine, [1] window QZ, [2] spike test + reordering, [3] spike reflector
+// + RQ update, [4] Hessenberg-triangular re-reduction; [5] AED routine calls.
+static long g_barriers[6] = {0, 0, 0, 0, 0, 0};
+static int g_phase = 0;
+
 struct HostExec {
   int tid = 0, nt = 1;
   int si[64];
   double* sd;
   std::vector<double> sdv;
   HostExec() : sdv(16384, 0.0) { sd = sdv.data(); }
-  void sync() {}
-  void stamp(int) {}
+  void sync() { ++g_barriers[g_phase]; }
+  void stamp(int k) {
+    g_phase = (k < 4) ? k + 1 : 0;
+    if (k == 0) ++g_barriers[5];
+  }
   void count(int) {}
 };
 
@@ -229,6 +239,12 @@ struct HostBK {
 }  // namespace
 
 extern "C" {
+
+void host_barriers(long* out, int reset) {
+  for (int i = 0; i < 6; ++i) out[i] = g_barriers[i];
+  if (reset)
+    for (int i = 0; i < 6; ++i) g_barriers[i] = 0;
+}
 
 // Window QZ of an n x n pencil (Q, Z accumulate from their input).
 int host_small_qz(int n, double* H, double* T, double* Q, double* Z) {

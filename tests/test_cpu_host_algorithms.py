@@ -35,6 +35,8 @@ def host(tmp_path_factory):
     L.host_chase.restype = None
     L.host_solve_p.argtypes = [ctypes.c_int] + [_pd] * 4 + [_pi] + [_pd] * 3 + [_pi]
     L.host_solve_p.restype = ctypes.c_int
+    L.host_barriers.argtypes = [ctypes.POINTER(ctypes.c_long), ctypes.c_int]
+    L.host_barriers.restype = None
     return L
 
 
@@ -285,3 +287,25 @@ def test_host_job_e(pkg, lapack, host, kind):
     eps = np.finfo(float).eps
     assert np.linalg.norm(Q.T @ Q - np.eye(n)) <= 50 * n * eps
     assert np.linalg.norm(Z.T @ Z - np.eye(n)) <= 50 * n * eps
+
+
+def test_host_aed_barrier_budget(pkg, lapack, host):
+    """The AED kernel's latency model: barriers per AED-routine call on a
+    graded pencil with the default window 48 and the whole-window spike test.
+    The multishift window QZ needs fewer barriers than double-shift sweeps;
+    the total stays under the budget the kernel was designed to (a
+    regression guard for the dependent-step count)."""
+    H, T = pkg.pencils.graded_ht(900, 2)
+    per = {}
+    for ms in (0, 1):
+        b = (ctypes.c_long * 6)()
+        host.host_barriers(b, 1)
+        info, (S, P, Q, Z), eig, st = _solve_p(host, H, T, nw=48, wc=80, nmin=80, nskip=0, ms=ms)
+        assert info == 0
+        host.host_barriers(b, 1)
+        calls = max(1, b[5])
+        per[ms] = [b[i] / calls for i in range(5)]
+        _check(lapack, H, T, S, P, Q, Z, eig=eig)
+    print("barriers per AED call (double shift / multishift):", per)
+    assert per[1][1] < 0.8 * per[0][1]
+    assert sum(per[1][1:]) < 6000
