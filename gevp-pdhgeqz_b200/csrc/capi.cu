@@ -87,8 +87,17 @@ struct BatchKey {
   }
 };
 
+// Tensor maps of the split-precision update, cached by matrix and box.
+struct TmapEntry {
+  const double* M;
+  int64_t ld;
+  int n, left, k;
+  CUtensorMap map;
+};
+
 struct b200qz_ctx {
   int device = 0;
+  std::vector<TmapEntry> tmaps;       // split-precision update: encoded tensor maps
   cudaStream_t stream = nullptr;
   double* Ua = nullptr;  // AED window factors (kAedMax^2)
   double* Va = nullptr;
@@ -276,10 +285,34 @@ struct GpuBackend {
     R.njobs = 0;
     L.bslices = R.bslices = c->ozb;
     L.err = R.err = c->ozerr;
+    // TMA tensor map of (M, side, k) in batch B: index, or -1 (plain loads)
+    auto map_for = [&](OzBatch& B, int& nmaps, const double* (&mm)[kOzMaxMaps], int (&mk)[kOzMaxMaps],
+                       int (&ml)[kOzMaxMaps], const double* M, int left, int k) -> int {
+      for (int i = 0; i < nmaps; ++i)
+        if (mm[i] == M && mk[i] == k && ml[i] == left) return i;
+      if (nmaps == kOzMaxMaps) return -1;
+      const TmapEntry* hit = nullptr;
+      for (const TmapEntry& e : c->tmaps)
+        if (e.M == M && e.ld == ld && e.n == n && e.left == left && e.k == k) { hit = &e; break; }
+      if (!hit) {
+        TmapEntry e{M, ld, n, left, k, {}};
+        if (!ozaki_tensor_map(&e.map, M, ld, n, n, left, k)) return -1;
+        if (c->tmaps.size() >= 64) c->tmaps.erase(c->tmaps.begin());
+        c->tmaps.push_back(e);
+        hit = &c->tmaps.back();
+      }
+      B.maps[nmaps] = hit->map;
+      mm[nmaps] = M; mk[nmaps] = k; ml[nmaps] = left;
+      return nmaps++;
+    };
+    int nmL = 0, nmR = 0;
+    const double* mmL[kOzMaxMaps]; int mkL[kOzMaxMaps], mlL[kOzMaxMaps];
+    const double* mmR[kOzMaxMaps]; int mkR[kOzMaxMaps], mlR[kOzMaxMaps];
     auto job = [&](OzBatch& B, double* M, int r0, int c0, int len, int k, int left, int fac) {
       OzJob& j = B.job[B.njobs++];
       j.M = M; j.ld = ld; j.r0 = r0; j.c0 = c0; j.len = len; j.k = k; j.left = left; j.fac = fac;
       j.tiles = (len + 127) / 128;
+      j.map = (&B == &L) ? map_for(B, nmL, mmL, mkL, mlL, M, left, k) : map_for(B, nmR, mmR, mkR, mlR, M, left, k);
     };
     for (int i = 0; i < nwin; ++i) {
       const int k = wk[i], w0 = w[i];
@@ -804,6 +837,13 @@ int b200qz_update_split(b200qz_ctx* c, char side, double* m, int ldm, int r0, in
   OzJob& j = B.job[0];
   j.M = m; j.ld = ldm; j.r0 = r0; j.c0 = c0; j.len = len; j.k = k; j.left = is(side, 'L') ? 1 : 0; j.fac = 0;
   j.tiles = (len + 127) / 128;
+  // the slab as a TMA tensor map when its leading dimension allows
+  j.map = -1;
+  {
+    // the map spans exactly the slab's rows and columns from the origin
+    const int rows = r0 + (j.left ? k : len), cols = c0 + (j.left ? len : k);
+    if (rows <= ldm && ozaki_tensor_map(&B.maps[0], m, ldm, rows, cols, j.left, k)) j.map = 0;
+  }
   launch_ozaki_prep(c->stream, P, slices);
   launch_ozaki_update(c->stream, B, slices);
   QZ_CK(cudaGetLastError());

@@ -179,14 +179,58 @@ __device__ __forceinline__ int oz_find_job(const OzBatch& B, int& tile) {
 }
 
 // shared memory: A digits (S x 128 x Kp) | B digits + scales | FP64 staging
-// (64 input rows x (k+1), or one 128 x 33 output chunk)
-constexpr int kOzStageDoubles = 64 * (kOzMaxK + 1);
+// (half a slab tile: a TMA box of 66 x k or kbox x 64, or 64 x (k+1) for
+// plain loads; or one 128 x 33 output chunk)
+constexpr int kOzStageDoubles = kOzBoxRows * kOzMaxK;
 static_assert(kOzStageDoubles >= kOzRows * (kOzOutN + 1), "staging too small");
+static_assert(kOzStageDoubles >= 64 * (kOzMaxK + 1), "staging too small");
+static_assert(kOzStageDoubles >= 64 * oz_left_box(kOzMaxK), "staging too small");
+
+__device__ __forceinline__ void mbar_init(uint64_t* m, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(m)), "r"(count));
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* m, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(m)), "r"(bytes) : "memory");
+}
+// bounded wait on an mbarrier phase; false if it did not complete
+__device__ __forceinline__ bool mbar_wait(uint64_t* m, uint32_t parity) {
+  uint32_t done = 0, spins = 0;
+  while (!done && spins < kOzSpinLimit) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(smem_u32(m)), "r"(parity)
+        : "memory");
+    ++spins;
+  }
+  return done != 0;
+}
+// one-dimensional bulk copy global -> shared (16-byte aligned, size a
+// multiple of 16), completion counted on the mbarrier
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* m) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(m))
+               : "memory");
+}
+// two-dimensional TMA tile load (no multicast): box of the tensor map at
+// element coordinates (x, y), x the contiguous dimension
+__device__ __forceinline__ void tma_g2s_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* m) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::
+          "r"(smem_u32(dst)),
+      "l"(map), "r"(x), "r"(y), "r"(smem_u32(m))
+      : "memory");
+}
 
 template <int S>
-__global__ void __launch_bounds__(kOzThreads, 1) k_ozaki_update(const OzBatch B) {
+__global__ void __launch_bounds__(kOzThreads, 1) k_ozaki_update(const __grid_constant__ OzBatch B) {
   extern __shared__ __align__(1024) uint8_t oz_smem[];
   __shared__ uint64_t mbar;
+  __shared__ uint64_t lbar;  // loads (bulk copy of the B digits, TMA halves of the slab tile)
   __shared__ uint32_t tmem_base_s;
   __shared__ int escale[kOzRows];
   int tile;
@@ -214,39 +258,77 @@ __global__ void __launch_bounds__(kOzThreads, 1) k_ozaki_update(const OzBatch B)
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   if (tid == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&mbar)), "r"(1));
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    mbar_init(&mbar, 1);
+    mbar_init(&lbar, 1);
   }
-  // B digits and column scales (prepared once per factor)
-  {
-    const int nb = (S * kp * Kp + 4 * kp) / 16;
-    const uint4* src = (const uint4*)Bg;
-    uint4* dst = (uint4*)Bs;
-    for (int i = tid; i < nb; i += kOzThreads) dst[i] = src[i];
+  __syncthreads();
+  // Loads.  The B digits and column scales (prepared once per factor) come
+  // in one bulk copy; the FP64 slab tile comes in two halves of 64 rows of A
+  // by TMA when the job has a tensor map (right update: box 66 x k at the
+  // tile's first row rounded down to even; left update: box kbox x 64 at
+  // row r0 rounded down to even), else by plain loads.  Each half is sliced
+  // into the INT8 digit planes of A; thread t takes row (t & 63) of the half
+  // and every other K chunk.
+  const bool tma = J.map >= 0;
+  const CUtensorMap* map = tma ? &B.maps[J.map] : nullptr;
+  const int kbox = oz_left_box(k);
+  const uint32_t box_bytes = (uint32_t)(J.left ? kbox * 64 : kOzBoxRows * k) * 8u;
+  bool lok = true;
+  uint32_t lphase = 0;
+  if (tid == 0) {
+    mbar_expect_tx(&lbar, (uint32_t)kOzFacBytes + (tma ? box_bytes : 0u));
+    bulk_g2s(Bs, Bg, (uint32_t)kOzFacBytes, &lbar);
   }
-  // A: two halves of 64 rows staged in FP64 (coalesced), then sliced;
-  // thread t takes row (t & 63) of the half and every other K chunk
   for (int h = 0; h < 2; ++h) {
     const int rb = 64 * h;
-    if (J.left) {
-      // A(i, kk) = M(r0 + kk, c0 + row0 + i): contiguous in kk
-      for (int idx = tid; idx < 64 * k; idx += kOzThreads) {
-        const int kk = idx % k, i = idx / k;
-        Xs[i * ldx + kk] = (rb + i < nrow) ? J.M[(J.r0 + kk) + (int64_t)(J.c0 + row0 + rb + i) * J.ld] : 0.0;
+    int off = 0;  // rows the box starts above the first wanted one
+    if (tma) {
+      const int xr = J.left ? J.r0 : J.r0 + row0 + rb;
+      off = xr & 1;
+      if (tid == 0) {
+        if (h == 1) {
+          fence_async_smem();  // the first half's reads of the staging buffer come first
+          mbar_expect_tx(&lbar, box_bytes);
+        }
+        if (J.left) tma_g2s_2d(Xs, map, xr - off, J.c0 + row0 + rb, &lbar);
+        else tma_g2s_2d(Xs, map, xr - off, J.c0, &lbar);
       }
+      lok = __syncthreads_and(mbar_wait(&lbar, lphase) ? 1 : 0) != 0;
+      lphase ^= 1u;
+      if (!lok) break;
     } else {
-      // A(i, kk) = M(r0 + row0 + i, c0 + kk): contiguous in i
-      for (int idx = tid; idx < 64 * k; idx += kOzThreads) {
-        const int i = idx % 64, kk = idx / 64;
-        Xs[i * ldx + kk] = (rb + i < nrow) ? J.M[(J.r0 + row0 + rb + i) + (int64_t)(J.c0 + kk) * J.ld] : 0.0;
+      if (h == 0) {
+        lok = __syncthreads_and(mbar_wait(&lbar, lphase) ? 1 : 0) != 0;  // B digits
+        lphase ^= 1u;
+        if (!lok) break;
       }
+      if (J.left) {
+        // A(i, kk) = M(r0 + kk, c0 + row0 + i): contiguous in kk
+        for (int idx = tid; idx < 64 * k; idx += kOzThreads) {
+          const int kk = idx % k, i = idx / k;
+          Xs[i * ldx + kk] = (rb + i < nrow) ? J.M[(J.r0 + kk) + (int64_t)(J.c0 + row0 + rb + i) * J.ld] : 0.0;
+        }
+      } else {
+        // A(i, kk) = M(r0 + row0 + i, c0 + kk): contiguous in i
+        for (int idx = tid; idx < 64 * k; idx += kOzThreads) {
+          const int i = idx % 64, kk = idx / 64;
+          Xs[i * ldx + kk] = (rb + i < nrow) ? J.M[(J.r0 + row0 + rb + i) + (int64_t)(J.c0 + kk) * J.ld] : 0.0;
+        }
+      }
+      __syncthreads();
     }
-    __syncthreads();
     {
       const int il = tid & 63, par = tid >> 6;
       const int i = rb + il;
+      // element (il, kk) of the half in the staging layout
+      auto xv = [&](int kk) -> double {
+        if (!tma) return Xs[il * ldx + kk];
+        if (J.left) return Xs[il * kbox + kk + off];
+        return Xs[kk * kOzBoxRows + il + off];
+      };
       double mx = 0.0;
-      for (int kk = 0; kk < k; ++kk) mx = fmax(mx, fabs(Xs[il * ldx + kk]));
+      if (rb + il < nrow)
+        for (int kk = 0; kk < k; ++kk) mx = fmax(mx, fabs(xv(kk)));
       int e = 0;
       if (mx > 0.0) frexp(mx, &e);
       if (par == 0) escale[i] = e;
@@ -256,16 +338,27 @@ __global__ void __launch_bounds__(kOzThreads, 1) k_ozaki_update(const OzBatch B)
 #pragma unroll
         for (int t = 0; t < 16; ++t) {
           const int kk = kc * 16 + t;
-          x[t] = (kk < k) ? sc(Xs[il * ldx + kk]) : 0.0;
+          x[t] = (kk < k && rb + il < nrow) ? sc(xv(kk)) : 0.0;
         }
         uint4 d[S];
         digits16<S>(x, d);
-        const size_t off = (size_t)(kc * (kOzRows / 8) + i / 8) * 128 + (i % 8) * 16;
+        const size_t o = (size_t)(kc * (kOzRows / 8) + i / 8) * 128 + (i % 8) * 16;
 #pragma unroll
-        for (int s = 0; s < S; ++s) *(uint4*)(As + (size_t)s * kOzRows * Kp + off) = d[s];
+        for (int s = 0; s < S; ++s) *(uint4*)(As + (size_t)s * kOzRows * Kp + o) = d[s];
       }
     }
+    __syncthreads();  // the staging buffer is reused by the next half
+  }
+  if (!lok) {
+    // a load did not complete in time: nothing was computed; report it, and
+    // give the copy in flight one more bounded wait before the CTA (and its
+    // shared memory) goes away
+    if (tid == 0) atomicExch(B.err, 1);
+    (void)mbar_wait(&lbar, lphase ^ 1u);
     __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base_s),
+                                "r"(kOzTmemCols));
+    return;
   }
   fence_async_smem();
   tc_fence_before();
@@ -381,6 +474,33 @@ __global__ void __launch_bounds__(kOzThreads, 1) k_ozaki_update(const OzBatch B)
 }
 
 }  // namespace
+
+bool ozaki_tensor_map(CUtensorMap* map, const double* M, int64_t ld, int rows, int cols, int left, int k) {
+  using Encode = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                              const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                              CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+  static Encode encode = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      encode = (Encode)fn;
+  }
+  if (!encode || !M || rows < 1 || cols < 1 || k < 1 || k > kOzMaxK) return false;
+  // TMA: base 16-byte aligned, column stride a multiple of 16 bytes
+  if (((uintptr_t)M & 15u) != 0 || (ld * 8) % 16 != 0 || ld < rows) return false;
+  const cuuint64_t dims[2] = {(cuuint64_t)rows, (cuuint64_t)cols};
+  const cuuint64_t strides[1] = {(cuuint64_t)ld * 8u};
+  const cuuint32_t box[2] = {left ? (cuuint32_t)oz_left_box(k) : (cuuint32_t)kOzBoxRows,
+                             left ? 64u : (cuuint32_t)k};
+  const cuuint32_t estr[2] = {1, 1};
+  return encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, (void*)M, dims, strides, box, estr,
+                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
 
 size_t ozaki_smem_bytes(int slices) {
   return (size_t)slices * kOzRows * kOzMaxKp + kOzFacBytes + (size_t)kOzStageDoubles * sizeof(double);

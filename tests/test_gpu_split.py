@@ -33,9 +33,12 @@ def _split_update(pkg, side, M, r0, c0, length, W, slices):
 @pytest.mark.parametrize("slices,tol", [(7, 2.0 ** -44), (8, 2.0 ** -51)])
 @pytest.mark.parametrize("k", [1, 7, 16, 33, 64, 80])
 @pytest.mark.parametrize("side", ["L", "R"])
-def test_split_update_matches_fp64(pkg, k, side, slices, tol):
+@pytest.mark.parametrize("n", [400, 401])
+def test_split_update_matches_fp64(pkg, k, side, slices, tol, n):
+    """n = 400: the slab tile comes in by TMA (even leading dimension; the
+    odd row offset 37 exercises the box start rounded down to an even row);
+    n = 401: odd leading dimension, plain loads."""
     rng = np.random.default_rng(100 + k)
-    n = 400
     M = rng.standard_normal((n, n)) * 10.0 ** rng.uniform(-6, 6, size=(n, 1))
     M *= 10.0 ** rng.uniform(-3, 3, size=(1, n))
     W = np.linalg.qr(rng.standard_normal((k, k)))[0]
