@@ -106,6 +106,18 @@ QZ_HD bool seg_item(const Seg& a, const Seg& b, const Seg& c, int idx, double*& 
   if (idx < nc) { q = c.p + (int64_t)idx * c.step; st = c.stride; return true; }
   return false;
 }
+// Threads that apply the far parts of a step whose small block thread 0
+// transforms: with at least two warps, warp 0 is left to the block (its
+// lanes would otherwise wait for lane 0's serial block work), the others
+// take the far items; a lone warp does both.
+struct FarTeam {
+  int first, stride;
+};
+template <class X>
+QZ_HD FarTeam far_team(const X& x) {
+  return (x.nt >= 64) ? FarTeam{x.tid - 32, x.nt - 32} : FarTeam{x.tid, x.nt};
+}
+
 QZ_HD int seg_total(const Seg& a, const Seg& b, const Seg& c) {
   return (a.count > 0 ? a.count : 0) + (b.count > 0 ? b.count : 0) + (c.count > 0 ? c.count : 0);
 }
@@ -395,7 +407,9 @@ QZ_HD void cta_ds_sweep(X& x, WinState& w, int f, int l, double c2, double c1, d
         const Seg d = seg_cols(w.H, j, 0, j), e = seg_cols(w.T, j, 0, j);
         const Seg g = w.wantz ? seg_cols(w.Z, j, 0, n) : no_seg();
         const int n1 = seg_total(a, b, c), total = n1 + seg_total(d, e, g);
-        for (int idx = x.tid; idx < total; idx += x.nt) {
+        const FarTeam ft = far_team(x);
+        for (int idx = ft.first; idx < total; idx += ft.stride) {
+          if (idx < 0) break;
           double* q;
           int64_t st;
           const bool left = idx < n1;
@@ -441,7 +455,9 @@ QZ_HD void cta_ds_sweep(X& x, WinState& w, int f, int l, double c2, double c1, d
         const Seg d = seg_cols(w.H, j, 0, j), e = seg_cols(w.T, j, 0, j);
         const Seg g = w.wantz ? seg_cols(w.Z, j, 0, n) : no_seg();
         const int n1 = seg_total(a, b, cq), total = n1 + seg_total(d, e, g);
-        for (int idx = x.tid; idx < total; idx += x.nt) {
+        const FarTeam ft = far_team(x);
+        for (int idx = ft.first; idx < total; idx += ft.stride) {
+          if (idx < 0) break;
           double* q;
           int64_t st;
           const bool left = idx < n1;
@@ -619,7 +635,7 @@ QZ_HD void small_qr_q(double* X, double* Q) {
 // the swap's stability test, which then rejects the swap.
 template <int S, int K>
 struct SmallElim {
-  static QZ_HD void run(double* A, double* rhs, double smin, bool& exact) {
+  static QZ_HD void run(double* A, double* rhs, double* rpv, double smin, bool& exact) {
     if constexpr (K < S) {
       int pi = K;
       double best = fabs(A[K + S * K]);
@@ -643,6 +659,7 @@ struct SmallElim {
       }
       if (fabs(A[K + S * K]) < smin) { A[K + S * K] = smin; exact = false; }
       const double rpiv = 1.0 / A[K + S * K];
+      rpv[K] = rpiv;
 #pragma unroll
       for (int i = K + 1; i < S; ++i) {
         const double f = A[i + S * K] * rpiv;
@@ -650,20 +667,21 @@ struct SmallElim {
         for (int j = K + 1; j < S; ++j) A[i + S * j] -= f * A[K + S * j];
         rhs[i] -= f * rhs[K];
       }
-      SmallElim<S, K + 1>::run(A, rhs, smin, exact);
+      SmallElim<S, K + 1>::run(A, rhs, rpv, smin, exact);
     }
   }
 };
 template <int S>
 QZ_HD bool small_solve_cp(double* A, double* rhs, double smin) {
   bool exact = true;
-  SmallElim<S, 0>::run(A, rhs, smin, exact);
+  double rpv[S];  // reciprocal pivots, reused by the back substitution
+  SmallElim<S, 0>::run(A, rhs, rpv, smin, exact);
 #pragma unroll
   for (int k = S - 1; k >= 0; --k) {
     double acc = rhs[k];
 #pragma unroll
     for (int j = k + 1; j < S; ++j) acc -= A[k + S * j] * rhs[j];
-    rhs[k] = acc / A[k + S * k];
+    rhs[k] = acc * rpv[k];
   }
   return exact;
 }

@@ -459,7 +459,9 @@ QZ_HD void cta_aed(X& x, WinState& w, double s, double* sr, double* si_, double*
         const Seg z = w.wantz ? Seg{&w.Z(0, jr), 1, -(int64_t)w.Z.ld, n} : no_seg();
         const int n1 = seg_total(a, b, t), n2 = n1 + seg_total(q, no_seg(), no_seg());
         const int n3 = n2 + seg_total(d, e, g), total = n3 + seg_total(z, no_seg(), no_seg());
-        for (int idx = x.tid; idx < total; idx += x.nt) {
+        const FarTeam ft = far_team(x);
+        for (int idx = ft.first; idx < total; idx += ft.stride) {
+          if (idx < 0) break;
           double* p;
           int64_t st;
           bool row;
