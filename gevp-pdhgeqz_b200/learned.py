@@ -40,8 +40,10 @@ TRACES = os.path.join(POLICY_DIR, "traces.npz")
 
 NIN, NHID, NOUT = 64, 128, 2
 NW_MIN, NW_SPAN, NW_MAX = 16, 64, 80
-GRID_NW = (24, 40, 56, 80)
+TABLE_NW = 48  # the solver's fixed AED window (SolveParams::nw_max)
+GRID_NW = (24, 32, 40, 48, 56, 64, 80)
 GRID_NSF = (0.5, 1.0)
+DECISIONS = (0, 5, 20, 60, 150)  # AED indices at which a trace samples the choice
 AED_FLOP_FACTOR = 10.0  # window QZ + reordering cost per AED, in units of nw^3
 
 
@@ -152,7 +154,7 @@ def encode(nw: int, nsf: float):
     return np.array([(nw - NW_MIN) / NW_SPAN, nsf], dtype=np.float32)
 
 
-def table_choice(nh: int):
+def table_choice(nh: int, table_nw: int = TABLE_NW):
     """(nw, ns/nw) the fixed table gives (nw_max and NS(NH), piparmq.f:504-533)."""
     ns = 2
     if nh >= 30:
@@ -166,13 +168,13 @@ def table_choice(nh: int):
     if nh >= 3000:
         ns = 128
     ns = max(2, ns - ns % 2)
-    nw = min(NW_MAX, nh)
+    nw = min(table_nw, nh)
     return nw, min(1.0, ns / nw)
 
 
-def nearest_candidate(nw, nsf):
-    i = int(np.argmin([abs(nw - g) for g in GRID_NW]))
-    j = int(np.argmin([abs(nsf - g) for g in GRID_NSF]))
+def nearest_candidate(nw, nsf, grid_nw=GRID_NW, grid_nsf=GRID_NSF):
+    i = int(np.argmin([abs(nw - g) for g in grid_nw]))
+    j = int(np.argmin([abs(nsf - g) for g in grid_nsf]))
     return i, j
 
 
@@ -226,7 +228,7 @@ def _set(solver, nw_max, ns_max, aed_limit):
     solver.set_param("aed_limit", aed_limit)
 
 
-def trace_pencil(solver, H, T, decisions=(0, 3), horizon=3):
+def trace_pencil(solver, H, T, decisions=DECISIONS, horizon=3):
     """Samples (features, scores_per_second, scores_per_flop, nh) of one
     pencil at the given AED decision points; scores are arrays
     [len(GRID_NW), len(GRID_NSF)]."""
@@ -242,7 +244,7 @@ def trace_pencil(solver, H, T, decisions=(0, 3), horizon=3):
     for j in decisions:
         bufs[0].copy_(dH0)
         bufs[1].copy_(dT0)
-        _set(solver, NW_MAX, 0, j)
+        _set(solver, TABLE_NW, 0, j)
         info = _solve(solver, bufs, n)
         st = solver.stats()
         if info != 10003:
@@ -256,7 +258,7 @@ def trace_pencil(solver, H, T, decisions=(0, 3), horizon=3):
         # cost of restarting from the snapshot alone (scans down to kbot)
         bufs[0].copy_(snapH)
         bufs[1].copy_(snapT)
-        _set(solver, NW_MAX, 0, 0)
+        _set(solver, TABLE_NW, 0, 0)
         _solve(solver, bufs, n)
         t0 = solver.stats()["seconds"]
         s_time = np.zeros((len(GRID_NW), len(GRID_NSF)))
@@ -276,41 +278,51 @@ def trace_pencil(solver, H, T, decisions=(0, 3), horizon=3):
                 s_flop[a, b] = defl / max(cost, 1.0)
                 s_time[a, b] = defl / max(st["seconds"] - t0, 1e-6)
         out.append((feat, s_time, s_flop, kbot - ktop + 1))
-    _set(solver, NW_MAX, 0, -1)
+    _set(solver, TABLE_NW, 0, -1)
     return out
 
 
-def labels_from_scores(scores):
+def labels_from_scores(scores, grid_nw=GRID_NW, grid_nsf=GRID_NSF):
     """Best candidate of each sample as the regression target."""
     T = []
     for sc in scores:
         a, b = np.unravel_index(int(np.argmax(sc)), sc.shape)
-        T.append(encode(GRID_NW[a], GRID_NSF[b]))
+        T.append(encode(grid_nw[a], grid_nsf[b]))
     return np.stack(T)
 
 
-def score_of_choice(score, nw, nsf):
-    i, j = nearest_candidate(nw, nsf)
+def score_of_choice(score, nw, nsf, grid_nw=GRID_NW, grid_nsf=GRID_NSF):
+    i, j = nearest_candidate(nw, nsf, grid_nw, grid_nsf)
     return float(score[i, j])
 
 
-def offline_gain(P, X, scores, nh):
+def trace_grid(tr):
+    """(grid_nw, grid_nsf, table_nw) a trace file was recorded with (files
+    without them predate the current grid)."""
+    if "grid_nw" in tr:
+        return tuple(int(v) for v in tr["grid_nw"]), tuple(float(v) for v in tr["grid_nsf"]), int(tr["table_nw"])
+    return (24, 40, 56, 80), (0.5, 1.0), 80
+
+
+def offline_gain(P, X, scores, nh, grid=None):
     """Geometric mean over samples of score(network's choice) /
     score(table's choice), both taken at the nearest grid candidate (ratios
-    floored at 1e-3 so that a zero score counts as a large loss, not -inf)."""
+    floored at 1e-3 so that a zero score counts as a large loss, not -inf).
+    grid: (grid_nw, grid_nsf, table_nw) of the traces (trace_grid)."""
+    gnw, gnsf, tnw_fixed = grid if grid is not None else (GRID_NW, GRID_NSF, TABLE_NW)
     _, _, Y = forward_np(P, X)
     logs = []
     for y, sc, h in zip(Y, scores, nh):
         nw, ns = decode(y, int(h))
-        tnw, tnsf = table_choice(int(h))
-        s_net = score_of_choice(sc, nw, ns / max(nw, 1))
-        s_tab = score_of_choice(sc, tnw, tnsf)
+        tnw, tnsf = table_choice(int(h), tnw_fixed)
+        s_net = score_of_choice(sc, nw, ns / max(nw, 1), gnw, gnsf)
+        s_tab = score_of_choice(sc, tnw, tnsf, gnw, gnsf)
         if s_tab > 0:
             logs.append(np.log(max(s_net / s_tab, 1e-3)))
     return float(np.exp(np.mean(logs))) if logs else 1.0
 
 
-def generate_traces(count=200, decisions=(0, 3), device=0, log=None):
+def generate_traces(count=200, decisions=DECISIONS, device=0, log=None):
     """Trace all training pencils on the GPU.  Returns dict of arrays."""
     import torch
     pkg = _pkg()
@@ -331,4 +343,6 @@ def generate_traces(count=200, decisions=(0, 3), device=0, log=None):
     finally:
         solver.close()
     return {"features": np.stack(feats).astype(np.float32), "scores": np.stack(scores),
-            "scores_per_flop": np.stack(sflop), "nh": np.array(nhs), "pencil": np.array(ids)}
+            "scores_per_flop": np.stack(sflop), "nh": np.array(nhs), "pencil": np.array(ids),
+            "grid_nw": np.array(GRID_NW), "grid_nsf": np.array(GRID_NSF), "table_nw": TABLE_NW,
+            "decisions": np.array(decisions)}

@@ -39,6 +39,9 @@ def _pkg():
     return mod
 
 
+DECISIONS_DEFAULT = (0, 5, 20, 60, 150)
+
+
 def cmd_traces(a):
     pkg = _pkg()
     t0 = time.time()
@@ -53,7 +56,8 @@ def cmd_train(a):
     lrn = pkg.learned
     tr = np.load(a.traces)
     X, scores, nh, pid = tr["features"], tr["scores"], tr["nh"], tr["pencil"]
-    T = lrn.labels_from_scores(scores)
+    grid = lrn.trace_grid(tr)
+    T = lrn.labels_from_scores(scores, grid[0], grid[1])
     hold = pid % 5 == 0
     P0 = lrn.init_params(a.seed)
     t0 = time.time()
@@ -62,8 +66,8 @@ def cmd_train(a):
     res = {"samples_train": int((~hold).sum()), "samples_holdout": int(hold.sum()), "mse_train": mse,
            "label": "argmax deflations per device second",
            "mse_holdout": lrn.loss_np(P, X[hold], T[hold]), "train_seconds": dt,
-           "gain_train": lrn.offline_gain(P, X[~hold], scores[~hold], nh[~hold]),
-           "gain_holdout": lrn.offline_gain(P, X[hold], scores[hold], nh[hold])}
+           "gain_train": lrn.offline_gain(P, X[~hold], scores[~hold], nh[~hold], grid),
+           "gain_holdout": lrn.offline_gain(P, X[hold], scores[hold], nh[hold], grid)}
     os.makedirs(a.out, exist_ok=True)
     np.savez_compressed(os.path.join(a.out, "weights.npz"), params=P, epochs=a.epochs, lr=a.lr, seed=a.seed)
     print(json.dumps(res), flush=True)
@@ -112,7 +116,7 @@ def main():
     p = sub.add_parser("traces")
     p.add_argument("--out", required=True)
     p.add_argument("--count", type=int, default=200)
-    p.add_argument("--decisions", type=int, nargs="+", default=[0, 3])
+    p.add_argument("--decisions", type=int, nargs="+", default=list(DECISIONS_DEFAULT))
     p = sub.add_parser("train")
     p.add_argument("--traces", required=True)
     p.add_argument("--out", required=True)

@@ -29,7 +29,8 @@ def test_decode_and_table(pkg):
     assert lrn.decode([1.0, 1.0], 10000) == (80, 80)
     assert lrn.decode([2.0, 0.5], 50) == (50, 40)
     assert lrn.decode([0.5, 0.5], 10000) == (48, 24)
-    assert lrn.table_choice(10000) == (80, 1.0)
+    assert lrn.table_choice(10000) == (48, 1.0)
+    assert lrn.table_choice(10000, 80) == (80, 1.0)
     assert lrn.nparams() == 25090
 
 
@@ -43,9 +44,10 @@ def test_learned_policy_gains_offline(pkg):
     if P is None:
         pytest.skip("no trained weights committed")
     tr = np.load(lrn.TRACES)
+    grid = lrn.trace_grid(tr)
     hold = tr["pencil"] % 5 == 0
-    g_train = lrn.offline_gain(P, tr["features"][~hold], tr["scores"][~hold], tr["nh"][~hold])
-    g_hold = lrn.offline_gain(P, tr["features"][hold], tr["scores"][hold], tr["nh"][hold])
+    g_train = lrn.offline_gain(P, tr["features"][~hold], tr["scores"][~hold], tr["nh"][~hold], grid)
+    g_hold = lrn.offline_gain(P, tr["features"][hold], tr["scores"][hold], tr["nh"][hold], grid)
     print("offline gain over the table: train %.3f, held-out %.3f" % (g_train, g_hold))
     assert g_train > 1.0, g_train
     assert g_hold >= 0.95, g_hold
