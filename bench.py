@@ -341,7 +341,7 @@ def roofline_of(pst, phases, peaks, peak_kind, fp64_peak, split):
                 "frac": ach / peaks["hbm_gbs"], "traffic": None, "launches": int(launches),
                 "avg_launch_ms": dur * 1e3, "bytes_per_launch": byts / max(launches, 1.0),
                 "peak_source": "%s HBM copy bandwidth (of %s)" % (peak_kind, peak_kind),
-                "traffic_note": "ncu DRAM bytes per launch: profiles/ncu_%s.md" % kname}
+                "traffic_note": "ncu DRAM bytes per launch: profiles/ncu_%s_c1_n2000.md" % kname}
     elif dom in ("aed_update", "chase_update"):
         roof = {"kernel": upd["kernel"], "bound": "tensor", "achieved": upd["achieved_tflops"],
                 "peak": fp64_peak, "unit": "TFLOP/s", "frac": upd["frac"], "traffic": None,
