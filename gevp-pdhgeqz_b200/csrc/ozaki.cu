@@ -44,7 +44,8 @@ namespace qz {
 
 namespace {
 
-constexpr int kOzThreads = 128;
+constexpr int kOzThreads = 256;     // k_ozaki_update: 8 warps (two per TMEM lane quarter)
+constexpr int kOzPrepThreads = 128;
 constexpr int kOzRows = 128;  // MMA M
 constexpr int kOzChunkN = 64; // output columns per MMA pass (one TMEM accumulator each)
 constexpr int kOzOutN = 32;   // output columns per staged write-back
@@ -131,9 +132,16 @@ struct DigitScale {
   __device__ double operator()(double a) const { return fast ? a * m : ldexp(a, sh); }
 };
 
+// v * 2^e: one multiplication by the power of two built from its exponent
+// bits while 2^e is a normal number, ldexp otherwise
+__device__ __forceinline__ double scale_pow2(double v, int e) {
+  if (e >= -1022 && e <= 1023) return v * __longlong_as_double((long long)(e + 1023) << 52);
+  return ldexp(v, e);
+}
+
 // ---------------------------------------------------------------------------
 template <int S>
-__global__ void __launch_bounds__(kOzThreads) k_ozaki_prep(OzPrep P) {
+__global__ void __launch_bounds__(kOzPrepThreads) k_ozaki_prep(OzPrep P) {
   const int f = blockIdx.x;
   const double* W = P.W[f];
   const int ldw = P.ldw[f];
@@ -318,7 +326,7 @@ __global__ void __launch_bounds__(kOzThreads, 1) k_ozaki_update(const __grid_con
       __syncthreads();
     }
     {
-      const int il = tid & 63, par = tid >> 6;
+      const int il = tid & 63, par = tid >> 6;  // par: 0 .. kOzThreads/64 - 1
       const int i = rb + il;
       // element (il, kk) of the half in the staging layout
       auto xv = [&](int kk) -> double {
@@ -333,7 +341,7 @@ __global__ void __launch_bounds__(kOzThreads, 1) k_ozaki_update(const __grid_con
       if (mx > 0.0) frexp(mx, &e);
       if (par == 0) escale[i] = e;
       const DigitScale sc(S, e);
-      for (int kc = par; kc < kc_n; kc += 2) {
+      for (int kc = par; kc < kc_n; kc += kOzThreads / 64) {
         double x[16];
 #pragma unroll
         for (int t = 0; t < 16; ++t) {
@@ -429,9 +437,12 @@ __global__ void __launch_bounds__(kOzThreads, 1) k_ozaki_update(const __grid_con
     for (int p0 = 0; p0 < nn; p0 += kOzOutN) {
       const int pn = min(kOzOutN, nn - p0);
       if (ok) {
-        const int i = warp * 32 + lane;
-        const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
-        for (int g = 0; g < pn / 8; ++g) {
+        // a warp reads the TMEM lanes of its quarter (warp % 4); the two
+        // warps of a quarter take alternate 8-column groups
+        const int wq = warp & 3, half = warp >> 2;
+        const int i = wq * 32 + lane;
+        const uint32_t lane_addr = tmem + ((uint32_t)(wq * 32) << 16);
+        for (int g = half; g < pn / 8; g += kOzThreads / 128) {
           int32_t v[S][8];
 #pragma unroll
           for (int d = 0; d < S; ++d) tmem_ld8(lane_addr + (uint32_t)(d * kOzChunkN + p0 + 8 * g), v[d]);
@@ -442,7 +453,7 @@ __global__ void __launch_bounds__(kOzThreads, 1) k_ozaki_update(const __grid_con
 #pragma unroll
             for (int d = S - 2; d >= 0; --d) val = fma(val, 0.0078125, (double)v[d][e]);
             const int j = n0 + p0 + 8 * g + e;
-            Xs[i * ldo + 8 * g + e] = (j < k) ? ldexp(val, escale[i] + fscale[j] - 12) : 0.0;
+            Xs[i * ldo + 8 * g + e] = (j < k) ? scale_pow2(val, escale[i] + fscale[j] - 12) : 0.0;
           }
         }
       }
@@ -516,8 +527,8 @@ cudaError_t ozaki_init() {
 
 void launch_ozaki_prep(cudaStream_t st, const OzPrep& P, int slices) {
   if (P.nfac <= 0) return;
-  if (slices == 8) k_ozaki_prep<8><<<P.nfac, kOzThreads, 0, st>>>(P);
-  else k_ozaki_prep<7><<<P.nfac, kOzThreads, 0, st>>>(P);
+  if (slices == 8) k_ozaki_prep<8><<<P.nfac, kOzPrepThreads, 0, st>>>(P);
+  else k_ozaki_prep<7><<<P.nfac, kOzPrepThreads, 0, st>>>(P);
 }
 
 void launch_ozaki_update(cudaStream_t st, const OzBatch& B, int slices) {

@@ -106,16 +106,26 @@ QZ_HD bool seg_item(const Seg& a, const Seg& b, const Seg& c, int idx, double*& 
   if (idx < nc) { q = c.p + (int64_t)idx * c.step; st = c.stride; return true; }
   return false;
 }
-// Threads that apply the far parts of a step whose small block thread 0
-// transforms: with at least two warps, warp 0 is left to the block (its
-// lanes would otherwise wait for lane 0's serial block work), the others
-// take the far items; a lone warp does both.
-struct FarTeam {
-  int first, stride;
-};
+// Steps that transform a small block on one thread and the far parts on all
+// threads use index ownership: thread t applies the step to every vector
+// indexed t (column t of the rows a left transformation touches, row t of
+// the columns a right one touches, row t of Q and Z), so each thread has a
+// few independent short chains and no per-item dispatch.  The small block
+// goes to the CTA's last thread, whose warp has no index work while the
+// window is at most nt - 32 wide.
 template <class X>
-QZ_HD FarTeam far_team(const X& x) {
-  return (x.nt >= 64) ? FarTeam{x.tid - 32, x.nt - 32} : FarTeam{x.tid, x.nt};
+QZ_HD bool block_thread(const X& x) {
+  return x.tid == x.nt - 1;
+}
+QZ_HD void house3_vec(const House3& h, double* q, int64_t st) {
+  double a0 = q[0], a1 = q[st], a2 = q[2 * st];
+  house3_apply(h, a0, a1, a2);
+  q[0] = a0; q[st] = a1; q[2 * st] = a2;
+}
+QZ_HD void rot_vec(double c, double s, double* q, int64_t st) {
+  const double u = q[0], v = q[st];
+  q[0] = c * u + s * v;
+  q[st] = -s * u + c * v;
 }
 
 QZ_HD int seg_total(const Seg& a, const Seg& b, const Seg& c) {
@@ -393,34 +403,30 @@ QZ_HD void cta_ds_sweep(X& x, WinState& w, int f, int l, double c2, double c1, d
       tb[1] = 0.0; tb[2] = 0.0;
       // rows of the block touched by PR: up to j+3 while j+3 <= l
       const int nr = (j + 3 <= l) ? 4 : 3;
+      const bool bt = block_thread(x);
       double hb[12];
-      if (x.tid == 0) {
+      if (bt) {
         for (int cc = 0; cc < 3; ++cc)
           for (int rr = 0; rr < 4; ++rr) hb[rr + 4 * cc] = (rr < nr) ? w.H(j + rr, j + cc) : 0.0;
         for (int cc = 0; cc < 3; ++cc) house3_apply(PL, hb[4 * cc], hb[4 * cc + 1], hb[4 * cc + 2]);
         for (int rr = 0; rr < 4; ++rr) house3_apply(PR, hb[rr], hb[rr + 4], hb[rr + 8]);
       }
       x.sync();  // everyone has read H(.,j-1), the T block and the block
-      {
-        const Seg a = seg_rows(w.H, j, j + 3, n), b = seg_rows(w.T, j, j + 3, n);
-        const Seg c = w.wantq ? seg_cols(w.Q, j, 0, n) : no_seg();
-        const Seg d = seg_cols(w.H, j, 0, j), e = seg_cols(w.T, j, 0, j);
-        const Seg g = w.wantz ? seg_cols(w.Z, j, 0, n) : no_seg();
-        const int n1 = seg_total(a, b, c), total = n1 + seg_total(d, e, g);
-        const FarTeam ft = far_team(x);
-        for (int idx = ft.first; idx < total; idx += ft.stride) {
-          if (idx < 0) break;
-          double* q;
-          int64_t st;
-          const bool left = idx < n1;
-          if (left) seg_item(a, b, c, idx, q, st);
-          else seg_item(d, e, g, idx - n1, q, st);
-          double v0 = q[0], v1 = q[st], v2 = q[2 * st];
-          house3_apply(left ? PL : PR, v0, v1, v2);
-          q[0] = v0; q[st] = v1; q[2 * st] = v2;
+      // far parts, by index: H, T rows j..j+2 right of the block (PL), Q
+      // columns j..j+2 (PL), H, T columns j..j+2 above it (PR), Z columns
+      for (int t = x.tid; t < n; t += x.nt) {
+        if (t >= j + 3) {
+          house3_vec(PL, &w.H(j, t), 1);
+          house3_vec(PL, &w.T(j, t), 1);
         }
+        if (w.wantq) house3_vec(PL, &w.Q(t, j), w.Q.ld);
+        if (t < j) {
+          house3_vec(PR, &w.H(t, j), w.H.ld);
+          house3_vec(PR, &w.T(t, j), w.T.ld);
+        }
+        if (w.wantz) house3_vec(PR, &w.Z(t, j), w.Z.ld);
       }
-      if (x.tid == 0) {
+      if (bt) {
         for (int cc = 0; cc < 3; ++cc) {
           for (int rr = 0; rr < 3; ++rr) w.T(j + rr, j + cc) = tb[rr + 3 * cc];
           for (int rr = 0; rr < nr; ++rr) w.H(j + rr, j + cc) = hb[rr + 4 * cc];
@@ -441,7 +447,8 @@ QZ_HD void cta_ds_sweep(X& x, WinState& w, int f, int l, double c2, double c1, d
       rot2(cr, sr, t10, t11);
       t10 = 0.0;
       double hb[4];
-      if (x.tid == 0) {
+      const bool bt = block_thread(x);
+      if (bt) {
         hb[0] = w.H(j, j); hb[1] = w.H(j + 1, j); hb[2] = w.H(j, j + 1); hb[3] = w.H(j + 1, j + 1);
         rot2(c, s, hb[0], hb[1]);
         rot2(c, s, hb[2], hb[3]);
@@ -449,27 +456,21 @@ QZ_HD void cta_ds_sweep(X& x, WinState& w, int f, int l, double c2, double c1, d
         rot2(cr, sr, hb[1], hb[3]);
       }
       x.sync();
-      {
-        const Seg a = seg_rows(w.H, j, j + 2, n), b = seg_rows(w.T, j, j + 2, n);
-        const Seg cq = w.wantq ? seg_cols(w.Q, j, 0, n) : no_seg();
-        const Seg d = seg_cols(w.H, j, 0, j), e = seg_cols(w.T, j, 0, j);
-        const Seg g = w.wantz ? seg_cols(w.Z, j, 0, n) : no_seg();
-        const int n1 = seg_total(a, b, cq), total = n1 + seg_total(d, e, g);
-        const FarTeam ft = far_team(x);
-        for (int idx = ft.first; idx < total; idx += ft.stride) {
-          if (idx < 0) break;
-          double* q;
-          int64_t st;
-          const bool left = idx < n1;
-          if (left) seg_item(a, b, cq, idx, q, st);
-          else seg_item(d, e, g, idx - n1, q, st);
-          const double u = q[0], v = q[st];
-          const double cc = left ? c : cr, ss = left ? s : sr;
-          q[0] = cc * u + ss * v;
-          q[st] = -ss * u + cc * v;
+      // far parts by index: H, T rows j, j+1 right of the block, Q columns
+      // (row rotation); H, T columns j, j+1 above it, Z columns (column one)
+      for (int t = x.tid; t < n; t += x.nt) {
+        if (t >= j + 2) {
+          rot_vec(c, s, &w.H(j, t), 1);
+          rot_vec(c, s, &w.T(j, t), 1);
         }
+        if (w.wantq) rot_vec(c, s, &w.Q(t, j), w.Q.ld);
+        if (t < j) {
+          rot_vec(cr, sr, &w.H(t, j), w.H.ld);
+          rot_vec(cr, sr, &w.T(t, j), w.T.ld);
+        }
+        if (w.wantz) rot_vec(cr, sr, &w.Z(t, j), w.Z.ld);
       }
-      if (x.tid == 0) {
+      if (bt) {
         w.T(j, j) = t00; w.T(j + 1, j) = 0.0; w.T(j, j + 1) = t01; w.T(j + 1, j + 1) = t11;
         w.H(j, j) = hb[0]; w.H(j + 1, j) = hb[1]; w.H(j, j + 1) = hb[2]; w.H(j + 1, j + 1) = hb[3];
         w.H(j, j - 1) = r; w.H(j + 1, j - 1) = 0.0;

@@ -417,9 +417,9 @@ QZ_HD void cta_aed(X& x, WinState& w, double s, double* sr, double* si_, double*
   //      by Givens rotations (the job of DGGHRD at qzearly.f:449).  Each
   //      pair (row rotation zeroing H(jr, jc), column rotation removing the
   //      T(jr, jr-1) it creates) is computed by every thread from the 2x2
-  //      block of T; thread 0 transforms the 2x2 blocks of H and T that both
-  //      rotations touch, everyone else the disjoint rest: two barriers per
-  //      pair ----
+  //      block of T; the block thread transforms the 2x2 blocks of H and T
+  //      that both rotations touch, every thread its indices of the disjoint
+  //      rest: two barriers per pair ----
   for (int jc = 0; jc < m - 2; ++jc) {
     for (int jr = m - 1; jr >= jc + 2; --jr) {
       x.count(2);
@@ -431,7 +431,8 @@ QZ_HD void cta_aed(X& x, WinState& w, double s, double* sr, double* si_, double*
       double cz, sz, rz;
       lartg(u11, u10, cz, sz, rz);  // pair (col jr, col jr-1): zero T(jr, jr-1)
       double hb[4], tb2[2];
-      if (x.tid == 0) {
+      const bool bt = block_thread(x);
+      if (bt) {
         // H(jr-1..jr, jr-1..jr): row rotation, then column rotation
         double h00 = w.H(jr - 1, jr - 1), h10 = w.H(jr, jr - 1), h01 = w.H(jr - 1, jr), h11 = w.H(jr, jr);
         rot2(c, sn, h00, h10);
@@ -445,37 +446,19 @@ QZ_HD void cta_aed(X& x, WinState& w, double s, double* sr, double* si_, double*
         tb2[0] = u00; tb2[1] = u01;
       }
       x.sync();
-      {
-        // row rotation: H rows jr-1, jr, columns jc+1..jr-2 and jr+1..n-1;
-        // T rows jr-1, jr, columns jr+1..n-1; Q columns jr-1, jr
-        const Seg a = seg_rows(w.H, jr - 1, jc + 1, jr - 1), b = seg_rows(w.H, jr - 1, jr + 1, n);
-        const Seg t = seg_rows(w.T, jr - 1, jr + 1, n);
-        const Seg q = w.wantq ? seg_cols(w.Q, jr - 1, 0, n) : no_seg();
-        // column rotation (col jr, col jr-1): H rows 0..jr-2 and jr+1..m-1;
-        // T rows 0..jr-2; Z columns
-        const Seg d = Seg{&w.H(0, jr), 1, -(int64_t)w.H.ld, jr - 1};
-        const Seg e = Seg{&w.H(jr + 1, jr), 1, -(int64_t)w.H.ld, m - jr - 1};
-        const Seg g = Seg{&w.T(0, jr), 1, -(int64_t)w.T.ld, jr - 1};
-        const Seg z = w.wantz ? Seg{&w.Z(0, jr), 1, -(int64_t)w.Z.ld, n} : no_seg();
-        const int n1 = seg_total(a, b, t), n2 = n1 + seg_total(q, no_seg(), no_seg());
-        const int n3 = n2 + seg_total(d, e, g), total = n3 + seg_total(z, no_seg(), no_seg());
-        const FarTeam ft = far_team(x);
-        for (int idx = ft.first; idx < total; idx += ft.stride) {
-          if (idx < 0) break;
-          double* p;
-          int64_t st;
-          bool row;
-          if (idx < n1) { seg_item(a, b, t, idx, p, st); row = true; }
-          else if (idx < n2) { seg_item(q, no_seg(), no_seg(), idx - n1, p, st); row = true; }
-          else if (idx < n3) { seg_item(d, e, g, idx - n2, p, st); row = false; }
-          else { seg_item(z, no_seg(), no_seg(), idx - n3, p, st); row = false; }
-          const double u = p[0], v = p[st];
-          const double cc = row ? c : cz, ss = row ? sn : sz;
-          p[0] = cc * u + ss * v;
-          p[st] = -ss * u + cc * v;
-        }
+      // far parts by index.  Row rotation: H rows jr-1, jr at columns
+      // jc+1..jr-2 and jr+1..n-1, T rows jr-1, jr at columns jr+1..n-1, Q
+      // columns jr-1, jr.  Column rotation (col jr, col jr-1): H rows 0..jr-2
+      // and jr+1..m-1, T rows 0..jr-2, Z columns.
+      for (int t = x.tid; t < n; t += x.nt) {
+        if ((t >= jc + 1 && t <= jr - 2) || t >= jr + 1) rot_vec(c, sn, &w.H(jr - 1, t), 1);
+        if (t >= jr + 1) rot_vec(c, sn, &w.T(jr - 1, t), 1);
+        if (w.wantq) rot_vec(c, sn, &w.Q(t, jr - 1), w.Q.ld);
+        if (t <= jr - 2 || (t >= jr + 1 && t < m)) rot_vec(cz, sz, &w.H(t, jr), -(int64_t)w.H.ld);
+        if (t <= jr - 2) rot_vec(cz, sz, &w.T(t, jr), -(int64_t)w.T.ld);
+        if (w.wantz) rot_vec(cz, sz, &w.Z(t, jr), -(int64_t)w.Z.ld);
       }
-      if (x.tid == 0) {
+      if (bt) {
         w.H(jr - 1, jc) = r; w.H(jr, jc) = 0.0;
         w.H(jr - 1, jr - 1) = hb[0]; w.H(jr, jr - 1) = hb[1]; w.H(jr - 1, jr) = hb[2]; w.H(jr, jr) = hb[3];
         w.T(jr - 1, jr - 1) = tb2[0]; w.T(jr - 1, jr) = tb2[1];
