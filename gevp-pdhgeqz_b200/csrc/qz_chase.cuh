@@ -123,103 +123,56 @@ QZ_HD void cta_chase_window(X& x, int wk, int last, MatV H, MatV T, MatV U, MatV
       if (r.kind == 1) H(j + 2, j - 1) = 0.0;
     }
     // Items of different bulges, and different items of one bulge, touch
-    // disjoint entries.  A warp takes one bulge at a time (reflector in
-    // registers) and its lanes walk the bulge's items: H columns j..wk-1,
-    // T columns past the T block, U rows 0..wk-1; two items per lane per
-    // round so their loads overlap.
-    const int lanes = x.nt < 32 ? x.nt : 32;
-    const int lane = x.tid % lanes;
-    const int nwarp = x.nt / lanes;
-    const int wid = x.tid / lanes;
-    for (int b = wid; b < nb; b += nwarp) {
-      const BulgeRec& r = rec[b];
-      if (r.kind == 0) continue;
-      const int j = r.j;
-      const int t0 = (r.kind == 1) ? j + 3 : j + 2;
-      const int nh = wk - j;
-      const int ntt = (wk - t0 > 0) ? wk - t0 : 0;
-      const int tot = nh + ntt + wk;
-      const House3 L = r.L;
-      const int kind = r.kind;
-      for (int l0 = lane; l0 < tot; l0 += 2 * lanes) {
-        double* p[2];
-        int st[2];
-#pragma unroll
-        for (int q = 0; q < 2; ++q) {
-          const int loc = l0 + q * lanes;
-          p[q] = nullptr;
-          st[q] = 1;
-          if (loc < nh) p[q] = &H(j, j + loc);
-          else if (loc < nh + ntt) p[q] = &T(j, t0 + (loc - nh));
-          else if (loc < tot) { p[q] = &U(loc - nh - ntt, j); st[q] = U.ld; }
+    // disjoint entries.  Index ownership: thread tid takes index t = tid %
+    // wk of bulges b = tid / wk, tid / wk + nt / wk, ...: column t of the
+    // bulge's three H rows (t >= j) and T rows (t past the T block), row t
+    // of U; a reflector kept in registers per bulge, no per-item dispatch.
+    const int tix = (x.nt >= wk) ? x.tid % wk : x.tid;
+    const int bix = (x.nt >= wk) ? x.tid / wk : 0;
+    const int bstep = (x.nt >= wk) ? x.nt / wk : 1;
+    const int tstep = (x.nt >= wk) ? wk : x.nt;  // threads per bulge index set
+    const bool active = bix < bstep;             // the last partial group idles
+    if (active)
+      for (int b = bix; b < nb; b += bstep) {
+        const BulgeRec& r = rec[b];
+        if (r.kind == 0) continue;
+        const int j = r.j;
+        const int t0 = (r.kind == 1) ? j + 3 : j + 2;
+        const House3 L = r.L;
+        for (int t = tix; t < wk; t += tstep) {
+          if (r.kind == 1) {
+            if (t >= j) house3_vec(L, &H(j, t), 1);
+            if (t >= t0) house3_vec(L, &T(j, t), 1);
+            house3_vec(L, &U(t, j), U.ld);
+          } else {
+            if (t >= j) rot_vec(L.s, L.u0, &H(j, t), 1);
+            if (t >= t0) rot_vec(L.s, L.u0, &T(j, t), 1);
+            rot_vec(L.s, L.u0, &U(t, j), U.ld);
+          }
         }
-        double a[2][3];
-#pragma unroll
-        for (int q = 0; q < 2; ++q)
-          if (p[q]) {
-            a[q][0] = p[q][0];
-            a[q][1] = p[q][st[q]];
-            a[q][2] = (kind == 1) ? p[q][2 * st[q]] : 0.0;
-          }
-#pragma unroll
-        for (int q = 0; q < 2; ++q)
-          if (p[q]) {
-            if (kind == 1) {
-              house3_apply(L, a[q][0], a[q][1], a[q][2]);
-              p[q][0] = a[q][0]; p[q][st[q]] = a[q][1]; p[q][2 * st[q]] = a[q][2];
-            } else {
-              const double c = L.s, sn = L.u0;
-              p[q][0] = c * a[q][0] + sn * a[q][1];
-              p[q][st[q]] = -sn * a[q][0] + c * a[q][1];
-            }
-          }
       }
-    }
     x.sync();
     // ---- phase C: right transformations: H columns j.. (rows 0..hr-1),
     // T columns j.. above the T block, V columns j.. (all rows) ----
-    for (int b = wid; b < nb; b += nwarp) {
-      const BulgeRec& r = rec[b];
-      if (r.kind == 0) continue;
-      const int j = r.j;
-      const int hr = (r.kind == 1) ? ((j + 4 < last + 1) ? j + 4 : last + 1) : last + 1;
-      const int tot = hr + j + wk;
-      const House3 R = r.R;
-      const int kind = r.kind;
-      for (int l0 = lane; l0 < tot; l0 += 2 * lanes) {
-        double* p[2];
-        int st[2];
-#pragma unroll
-        for (int q = 0; q < 2; ++q) {
-          const int loc = l0 + q * lanes;
-          p[q] = nullptr;
-          st[q] = H.ld;
-          if (loc < hr) p[q] = &H(loc, j);
-          else if (loc < hr + j) { p[q] = &T(loc - hr, j); st[q] = T.ld; }
-          else if (loc < tot) { p[q] = &V(loc - hr - j, j); st[q] = V.ld; }
+    if (active)
+      for (int b = bix; b < nb; b += bstep) {
+        const BulgeRec& r = rec[b];
+        if (r.kind == 0) continue;
+        const int j = r.j;
+        const int hr = (r.kind == 1) ? ((j + 4 < last + 1) ? j + 4 : last + 1) : last + 1;
+        const House3 R = r.R;
+        for (int t = tix; t < wk; t += tstep) {
+          if (r.kind == 1) {
+            if (t < hr) house3_vec(R, &H(t, j), H.ld);
+            if (t < j) house3_vec(R, &T(t, j), T.ld);
+            house3_vec(R, &V(t, j), V.ld);
+          } else {
+            if (t < hr) rot_vec(R.s, R.u0, &H(t, j), H.ld);
+            if (t < j) rot_vec(R.s, R.u0, &T(t, j), T.ld);
+            rot_vec(R.s, R.u0, &V(t, j), V.ld);
+          }
         }
-        double a[2][3];
-#pragma unroll
-        for (int q = 0; q < 2; ++q)
-          if (p[q]) {
-            a[q][0] = p[q][0];
-            a[q][1] = p[q][st[q]];
-            a[q][2] = (kind == 1) ? p[q][2 * st[q]] : 0.0;
-          }
-#pragma unroll
-        for (int q = 0; q < 2; ++q)
-          if (p[q]) {
-            if (kind == 1) {
-              house3_apply(R, a[q][0], a[q][1], a[q][2]);
-              p[q][0] = a[q][0]; p[q][st[q]] = a[q][1]; p[q][2 * st[q]] = a[q][2];
-            } else {
-              const double c = R.s, sn = R.u0;
-              p[q][0] = c * a[q][0] + sn * a[q][1];
-              p[q][st[q]] = -sn * a[q][0] + c * a[q][1];
-            }
-          }
       }
-    }
     // deferred stores owned by the bulge's thread
     for (int b = x.tid; b < nb; b += x.nt) {
       const BulgeRec& r = rec[b];
