@@ -29,6 +29,7 @@ struct DevExecT {
   int* si;
   double* sd;
   unsigned long long* ts = nullptr;  // phase timestamps (ns), thread 0 writes
+  PipeBuf* pipe = nullptr;            // pipelined double-shift sweeps (shared memory)
   __device__ void sync() {
     if constexpr (kWarp) __syncwarp();
     else __syncthreads();
@@ -85,10 +86,11 @@ __global__ void __launch_bounds__(kThreads) k_aed_win(double* H, double* T, int6
     Zs = Zw;
     sd = smem;
   }
-  // sd: 64 doubles of swap/spike scalars, 4n of spike vectors, then the
-  // multishift window QZ's scratch
-  int* si = (int*)(sd + 64 + 4 * n + kMsScratch);
+  // sd: 64 doubles of swap/spike scalars, 4n of spike vectors, the
+  // multishift window QZ's scratch, then the sweep pipeline's buffer
+  int* si = (int*)(sd + 64 + 4 * n + kMsScratch + kPipeDoubles);
   DevExecT<kThreads == 32> x{(int)threadIdx.x, kThreads, si, sd, ts};
+  if (kThreads >= 64) x.pipe = (PipeBuf*)(sd + 64 + 4 * n + kMsScratch);
   for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
     int i = idx % n, j = idx / n;
     Hs[i + j * lw] = G(H, ld, kwtop + i, kwtop + j);
@@ -394,7 +396,7 @@ __global__ void k_scale_pow2(double* A, int64_t ld, int n, int e) {
 // ---------------------------------------------------------------------------
 size_t aed_smem_bytes(int nw) {
   size_t d = (nw <= kWinSmemMax) ? (size_t)4 * nw * smem_ld(nw) : 0;
-  d += 64 + 4 * (size_t)nw + kMsScratch;
+  d += 64 + 4 * (size_t)nw + kMsScratch + kPipeDoubles;
   return d * sizeof(double) + kSi * sizeof(int);
 }
 size_t chase_smem_bytes(int wk) {

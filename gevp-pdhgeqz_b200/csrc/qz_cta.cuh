@@ -378,7 +378,7 @@ QZ_HD void cta_inf_chase_down(X& x, WinState& w, int f, int jz, int l) {
 // stores its block; the second barrier publishes the step.
 // ---------------------------------------------------------------------------
 template <class X>
-QZ_HD void cta_ds_sweep(X& x, WinState& w, int f, int l, double c2, double c1, double c0) {
+QZ_HD void cta_ds_sweep_sync(X& x, WinState& w, int f, int l, double c2, double c1, double c0) {
   int n = w.n;
   for (int j = f; j < l; ++j) {
     x.count(0);
@@ -480,6 +480,322 @@ QZ_HD void cta_ds_sweep(X& x, WinState& w, int f, int l, double c2, double c1, d
   }
 }
 
+// ---------------------------------------------------------------------------
+// Pipelined double-shift sweep: the same transformations as
+// cta_ds_sweep_sync, in the same order on every element, without barriers
+// between steps.
+//
+// The core (warp 0, every lane computing the same values) carries the bulge
+// in registers from step to step: the bulge column H(s..s+2, s-1), the T
+// block T(s..s+2, s..s+2), the H block H(s..s+3, s..s+2) and column s+3 of
+// both matrices (rows s..s+2), which the next block needs with PL_s
+// applied.  Per step it forms PL_s and PR_s, stores the block row that
+// leaves it (row s) and the new zeros, writes both reflectors to a ring in
+// shared memory and posts the step.  The far threads (threads 32..nt-1,
+// index t owned by far thread t mod nfar) apply the posted reflectors to
+// the rest, behind the core:
+//   PL_s  to H, T rows s..s+2 of columns t >= s+4 and to Q columns s..s+2,
+//   PR_s  to H, T columns s..s+2 of rows t < s and to Z columns s..s+2.
+// Ordering, all through release/acquire flags and one barrier of the far
+// threads per step:
+//   * core step s reads column s+3 after its owner applied PL_{s-1} (each
+//     far warp posts prog after the PL part of a step);
+//   * far step s reads block rows < s that the core stored before posting
+//     step s, and far columns that other far threads transformed in
+//     earlier PL parts (the far barrier at the end of every step);
+//   * a ring slot is rewritten after every far thread finished the step
+//     that used it (far_done).
+// The final 2x2 step of the sweep runs the same way with rotations.  Every
+// wait is bounded: on time-out a thread sets err and all threads leave the
+// sweep at the next wait (the far threads together, through a voting
+// barrier), and the sweep returns false.  An executor of one thread runs
+// core step s and then far step s, which meets every dependency in program
+// order and checks the split of the work on the host.
+// ---------------------------------------------------------------------------
+constexpr int kPipeSlots = 32;  // a power of two
+constexpr int kPipeMaxFarWarps = 8;
+struct PipeBuf {
+  double ring[kPipeSlots][8];  // step s: PL (s, u0, u1, u2; rotation c, s), then PR
+  int ready, far_done, err, pad;
+  int prog[kPipeMaxFarWarps];
+};
+constexpr int kPipeDoubles = (int)((sizeof(PipeBuf) + 7) / 8);
+
+QZ_HD int pipe_ld(const int* p) {
+#ifdef __CUDA_ARCH__
+  int v;
+  asm volatile("ld.acquire.cta.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+#else
+  return *(const volatile int*)p;
+#endif
+}
+QZ_HD void pipe_st(int* p, int v) {
+#ifdef __CUDA_ARCH__
+  asm volatile("st.release.cta.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+#else
+  *(volatile int*)p = v;
+#endif
+}
+constexpr int kPipeSpin = 1 << 22;  // polls before a wait gives up
+// wait for *p >= v; false once err is set or after kPipeSpin polls (then
+// this thread sets err)
+QZ_HD bool pipe_wait(PipeBuf* pb, const int* p, int v) {
+  for (int it = 0; it < kPipeSpin; ++it) {
+    if (pipe_ld(p) >= v) return true;
+    if ((it & 31) == 31 && pipe_ld(&pb->err) != 0) return false;
+  }
+  pipe_st(&pb->err, 1);
+  return false;
+}
+// barrier of the nfar far threads (named barrier 1) returning the OR of v
+QZ_HD bool far_vote(int nfar, bool v) {
+#ifdef __CUDA_ARCH__
+  int r;
+  asm volatile(
+      "{\n .reg .pred p, q;\n setp.ne.s32 p, %1, 0;\n bar.red.or.pred q, 1, %2, p;\n selp.s32 %0, 1, 0, q;\n}"
+      : "=r"(r)
+      : "r"((int)v), "r"(nfar)
+      : "memory");
+  return r != 0;
+#else
+  (void)nfar;
+  return v;
+#endif
+}
+QZ_HD void warp_bar() {
+#ifdef __CUDA_ARCH__
+  __syncwarp();
+#endif
+}
+
+// the core's registers and its two kinds of step
+struct DsCore {
+  int f, l, nfar;
+  double c2, c1, c0;
+  int64_t ld;
+  double* hd;  // &H(s, s)
+  double* td;  // &T(s, s)
+  int own;     // far thread that owns column s+3
+  double a0, a1, a2;  // H(s..s+2, s-1) (the shift column at s == f)
+  double tb[9];       // T(s..s+2, s..s+2), column-major
+  double hb[12];      // H(s..s+3, s..s+2), column-major, rows past l zero
+
+  QZ_HD void init(WinState& w) {
+    ld = w.H.ld;
+    hd = &w.H(f, f);
+    td = &w.T(f, f);
+    own = (f + 3) % nfar;
+    for (int cc = 0; cc < 3; ++cc)
+      for (int rr = 0; rr < 3; ++rr) tb[rr + 3 * cc] = td[rr + cc * ld];
+    const int nr = (f + 3 <= l) ? 4 : 3;
+    for (int cc = 0; cc < 3; ++cc)
+      for (int rr = 0; rr < 4; ++rr) hb[rr + 4 * cc] = (rr < nr) ? hd[rr + cc * ld] : 0.0;
+    a0 = a1 = a2 = 0.0;
+  }
+  QZ_HD double* slot_for(PipeBuf* pb, int s) const {
+    if (s - f >= kPipeSlots && !pipe_wait(pb, &pb->far_done, s - kPipeSlots + 1)) return nullptr;
+    return pb->ring[(s - f) & (kPipeSlots - 1)];
+  }
+
+  // 3x3 step at rows/cols s..s+2 (s <= l - 2)
+  QZ_HD bool step3(PipeBuf* pb, int n, int s) {
+    const int64_t l1 = ld, l2 = 2 * ld, l3 = 3 * ld;
+    // entries of the next block that no transformation touches before
+    // step s+1: T(s+3, s+3), H(s+3, s+3), H(s+4, s+3)
+    double nt33 = 0.0, nh33 = 0.0, nh43 = 0.0;
+    if (s + 1 <= l - 2) {
+      nt33 = td[3 + l3];
+      nh33 = hd[3 + l3];
+      if (s + 4 <= l) nh43 = hd[4 + l3];
+    }
+    if (s == f)
+      shift_column(hb[0], hb[1], hb[4], hb[5], hb[6], tb[0], tb[3], tb[4], c2, c1, c0, a0, a1, a2);
+    House3 PL, PR;
+    double beta;
+    house3(a0, a1, a2, PL, beta);
+    for (int cc = 0; cc < 3; ++cc) house3_apply(PL, tb[3 * cc], tb[3 * cc + 1], tb[3 * cc + 2]);
+    for (int cc = 0; cc < 3; ++cc) house3_apply(PL, hb[4 * cc], hb[4 * cc + 1], hb[4 * cc + 2]);
+    opposite_house3(tb, PR);
+    for (int rr = 0; rr < 3; ++rr) house3_apply(PR, tb[rr], tb[rr + 3], tb[rr + 6]);
+    tb[1] = 0.0; tb[2] = 0.0;
+    for (int rr = 0; rr < 4; ++rr) house3_apply(PR, hb[rr], hb[rr + 4], hb[rr + 8]);
+    double* slot = slot_for(pb, s);
+    if (!slot) return false;
+    slot[0] = PL.s; slot[1] = PL.u0; slot[2] = PL.u1; slot[3] = PL.u2;
+    slot[4] = PR.s; slot[5] = PR.u0; slot[6] = PR.u1; slot[7] = PR.u2;
+    // column s+3, rows s..s+2, once its owner has applied PL_{s-1}
+    const int c3 = s + 3;
+    double bh0 = 0.0, bh1 = 0.0, bh2 = 0.0, bt0 = 0.0, bt1 = 0.0, bt2 = 0.0;
+    if (c3 < n) {
+      if (s > f && !pipe_wait(pb, &pb->prog[own >> 5], s)) return false;
+      bh0 = hd[l3]; bh1 = hd[1 + l3]; bh2 = hd[2 + l3];
+      bt0 = td[l3]; bt1 = td[1 + l3]; bt2 = td[2 + l3];
+    }
+    house3_apply(PL, bh0, bh1, bh2);
+    house3_apply(PL, bt0, bt1, bt2);
+    // row s leaves the block; the bulge column becomes (beta, 0, 0)
+    td[0] = tb[0]; td[l1] = tb[3]; td[l2] = tb[6];
+    td[1] = 0.0; td[2] = 0.0;
+    hd[0] = hb[0]; hd[l1] = hb[4]; hd[l2] = hb[8];
+    if (s > f) { hd[-l1] = beta; hd[1 - l1] = 0.0; hd[2 - l1] = 0.0; }
+    if (c3 < n) {
+      hd[l3] = bh0; td[l3] = bt0;
+      if (s == l - 2) {  // the last 3x3 step: column l+1 is the rotation step's far part
+        hd[1 + l3] = bh1; hd[2 + l3] = bh2;
+        td[1 + l3] = bt1; td[2 + l3] = bt2;
+      }
+    }
+    pipe_st(&pb->ready, s + 1);
+    // the next step's block
+    a0 = hb[1]; a1 = hb[2]; a2 = hb[3];
+    const double t11 = tb[4], t21 = tb[5], t12 = tb[7], t22 = tb[8];
+    tb[0] = t11; tb[1] = t21; tb[2] = 0.0;
+    tb[3] = t12; tb[4] = t22; tb[5] = 0.0;
+    tb[6] = bt1; tb[7] = bt2; tb[8] = nt33;
+    const double h11 = hb[5], h21 = hb[6], h31 = hb[7], h12 = hb[9], h22 = hb[10], h32 = hb[11];
+    hb[0] = h11; hb[1] = h21; hb[2] = h31; hb[3] = 0.0;
+    hb[4] = h12; hb[5] = h22; hb[6] = h32; hb[7] = 0.0;
+    hb[8] = bh1; hb[9] = bh2; hb[10] = nh33; hb[11] = nh43;
+    hd += ld + 1;
+    td += ld + 1;
+    if (++own == nfar) own = 0;
+    return true;
+  }
+
+  // final 2x2 step at rows/cols l-1, l (the block carried from step l-2)
+  QZ_HD bool step2(PipeBuf* pb) {
+    const int j = l - 1;
+    const int64_t l1 = ld;
+    double c, sn, r;
+    lartg(a0, a1, c, sn, r);
+    double t00 = tb[0], t10 = tb[1], t01 = tb[3], t11 = tb[4];
+    rot2(c, sn, t00, t10);
+    rot2(c, sn, t01, t11);
+    double cr, sr;
+    opposite_rot2(t10, t11, cr, sr);
+    rot2(cr, sr, t00, t01);
+    rot2(cr, sr, t10, t11);
+    double h00 = hb[0], h10 = hb[1], h01 = hb[4], h11 = hb[5];
+    rot2(c, sn, h00, h10);
+    rot2(c, sn, h01, h11);
+    rot2(cr, sr, h00, h01);
+    rot2(cr, sr, h10, h11);
+    double* slot = slot_for(pb, j);
+    if (!slot) return false;
+    slot[0] = c; slot[1] = sn; slot[4] = cr; slot[5] = sr;
+    td[0] = t00; td[1] = 0.0; td[l1] = t01; td[1 + l1] = t11;
+    hd[0] = h00; hd[1] = h10; hd[l1] = h01; hd[1 + l1] = h11;
+    hd[-l1] = r; hd[1 - l1] = 0.0;
+    pipe_st(&pb->ready, j + 1);
+    return true;
+  }
+};
+
+// far step s of far thread fid (of nfar; lane and warp within the far
+// threads).  Returns false when the sweep is abandoned (same on every far
+// thread).
+QZ_HD bool ds_far_step(WinState& w, PipeBuf* pb, int f, int l, int s, int fid, int nfar, int lane, int warp) {
+  const int n = w.n;
+  const double* slot = pb->ring[(s - f) & (kPipeSlots - 1)];
+  const bool ok = pipe_wait(pb, &pb->ready, s + 1);
+  if (ok) {
+    if (s < l - 1) {
+      const House3 PL{slot[0], slot[1], slot[2], slot[3]};
+      for (int t = fid; t < n; t += nfar) {
+        if (t >= s + 4) {
+          house3_vec(PL, &w.H(s, t), 1);
+          house3_vec(PL, &w.T(s, t), 1);
+        }
+        if (w.wantq) house3_vec(PL, &w.Q(t, s), w.Q.ld);
+      }
+    } else {
+      const double c = slot[0], sn = slot[1];
+      for (int t = fid; t < n; t += nfar) {
+        if (t >= s + 2) {
+          rot_vec(c, sn, &w.H(s, t), 1);
+          rot_vec(c, sn, &w.T(s, t), 1);
+        }
+        if (w.wantq) rot_vec(c, sn, &w.Q(t, s), w.Q.ld);
+      }
+    }
+  }
+  warp_bar();
+  if (lane == 0) pipe_st(&pb->prog[warp], s + 1);
+  if (ok) {
+    if (s < l - 1) {
+      const House3 PR{slot[4], slot[5], slot[6], slot[7]};
+      for (int t = fid; t < n; t += nfar) {
+        if (t < s) {
+          house3_vec(PR, &w.H(t, s), w.H.ld);
+          house3_vec(PR, &w.T(t, s), w.T.ld);
+        }
+        if (w.wantz) house3_vec(PR, &w.Z(t, s), w.Z.ld);
+      }
+    } else {
+      const double cr = slot[4], sr = slot[5];
+      for (int t = fid; t < n; t += nfar) {
+        if (t < s) {
+          rot_vec(cr, sr, &w.H(t, s), w.H.ld);
+          rot_vec(cr, sr, &w.T(t, s), w.T.ld);
+        }
+        if (w.wantz) rot_vec(cr, sr, &w.Z(t, s), w.Z.ld);
+      }
+    }
+  }
+  const bool stop = far_vote(nfar, pipe_ld(&pb->err) != 0);
+  if (fid == 0) pipe_st(&pb->far_done, s + 1);
+  return !stop;
+}
+
+template <class X>
+QZ_HD bool cta_ds_sweep_pipe(X& x, PipeBuf* pb, WinState& w, int f, int l, double c2, double c1, double c0) {
+  if (x.tid == 0) {
+    pb->ready = f; pb->far_done = f; pb->err = 0;
+    for (int k = 0; k < kPipeMaxFarWarps; ++k) pb->prog[k] = f;
+  }
+  x.sync();
+  const int nfar = (x.nt == 1) ? 1 : x.nt - 32;
+  if (x.tid < 32) {
+    DsCore core{f, l, nfar, c2, c1, c0};
+    core.init(w);
+    for (int s = f; s < l; ++s) {
+      x.count(0);
+      const bool ok = (s < l - 1) ? core.step3(pb, w.n, s) : core.step2(pb);
+      if (!ok) break;
+      if (x.nt == 1 && !ds_far_step(w, pb, f, l, s, 0, 1, 0, 0)) break;
+    }
+  } else {
+    const int fid = x.tid - 32;
+    for (int s = f; s < l; ++s)
+      if (!ds_far_step(w, pb, f, l, s, fid, nfar, fid & 31, fid >> 5)) break;
+  }
+  x.sync();
+  return pb->err == 0;
+}
+
+// the executor's pipeline buffer, if it has one
+template <class X>
+QZ_HD auto pipe_of(X& x, int) -> decltype(x.pipe) {
+  return x.pipe;
+}
+template <class X>
+QZ_HD PipeBuf* pipe_of(X&, long) {
+  return nullptr;
+}
+
+// One double-shift sweep: pipelined when the executor provides a pipeline
+// buffer (one thread, or 64 or more threads in whole warps), otherwise with
+// two barriers per step.  False if a pipelined sweep gave up waiting.
+template <class X>
+QZ_HD bool cta_ds_sweep(X& x, WinState& w, int f, int l, double c2, double c1, double c0) {
+  PipeBuf* pb = pipe_of(x, 0);
+  if (pb && (x.nt == 1 || (x.nt >= 64 && x.nt % 32 == 0 && x.nt - 32 <= 32 * kPipeMaxFarWarps)))
+    return cta_ds_sweep_pipe(x, pb, w, f, l, c2, c1, c0);
+  cta_ds_sweep_sync(x, w, f, l, c2, c1, c0);
+  return true;
+}
+
 // negligible-subdiagonal test shared by all deflation scans
 QZ_HD bool negligible_sub(double hsub, double hkm1, double hkk, const Tol& t) {
   double tst = fabs(hkm1) + fabs(hkk);
@@ -552,7 +868,7 @@ QZ_HD int cta_small_qz(X& x, WinState& w, int maxit) {
       pencil2_poly(w.H(l - 1, l - 1), w.H(l, l - 1), w.H(l - 1, l), w.H(l, l),
                    w.T(l - 1, l - 1), w.T(l - 1, l), w.T(l, l), c2, c1, c0);
     }
-    cta_ds_sweep(x, w, ifirst, ilast, c2, c1, c0);
+    if (!cta_ds_sweep(x, w, ifirst, ilast, c2, c1, c0)) return ilast + 1;
   }
   return 0;
 }

@@ -173,7 +173,7 @@ QZ_HD int cta_small_qz_ms(X& x, WinState& w, int maxit, double* scr) {
       pencil2_poly(w.H(l - 1, l - 1), w.H(l, l - 1), w.H(l - 1, l), w.H(l, l),
                    w.T(l - 1, l - 1), w.T(l - 1, l), w.T(l, l), c2, c1, c0);
     }
-    cta_ds_sweep(x, w, ifirst, ilast, c2, c1, c0);
+    if (!cta_ds_sweep(x, w, ifirst, ilast, c2, c1, c0)) return ilast + 1;
   }
   return 0;
 }

@@ -28,12 +28,19 @@ namespace {
 static long g_barriers[6] = {0, 0, 0, 0, 0, 0};
 static int g_phase = 0;
 
+// Pipelined double-shift sweeps (core step, then far step, per step) when
+// set by host_set_pipe; the two-barrier form otherwise.
+static bool g_pipe = false;
+static PipeBuf g_pipebuf;
+
 struct HostExec {
   int tid = 0, nt = 1;
   int si[64];
   double* sd;
   std::vector<double> sdv;
+  PipeBuf* pipe = nullptr;
   HostExec() : sdv(16384, 0.0) { sd = sdv.data(); }
+  void use_pipe() { pipe = g_pipe ? &g_pipebuf : nullptr; }
   void sync() { ++g_barriers[g_phase]; }
   void stamp(int k) {
     g_phase = (k < 4) ? k + 1 : 0;
@@ -240,6 +247,10 @@ struct HostBK {
 
 extern "C" {
 
+void host_set_pipe(int on) { g_pipe = on != 0; }
+// steps of the last pipelined sweep that the far part completed (far_done)
+int host_pipe_far_done() { return g_pipebuf.far_done; }
+
 void host_barriers(long* out, int reset) {
   for (int i = 0; i < 6; ++i) out[i] = g_barriers[i];
   if (reset)
@@ -249,6 +260,7 @@ void host_barriers(long* out, int reset) {
 // Window QZ of an n x n pencil (Q, Z accumulate from their input).
 int host_small_qz(int n, double* H, double* T, double* Q, double* Z) {
   static HostExec x;
+  x.use_pipe();
   WinState w;
   w.n = n; w.H = MatV{H, n}; w.T = MatV{T, n}; w.Q = MatV{Q, n}; w.Z = MatV{Z, n};
   w.wantq = w.wantz = true;
@@ -259,6 +271,7 @@ int host_small_qz(int n, double* H, double* T, double* Q, double* Z) {
 // The same with the multishift window QZ (lockstep chains of bulges).
 int host_small_qz_ms(int n, double* H, double* T, double* Q, double* Z) {
   static HostExec x;
+  x.use_pipe();
   WinState w;
   w.n = n; w.H = MatV{H, n}; w.T = MatV{T, n}; w.Q = MatV{Q, n}; w.Z = MatV{Z, n};
   w.wantq = w.wantz = true;
@@ -270,6 +283,7 @@ int host_small_qz_ms(int n, double* H, double* T, double* Q, double* Z) {
 // {undeflated m, status, transformed}; shifts: alphar, alphai, beta (n each).
 void host_aed(int n, double* H, double* T, double* Q, double* Z, double s, int nskip, double* shifts, int* out3) {
   static HostExec x;
+  x.use_pipe();
   WinState w;
   w.n = n; w.H = MatV{H, n}; w.T = MatV{T, n}; w.Q = MatV{Q, n}; w.Z = MatV{Z, n};
   w.wantq = w.wantz = true;
@@ -284,6 +298,7 @@ void host_aed(int n, double* H, double* T, double* Q, double* Z, double s, int n
 void host_chase(int n, double* H, double* T, double* U, double* V, const int* bulges, const double* coef, int nb,
                 int tmax, int last) {
   static HostExec x;
+  x.use_pipe();
   std::vector<Bulge> bl(nb);
   for (int b = 0; b < nb; ++b) {
     bl[b].base = bulges[4 * b]; bl[b].tlo = bulges[4 * b + 1]; bl[b].thi = bulges[4 * b + 2];
@@ -300,6 +315,7 @@ void host_chase(int n, double* H, double* T, double* U, double* V, const int* bu
 int host_solve(int n, double* H, double* T, double* Q, double* Z, int nw_max, int w_chase, int nmin, int nskip,
                double* ar, double* ai, double* be, int* stats) {
   HostBK bk;
+  bk.x.use_pipe();
   bk.n = n; bk.ld = n; bk.H = H; bk.T = T; bk.Q = Q; bk.Z = Z; bk.nskip = nskip;
   // as the library does: T scaled by a power of two when its norm is far
   // from H's (shifts and their polynomials stay in range), undone at the end
@@ -335,6 +351,7 @@ int host_solve(int n, double* H, double* T, double* Q, double* Z, int nw_max, in
 int host_solve_p(int n, double* H, double* T, double* Q, double* Z, const int* ip, double* ar, double* ai, double* be,
                  int* stats) {
   HostBK bk;
+  bk.x.use_pipe();
   bk.n = n; bk.ld = n; bk.H = H; bk.T = T; bk.Q = Q; bk.Z = Z; bk.nskip = ip[3];
   bk.swapfail = ip[5];
   bk.schur = ip[6] != 0;

@@ -37,6 +37,9 @@ def host(tmp_path_factory):
     L.host_solve_p.restype = ctypes.c_int
     L.host_barriers.argtypes = [ctypes.POINTER(ctypes.c_long), ctypes.c_int]
     L.host_barriers.restype = None
+    L.host_set_pipe.argtypes = [ctypes.c_int]
+    L.host_set_pipe.restype = None
+    L.host_pipe_far_done.restype = ctypes.c_int
     return L
 
 
@@ -309,3 +312,46 @@ def test_host_aed_barrier_budget(pkg, lapack, host):
     print("barriers per AED call (double shift / multishift):", per)
     assert per[1][1] < 0.8 * per[0][1]
     assert sum(per[1][1:]) < 6000
+
+
+@pytest.mark.parametrize("n,seed,zf", [(3, 2, 0.0), (4, 1, 0.0), (17, 3, 0.0), (48, 7, 0.0), (60, 4, 0.05),
+                                       (120, 6, 0.02)])
+def test_host_pipelined_sweep_is_the_barrier_sweep(pkg, host, n, seed, zf):
+    """The pipelined double-shift sweep (core step, then far step, per step
+    on the host) splits the work between the core and the far threads so
+    that every element sees the same operations in the same order: the
+    window QZ gives bit-identical H, T, Q, Z to the two-barrier sweep."""
+    H, T = pkg.pencils.random_ht(n, seed, zf)
+    out = []
+    try:
+        for pipe in (0, 1):
+            host.host_set_pipe(pipe)
+            S, P, Q, Z = (np.array(M, order="F", copy=True) for M in (H, T, np.eye(n), np.eye(n)))
+            info = host.host_small_qz(n, _p(S), _p(P), _p(Q), _p(Z))
+            out.append((info, S, P, Q, Z))
+            if pipe and n >= 3:
+                assert host.host_pipe_far_done() > 0  # the pipelined sweep ran
+    finally:
+        host.host_set_pipe(0)
+    assert out[0][0] == out[1][0] == 0
+    for a, b in zip(out[0][1:], out[1][1:]):
+        assert np.array_equal(a, b)
+
+
+def test_host_pipelined_solve(pkg, lapack, host):
+    """A whole host solve with pipelined window sweeps: Schur form, backward
+    errors and LAPACK's eigenvalues."""
+    n = 300
+    H, T = pkg.pencils.random_ht(n, 11, 0.02)
+    S, P, Q, Z = (np.array(M, order="F", copy=True) for M in (H, T, np.eye(n), np.eye(n)))
+    ar, ai, be = np.zeros(n), np.zeros(n), np.zeros(n)
+    st = np.zeros(8, dtype=np.int32)
+    try:
+        host.host_set_pipe(1)
+        info = host.host_solve(n, _p(S), _p(P), _p(Q), _p(Z), 48, 80, 75, 0, _p(ar), _p(ai), _p(be),
+                               st.ctypes.data_as(_pi))
+    finally:
+        host.host_set_pipe(0)
+    assert info == 0
+    assert lapack.schur_structure_ok(S, P)
+    _check(lapack, H, T, S, P, Q, Z, (ar, ai, be))
