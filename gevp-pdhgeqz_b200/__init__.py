@@ -135,6 +135,12 @@ def lib() -> ctypes.CDLL:
     L.b200qz_mlp_backward.restype = _i
     L.b200qz_mlp_train.argtypes = [_vp, _vp, _vp, _i, _i, ctypes.c_float, _pf]
     L.b200qz_mlp_train.restype = _i
+    for f in ("b200qz_ggbal_dev", "b200qz_ggbal_host"):
+        getattr(L, f).argtypes = [_vp, _c, _i, _vp, _i, _vp, _i, _pi, _pi, _pd, _pd]
+        getattr(L, f).restype = _i
+    for f in ("b200qz_ggbak_dev", "b200qz_ggbak_host"):
+        getattr(L, f).argtypes = [_vp, _c, _c, _i, _i, _i, _pd, _pd, _i, _vp, _i]
+        getattr(L, f).restype = _i
     _lib = L
     return L
 
@@ -282,6 +288,42 @@ class Solver:
                                        _p(H), H.shape[0], _p(T), T.shape[0], _p(Qa), Qa.shape[0], _p(Za),
                                        Za.shape[0], _p(ar), _p(ai), _p(be))
         return ar, ai, be, info
+
+
+    def ggbal(self, A, B, job="B"):
+        """Balance the host pencil (A, B) in place on the GPU (DGGBAL
+        semantics).  Returns (ilo, ihi, lscale, rscale, info); ilo/ihi are
+        1-based."""
+        n = A.shape[0]
+        ls = np.zeros(max(1, n))
+        rs = np.zeros(max(1, n))
+        ilo = ctypes.c_int(0)
+        ihi = ctypes.c_int(0)
+        info = lib().b200qz_ggbal_host(self._h, job.encode(), n, _vp(A.ctypes.data), max(1, A.shape[0]),
+                                       _vp(B.ctypes.data), max(1, B.shape[0]), ctypes.byref(ilo), ctypes.byref(ihi),
+                                       _p(ls), _p(rs))
+        return ilo.value, ihi.value, ls[:n], rs[:n], info
+
+    def ggbal_device(self, a_ptr, b_ptr, n, ld, job="B"):
+        """Balance device arrays (column-major, leading dimension ld) in
+        place.  Returns (ilo, ihi, lscale, rscale, info)."""
+        ls = np.zeros(max(1, n))
+        rs = np.zeros(max(1, n))
+        ilo = ctypes.c_int(0)
+        ihi = ctypes.c_int(0)
+        info = lib().b200qz_ggbal_dev(self._h, job.encode(), n, _vp(a_ptr), ld, _vp(b_ptr), ld, ctypes.byref(ilo),
+                                      ctypes.byref(ihi), _p(ls), _p(rs))
+        return ilo.value, ihi.value, ls[:n], rs[:n], info
+
+    def ggbak(self, V, ilo, ihi, lscale, rscale, side="R", job="B"):
+        """Back-transform the host matrix V (n x m) in place (DGGBAK
+        semantics).  Returns info."""
+        n = V.shape[0]
+        m = V.shape[1] if V.ndim == 2 else 1
+        ls = np.ascontiguousarray(lscale, dtype=np.float64)
+        rs = np.ascontiguousarray(rscale, dtype=np.float64)
+        return lib().b200qz_ggbak_host(self._h, job.encode(), side.encode(), n, ilo, ihi, _p(ls), _p(rs), m,
+                                       _vp(V.ctypes.data), max(1, n))
 
 
 class Batch:

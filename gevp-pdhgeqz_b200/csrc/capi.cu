@@ -15,6 +15,7 @@
 #include <functional>
 
 #include "../../include/b200qz.h"
+#include "balance.h"
 #include "kernels.h"
 #include "ozaki.h"
 #include "policy.h"
@@ -1143,6 +1144,93 @@ void pdhgeqz_(const char* job, const char* compq, const char* compz, const int* 
   }
   *info = b200qz_solve_host(g_ctx, *job, *compq, *compz, N, ILO, IHI, h, ldh, t, ldt, q, ldq, z, ldz, alphar,
                             alphai, beta);
+}
+
+// ---------------------------------------------------------------------------
+// Balancing (DGGBAL / DGGBAK semantics) on device or host arrays.
+// ---------------------------------------------------------------------------
+static int ggbal_args(char job, int n, int lda, int ldb) {
+  if (!is(job, 'N') && !is(job, 'P') && !is(job, 'S') && !is(job, 'B')) return -1;
+  if (n < 0) return -2;
+  if (lda < std::max(1, n)) return -4;
+  if (ldb < std::max(1, n)) return -6;
+  return 0;
+}
+
+int b200qz_ggbal_dev(b200qz_ctx* c, char job, int n, double* a, int lda, double* b, int ldb, int* ilo, int* ihi,
+                     double* lscale, double* rscale) {
+  if (!c) return 10001;
+  const int bad = ggbal_args(job, n, lda, ldb);
+  if (bad) return bad;
+  if (cudaSetDevice(c->device) != cudaSuccess) return 10001;
+  return qz::ggbal_device(c->stream, job, n, a, lda, b, ldb, ilo, ihi, lscale, rscale) == cudaSuccess ? 0 : 10001;
+}
+
+int b200qz_ggbal_host(b200qz_ctx* c, char job, int n, double* a, int lda, double* b, int ldb, int* ilo, int* ihi,
+                      double* lscale, double* rscale) {
+  if (!c) return 10001;
+  const int bad = ggbal_args(job, n, lda, ldb);
+  if (bad) return bad;
+  if (n == 0) { *ilo = 1; *ihi = 0; return 0; }
+  if (cudaSetDevice(c->device) != cudaSuccess) return 10001;
+  double* d = nullptr;
+  const size_t nn = (size_t)n * n;
+  if (cudaMalloc(&d, 2 * nn * sizeof(double)) != cudaSuccess) return 10001;
+  cudaError_t e = cudaMemcpy2DAsync(d, n * sizeof(double), a, (size_t)lda * sizeof(double), n * sizeof(double), n,
+                                    cudaMemcpyHostToDevice, c->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpy2DAsync(d + nn, n * sizeof(double), b, (size_t)ldb * sizeof(double), n * sizeof(double), n,
+                          cudaMemcpyHostToDevice, c->stream);
+  if (e == cudaSuccess) e = qz::ggbal_device(c->stream, job, n, d, n, d + nn, n, ilo, ihi, lscale, rscale);
+  if (e == cudaSuccess)
+    e = cudaMemcpy2DAsync(a, (size_t)lda * sizeof(double), d, n * sizeof(double), n * sizeof(double), n,
+                          cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpy2DAsync(b, (size_t)ldb * sizeof(double), d + nn, n * sizeof(double), n * sizeof(double), n,
+                          cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  cudaFree(d);
+  return e == cudaSuccess ? 0 : 10001;
+}
+
+static int ggbak_args(char job, char side, int n, int ilo, int ihi, int m, int ldv) {
+  if (!is(job, 'N') && !is(job, 'P') && !is(job, 'S') && !is(job, 'B')) return -1;
+  if (!is(side, 'L') && !is(side, 'R')) return -2;
+  if (n < 0) return -3;
+  if (n > 0 ? (ilo < 1 || ilo > n) : ilo != 1) return -4;
+  if (n > 0 ? (ihi < ilo || ihi > n) : ihi != 0) return -5;
+  if (m < 0) return -8;
+  if (ldv < std::max(1, n)) return -10;
+  return 0;
+}
+
+int b200qz_ggbak_dev(b200qz_ctx* c, char job, char side, int n, int ilo, int ihi, const double* lscale,
+                     const double* rscale, int m, double* v, int ldv) {
+  if (!c) return 10001;
+  const int bad = ggbak_args(job, side, n, ilo, ihi, m, ldv);
+  if (bad) return bad;
+  if (cudaSetDevice(c->device) != cudaSuccess) return 10001;
+  return qz::ggbak_device(c->stream, job, side, n, ilo, ihi, lscale, rscale, m, v, ldv) == cudaSuccess ? 0 : 10001;
+}
+
+int b200qz_ggbak_host(b200qz_ctx* c, char job, char side, int n, int ilo, int ihi, const double* lscale,
+                      const double* rscale, int m, double* v, int ldv) {
+  if (!c) return 10001;
+  const int bad = ggbak_args(job, side, n, ilo, ihi, m, ldv);
+  if (bad) return bad;
+  if (n == 0 || m == 0) return 0;
+  if (cudaSetDevice(c->device) != cudaSuccess) return 10001;
+  double* d = nullptr;
+  if (cudaMalloc(&d, (size_t)n * m * sizeof(double)) != cudaSuccess) return 10001;
+  cudaError_t e = cudaMemcpy2DAsync(d, n * sizeof(double), v, (size_t)ldv * sizeof(double), n * sizeof(double), m,
+                                    cudaMemcpyHostToDevice, c->stream);
+  if (e == cudaSuccess) e = qz::ggbak_device(c->stream, job, side, n, ilo, ihi, lscale, rscale, m, d, n);
+  if (e == cudaSuccess)
+    e = cudaMemcpy2DAsync(v, (size_t)ldv * sizeof(double), d, n * sizeof(double), n * sizeof(double), m,
+                          cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  cudaFree(d);
+  return e == cudaSuccess ? 0 : 10001;
 }
 
 }  // extern "C"

@@ -262,6 +262,44 @@ int b200qz_update(b200qz_ctx* ctx, char side, double* m, int ldm, int r0, int c0
 int b200qz_update_split(b200qz_ctx* ctx, char side, double* m, int ldm, int r0, int c0, int len, const double* w,
                         int ldw, int k, int slices);
 
+/* ------------------------------------------------------------------ */
+/* Balancing: the step that produces ILO/IHI for PDHGEQZ                */
+/* ------------------------------------------------------------------ */
+
+/* Balance a general pencil (A, B) with the semantics of LAPACK DGGBAL,
+ * whose ILO/IHI output the reference's driver takes (PDHGEQZ.f:155-161;
+ * DGGBAL itself is LAPACK's, not the reference's).  job: 'N' nothing,
+ * 'P' permute only, 'S' scale only, 'B' both.  Permutation moves rows
+ * whose nonzeros lie in at most one active column to the bottom (searched
+ * from the bottom) and then columns whose nonzeros lie in at most one
+ * active row to the top (searched from the left), so that A and B are
+ * upper triangular outside rows/columns ILO..IHI.  Scaling multiplies
+ * rows and columns ILO..IHI by powers of ten chosen by Ward's
+ * least-squares method (conjugate gradients, at most IHI-ILO+3
+ * iterations).  ilo/ihi are returned 1-based (ilo = 1, ihi = 0 for
+ * n = 0); lscale/rscale (host arrays of n doubles) hold, for positions
+ * outside ILO..IHI, the 1-based row/column interchanged with that
+ * position, and inside it the row/column scale factors.  The _dev form
+ * takes device arrays (transformed in place on the context's stream),
+ * the _host form host arrays.  Returns 0; -1 bad job, -2 n < 0, -4 lda,
+ * -6 ldb (DGGBAL's argument positions); 10001 on a CUDA error. */
+int b200qz_ggbal_dev(b200qz_ctx* ctx, char job, int n, double* a, int lda, double* b, int ldb, int* ilo, int* ihi,
+                     double* lscale, double* rscale);
+int b200qz_ggbal_host(b200qz_ctx* ctx, char job, int n, double* a, int lda, double* b, int ldb, int* ilo, int* ihi,
+                      double* lscale, double* rscale);
+
+/* Back-transform the n x m matrix V (eigenvectors, or the Schur vectors
+ * Q (side 'L') / Z (side 'R') of the balanced pencil) with the semantics
+ * of LAPACK DGGBAK: rows ILO..IHI scaled by lscale ('L') or rscale ('R')
+ * when job is 'S' or 'B', then the recorded row interchanges undone when
+ * job is 'P' or 'B'.  lscale/rscale are the host arrays ggbal returned.
+ * Returns 0; -1 job, -2 side, -3 n, -4 ilo, -5 ihi, -8 m, -10 ldv
+ * (DGGBAK's argument positions); 10001 on a CUDA error. */
+int b200qz_ggbak_dev(b200qz_ctx* ctx, char job, char side, int n, int ilo, int ihi, const double* lscale,
+                     const double* rscale, int m, double* v, int ldv);
+int b200qz_ggbak_host(b200qz_ctx* ctx, char job, char side, int n, int ilo, int ihi, const double* lscale,
+                      const double* rscale, int m, double* v, int ldv);
+
 #ifdef __cplusplus
 }
 #endif

@@ -16,6 +16,9 @@ names:
 * ``DTGEVC`` + ``DTGSNA`` -- eigenvectors and reciprocal eigenvalue
   condition numbers used to scale the eigenvalue matching tolerance.
 * ``DGGHRD``  -- Hessenberg-triangular reduction (``qzearly.f:449``).
+* ``DGGBAL`` / ``DGGBAK`` -- balancing that produces the ILO/IHI the
+  reference's driver takes (``PDHGEQZ.f:155-161``) and its back
+  transformation; not in the reference, called from LAPACK.
 
 Residual definitions follow ``tools/PQZHLPS.f`` (PCOMPRES):
 ||S - Q^T A Z||_F / ||A||_F, ||P - Q^T B Z||_F / ||B||_F and
@@ -110,6 +113,37 @@ def dgghrd(A, B, compq="I", compz="I"):
                         _dp(H), _ip(ld), _dp(T), _ip(ld), _dp(Q), _ip(ld), _dp(Z), _ip(ld),
                         ctypes.byref(info), ctypes.c_size_t(1), ctypes.c_size_t(1))
     return H, T, Q, Z, info.value
+
+
+def dggbal(A, B, job="B"):
+    """LAPACK DGGBAL.  Returns (A', B', ilo, ihi, lscale, rscale, info)
+    with 1-based ilo/ihi and LAPACK's lscale/rscale (permutation indices,
+    1-based, outside ilo..ihi; scale factors inside)."""
+    n = A.shape[0]
+    Ab = np.array(A, dtype=np.float64, order="F", copy=True)
+    Bb = np.array(B, dtype=np.float64, order="F", copy=True)
+    ilo = ctypes.c_int(0)
+    ihi = ctypes.c_int(0)
+    ls = np.zeros(max(1, n))
+    rs = np.zeros(max(1, n))
+    work = np.zeros(max(1, 6 * n))
+    info = ctypes.c_int(0)
+    ld = max(1, n)
+    lib().scipy_dggbal_(_c(job.encode()), _ip(n), _dp(Ab), _ip(ld), _dp(Bb), _ip(ld), ctypes.byref(ilo),
+                        ctypes.byref(ihi), _dp(ls), _dp(rs), _dp(work), ctypes.byref(info), ctypes.c_size_t(1))
+    return Ab, Bb, ilo.value, ihi.value, ls[:n], rs[:n], info.value
+
+
+def dggbak(V, ilo, ihi, lscale, rscale, side="R", job="B"):
+    """LAPACK DGGBAK: back-transform the columns of V (n x m)."""
+    n, m = V.shape
+    Vb = np.array(V, dtype=np.float64, order="F", copy=True)
+    ls = np.array(lscale, dtype=np.float64, copy=True)
+    rs = np.array(rscale, dtype=np.float64, copy=True)
+    info = ctypes.c_int(0)
+    lib().scipy_dggbak_(_c(job.encode()), _c(side.encode()), _ip(n), _ip(ilo), _ip(ihi), _dp(ls), _dp(rs),
+                        _ip(m), _dp(Vb), _ip(max(1, n)), ctypes.byref(info), ctypes.c_size_t(1), ctypes.c_size_t(1))
+    return Vb, info.value
 
 
 def eig_condition(S, P, Q=None, Z=None):
