@@ -119,6 +119,7 @@ __global__ void __launch_bounds__(kPermThreads) k_bal_perm(double* A, int64_t ld
     }
     if (threadIdx.x == 0) { lrec[hi] = rs; rrec[hi] = jc; }
     if (rs != hi) swap_rows2(A, lda, B, ldb, n, rs, hi);
+    __syncthreads();  // the two swaps share four elements
     if (jc != hi) swap_cols2(A, lda, B, ldb, n, jc, hi);
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -149,6 +150,7 @@ __global__ void __launch_bounds__(kPermThreads) k_bal_perm(double* A, int64_t ld
     }
     if (threadIdx.x == 0) { lrec[lo] = ir; rrec[lo] = cs; }
     if (cs != lo) swap_cols2(A, lda, B, ldb, n, cs, lo);
+    __syncthreads();
     if (ir != lo) swap_rows2(A, lda, B, ldb, n, ir, lo);
     __syncthreads();
     if (threadIdx.x == 0) { int t = colcnt[cs]; colcnt[cs] = colcnt[lo]; colcnt[lo] = t; }

@@ -16,6 +16,7 @@
 
 #include "../../include/b200qz.h"
 #include "balance.h"
+#include "reorder.h"
 #include "kernels.h"
 #include "ozaki.h"
 #include "policy.h"
@@ -1231,6 +1232,83 @@ int b200qz_ggbak_host(b200qz_ctx* c, char job, char side, int n, int ilo, int ih
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   cudaFree(d);
   return e == cudaSuccess ? 0 : 10001;
+}
+
+// ---------------------------------------------------------------------------
+// Reordering of a generalized Schur form (DTGSEN semantics, IJOB 0 and 1).
+// ---------------------------------------------------------------------------
+static int tgsen_args(int ijob, int wantq, int wantz, int n, int lds, int ldt, int ldq, int ldz) {
+  if (ijob < 0 || ijob > 1) return -1;
+  if (n < 0) return -5;
+  if (lds < std::max(1, n)) return -7;
+  if (ldt < std::max(1, n)) return -9;
+  if (ldq < 1 || (wantq && ldq < n)) return -14;
+  if (ldz < 1 || (wantz && ldz < n)) return -16;
+  return 0;
+}
+
+int b200qz_tgsen_dev(b200qz_ctx* c, int ijob, int wantq, int wantz, const int* select, int n, double* s, int lds,
+                     double* t, int ldt, double* q, int ldq, double* z, int ldz, double* alphar, double* alphai,
+                     double* beta, int* m, double* pl, double* pr, int* info, int* counts) {
+  if (!c) return 10001;
+  const int bad = tgsen_args(ijob, wantq, wantz, n, lds, ldt, ldq, ldz);
+  if (bad) return bad;
+  if (cudaSetDevice(c->device) != cudaSuccess) return 10001;
+  qz::ReorderOut o;
+  const cudaError_t e = qz::tgsen_device(c->stream, ijob, wantq != 0, wantz != 0, select, n, s, lds, t, ldt, q, ldq,
+                                         z, ldz, alphar, alphai, beta, &o);
+  if (e != cudaSuccess) return 10001;
+  *m = o.m;
+  *pl = o.pl;
+  *pr = o.pr;
+  *info = o.info;
+  if (counts) { counts[0] = o.swaps; counts[1] = o.windows; }
+  return 0;
+}
+
+int b200qz_tgsen_host(b200qz_ctx* c, int ijob, int wantq, int wantz, const int* select, int n, double* s, int lds,
+                      double* t, int ldt, double* q, int ldq, double* z, int ldz, double* alphar, double* alphai,
+                      double* beta, int* m, double* pl, double* pr, int* info) {
+  if (!c) return 10001;
+  const int bad = tgsen_args(ijob, wantq, wantz, n, lds, ldt, ldq, ldz);
+  if (bad) return bad;
+  if (n == 0) { *m = 0; *pl = *pr = 1.0; *info = 0; return 0; }
+  if (cudaSetDevice(c->device) != cudaSuccess) return 10001;
+  const size_t nn = (size_t)n * n;
+  double* d = nullptr;
+  if (cudaMalloc(&d, (4 * nn + 3 * (size_t)n) * sizeof(double)) != cudaSuccess) return 10001;
+  double *ds = d, *dt = d + nn, *dq = d + 2 * nn, *dz = d + 3 * nn, *de = d + 4 * nn;
+  const size_t w = n * sizeof(double);
+  cudaError_t e = cudaMemcpy2DAsync(ds, w, s, (size_t)lds * sizeof(double), w, n, cudaMemcpyHostToDevice, c->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpy2DAsync(dt, w, t, (size_t)ldt * sizeof(double), w, n, cudaMemcpyHostToDevice, c->stream);
+  if (e == cudaSuccess && wantq)
+    e = cudaMemcpy2DAsync(dq, w, q, (size_t)ldq * sizeof(double), w, n, cudaMemcpyHostToDevice, c->stream);
+  if (e == cudaSuccess && wantz)
+    e = cudaMemcpy2DAsync(dz, w, z, (size_t)ldz * sizeof(double), w, n, cudaMemcpyHostToDevice, c->stream);
+  qz::ReorderOut o;
+  if (e == cudaSuccess)
+    e = qz::tgsen_device(c->stream, ijob, wantq != 0, wantz != 0, select, n, ds, n, dt, n, dq, n, dz, n, de, de + n,
+                         de + 2 * n, &o);
+  if (e == cudaSuccess)
+    e = cudaMemcpy2DAsync(s, (size_t)lds * sizeof(double), ds, w, w, n, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpy2DAsync(t, (size_t)ldt * sizeof(double), dt, w, w, n, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess && wantq)
+    e = cudaMemcpy2DAsync(q, (size_t)ldq * sizeof(double), dq, w, w, n, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess && wantz)
+    e = cudaMemcpy2DAsync(z, (size_t)ldz * sizeof(double), dz, w, w, n, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(alphar, de, w, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(alphai, de + n, w, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(beta, de + 2 * n, w, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  cudaFree(d);
+  if (e != cudaSuccess) return 10001;
+  *m = o.m;
+  *pl = o.pl;
+  *pr = o.pr;
+  *info = o.info;
+  return 0;
 }
 
 }  // extern "C"

@@ -521,6 +521,10 @@ void launch_finalize(cudaStream_t st, double* H, double* T, double* Z, int64_t l
   k_signs<<<n, 256, 0, st>>>(H, T, Z, ld, n, wantz);
   k_eigs<<<(n + 255) / 256, 256, 0, st>>>(H, T, ld, n, ar, ai, be);
 }
+void launch_eigs(cudaStream_t st, const double* H, const double* T, int64_t ld, int n, double* ar, double* ai,
+                 double* be) {
+  if (n > 0) k_eigs<<<(n + 255) / 256, 256, 0, st>>>(H, T, ld, n, ar, ai, be);
+}
 void launch_identity(cudaStream_t st, double* Q, int64_t ld, int n) {
   k_set_identity<<<592, 256, 0, st>>>(Q, ld, n);
 }

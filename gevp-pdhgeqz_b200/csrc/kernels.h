@@ -61,6 +61,9 @@ int update_tile(int k);
 void launch_finalize(cudaStream_t st, double* H, double* T, double* Z, int64_t ld, int n, int wantz, double* ar,
                      double* ai, double* be);
 void launch_identity(cudaStream_t st, double* Q, int64_t ld, int n);
+// eigenvalues (alphar, alphai, beta) of the diagonal blocks of a standardised Schur form
+void launch_eigs(cudaStream_t st, const double* H, const double* T, int64_t ld, int n, double* ar, double* ai,
+                 double* be);
 // out[0] = largest |A(i,j)| over A(o:o+n, o:o+n); partial: 592 doubles of scratch
 void launch_maxabs(cudaStream_t st, const double* A, int64_t ld, int o, int n, double* out, double* partial);
 // A(0:n, 0:n) <- 2^e A

@@ -16,6 +16,10 @@ names:
 * ``DTGEVC`` + ``DTGSNA`` -- eigenvectors and reciprocal eigenvalue
   condition numbers used to scale the eigenvalue matching tolerance.
 * ``DGGHRD``  -- Hessenberg-triangular reduction (``qzearly.f:449``).
+* ``DTGSEN`` -- reordering of a generalized Schur form and the
+  projection norms PL/PR (the role of the reference's PDTGSEN,
+  ``src/reorder/PDTGSEN.f:1``), through scipy's wrapper of the same
+  LAPACK.
 * ``DGGBAL`` / ``DGGBAK`` -- balancing that produces the ILO/IHI the
   reference's driver takes (``PDHGEQZ.f:155-161``) and its back
   transformation; not in the reference, called from LAPACK.
@@ -132,6 +136,18 @@ def dggbal(A, B, job="B"):
     lib().scipy_dggbal_(_c(job.encode()), _ip(n), _dp(Ab), _ip(ld), _dp(Bb), _ip(ld), ctypes.byref(ilo),
                         ctypes.byref(ihi), _dp(ls), _dp(rs), _dp(work), ctypes.byref(info), ctypes.c_size_t(1))
     return Ab, Bb, ilo.value, ihi.value, ls[:n], rs[:n], info.value
+
+
+def dtgsen(S, P, Q, Z, select, ijob=0):
+    """LAPACK DTGSEN.  Returns (S', P', alphar, alphai, beta, Q', Z', m,
+    pl, pr, dif, info); dif holds the Dif estimates for ijob >= 2."""
+    import scipy.linalg.lapack as SL
+    n = S.shape[0]
+    lw = 4 * n + 16 + 2 * n * n
+    r = SL.dtgsen(np.asarray(select, dtype=np.int32), np.array(S, order="F"), np.array(P, order="F"),
+                  np.array(Q, order="F"), np.array(Z, order="F"), ijob=ijob, lwork=lw, liwork=n + 6 + 2 * n * n)
+    a, b, ar, ai, be, q, z, m, pl, pr, dif, info = r
+    return a, b, ar, ai, be, q, z, int(m), float(pl), float(pr), np.array(dif), int(info)
 
 
 def dggbak(V, ilo, ihi, lscale, rscale, side="R", job="B"):
