@@ -2,6 +2,7 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--n 10000] [--workload c3] [--mode plain|split|learned|split+learned]
+       python bench.py --workload ggbal|tgsen   (balancing / reordering, LAPACK timed beside)
 
 One step = one complete reduction of a Hessenberg-triangular pencil to
 generalized real Schur form with Q and Z (JOB='S', COMPQ=COMPZ='I').
@@ -583,6 +584,184 @@ def run_batched(args, pkg, rank, world, local):
         dist.destroy_process_group()
 
 
+# ---------------------------------------------------------------------------
+# The steps either side of the solve: balancing (DGGBAL semantics) and
+# reordering of the Schur form (DTGSEN semantics), each timed on the GPU
+# with LAPACK's routine timed beside it on the same input.
+# ---------------------------------------------------------------------------
+def post_pencil(n, seed, k1, k2, decades):
+    """Dense pencil with k1 + k2 eigenvalues that permutations isolate
+    (block triangular under hidden row/column permutations) and rows and
+    columns graded over ``decades`` decades."""
+    rng = np.random.default_rng(seed)
+
+    def one():
+        M = rng.standard_normal((n, n))
+        M[k1:, :k1] = 0.0
+        M[n - k2:, :n - k2] = 0.0
+        M[:k1, :k1] = np.triu(M[:k1, :k1])
+        M[n - k2:, n - k2:] = np.triu(M[n - k2:, n - k2:])
+        return M
+
+    A, B = one(), one()
+    pr, pc = rng.permutation(n), rng.permutation(n)
+    d = np.logspace(-decades / 2, decades / 2, n)
+    return np.asfortranarray(A[pr][:, pc] * d[:, None]), np.asfortranarray(B[pr][:, pc] * d[None, ::-1])
+
+
+def run_post(args, pkg):
+    import time
+    import torch
+    from oracle import lapack as L
+    torch.cuda.set_device(0)
+    dev = torch.cuda.current_device()
+    solver = pkg.Solver(dev)
+    peaks, peak_kind = read_peaks()
+    clocks = ClockSampler(dev)
+    if args.workload == "ggbal":
+        n = args.n
+        A, B = post_pencil(n, 5, 64, 64, 8)
+        dA0 = torch.from_numpy(np.ascontiguousarray(A.T)).to(dev)
+        dB0 = torch.from_numpy(np.ascontiguousarray(B.T)).to(dev)
+        dA, dB = torch.empty_like(dA0), torch.empty_like(dB0)
+
+        def step():
+            dA.copy_(dA0)
+            dB.copy_(dB0)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            ilo, ihi, ls, rs, info = solver.ggbal_device(dA.data_ptr(), dB.data_ptr(), n, n, "B")
+            t = time.perf_counter() - t0
+            if info != 0:
+                raise RuntimeError("ggbal returned %d" % info)
+            return t, (ilo, ihi, ls, rs)
+
+        for _ in range(args.warmup):
+            step()
+        clocks.start()
+        ts = [step() for _ in range(args.steps)]
+        clk = clocks.stop()
+        t = float(np.mean([x[0] for x in ts]))
+        ilo, ihi, ls, rs = ts[-1][1]
+        # end to end: host arrays in, balanced host arrays out
+        te = []
+        for _ in range(args.steps):
+            Ah, Bh = np.array(A, order="F"), np.array(B, order="F")
+            t0 = time.perf_counter()
+            solver.ggbal(Ah, Bh, "B")
+            te.append(time.perf_counter() - t0)
+        cpu = None
+        if not args.no_cpu_baseline:
+            t0 = time.perf_counter()
+            La, Lb, lilo, lihi, lls, lrs, _ = L.dggbal(A, B, "B")
+            cpu_t = time.perf_counter() - t0
+            same = (lilo, lihi) == (ilo, ihi) and np.array_equal(lls, ls) and np.array_equal(lrs, rs)
+            cpu = {"value": cpu_t, "unit": "s", "cores": 1, "kind": "reference",
+                   "sample": "LAPACK DGGBAL (scipy's OpenBLAS) on the same pencil, one call",
+                   "identical_output": bool(same)}
+        nr = ihi - ilo + 1
+        # algorithmic bytes: counts (read A, B), logs (two reads of the
+        # active block), maxima (read), apply (read + write), nonzero byte
+        # matrix and its reads by the CG iterations (at most nr + 2)
+        alg = 16.0 * n * n * 4 + 32.0 * nr * nr + 1.0 * nr * nr
+        peak = peaks.get("hbm_gbs")
+        ach = alg / t / 1e9
+        line = {"metric": "balance_seconds", "value": t, "unit": "s", "n_gpus": 1, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": False, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": "ggbal: DGGBAL job B, n=%d, 128 isolatable eigenvalues under hidden "
+                                       "permutations, rows/columns graded over 8 decades (seed 5)" % n,
+                           "n": n, "ilo": ilo, "ihi": ihi, "inputs": "device-resident copies, 2 x %.2f GB" %
+                           (8e-9 * n * n)},
+                "e2e": {"value": float(np.mean(te)), "unit": "s", "h2d_bytes_per_step": 16 * n * n,
+                        "d2h_bytes_per_step": 16 * n * n},
+                "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
+                             "frac": (ach / peak) if peak else None, "traffic": None,
+                             "peak_source": "%s HBM copy bandwidth" % peak_kind,
+                             "note": "whole call (host isolation/CG control included) against the copy "
+                                     "bandwidth; algorithmic bytes %.3g" % alg},
+                "cpu_baseline": cpu, "clocks": clk, "gpu_launches": None}
+        print(json.dumps(line), flush=True)
+        solver.close()
+        return
+    # tgsen: reorder the GPU's Schur form of a random pencil so that the
+    # eigenvalues of modulus below the median lead (n = 2000 unless --n
+    # is given: LAPACK's DTGSEN beside it takes minutes above that)
+    n = args.n if args.n != 10000 else 2000
+    H, T = pkg.pencils.random_ht(n, 6, 0.0)
+    S, P, Q, Z, ar, ai, be, info = pkg.solve(H, T)
+    if info != 0:
+        raise RuntimeError("solve returned %d" % info)
+    lam = np.abs(ar + 1j * ai) / np.maximum(np.abs(be), 1e-300)
+    sel = (lam < np.median(lam)).astype(np.int32)
+    d0 = [torch.from_numpy(np.ascontiguousarray(M.T)).to(dev) for M in (S, P, Q, Z)]
+    dw = [torch.empty_like(x) for x in d0]
+    de = torch.empty(3 * n, dtype=torch.float64, device=dev)
+    lib = pkg.lib()
+
+    def step():
+        for a, b in zip(dw, d0):
+            a.copy_(b)
+        torch.cuda.synchronize()
+        m, inf = pkg.ctypes.c_int(0), pkg.ctypes.c_int(0)
+        pl, pr = pkg.ctypes.c_double(0), pkg.ctypes.c_double(0)
+        cnt = np.zeros(2, dtype=np.int32)
+        t0 = time.perf_counter()
+        rc = lib.b200qz_tgsen_dev(solver.handle, 0, 1, 1, sel.ctypes.data_as(pkg._pi), n,
+                                  pkg._vp(dw[0].data_ptr()), n, pkg._vp(dw[1].data_ptr()), n,
+                                  pkg._vp(dw[2].data_ptr()), n, pkg._vp(dw[3].data_ptr()), n,
+                                  pkg._vp(de.data_ptr()), pkg._vp(de.data_ptr() + 8 * n),
+                                  pkg._vp(de.data_ptr() + 16 * n), pkg.ctypes.byref(m), pkg.ctypes.byref(pl),
+                                  pkg.ctypes.byref(pr), pkg.ctypes.byref(inf), cnt.ctypes.data_as(pkg._pi))
+        t = time.perf_counter() - t0
+        if rc != 0 or inf.value != 0:
+            raise RuntimeError("tgsen returned %d / info %d" % (rc, inf.value))
+        return t, m.value, cnt
+
+    for _ in range(args.warmup):
+        step()
+    clocks.start()
+    ts = [step() for _ in range(args.steps)]
+    clk = clocks.stop()
+    t = float(np.mean([x[0] for x in ts]))
+    m, cnt = ts[-1][1], ts[-1][2]
+    te = []
+    for _ in range(args.steps):
+        Sh, Ph, Qh, Zh = (np.array(M, order="F") for M in (S, P, Q, Z))
+        t0 = time.perf_counter()
+        solver.tgsen(Sh, Ph, Qh, Zh, sel, ijob=0)
+        te.append(time.perf_counter() - t0)
+    cpu = None
+    if not args.no_cpu_baseline:
+        t0 = time.perf_counter()
+        out = L.dtgsen(S, P, Q, Z, sel, ijob=0)
+        cpu_t = time.perf_counter() - t0
+        cpu = {"value": cpu_t, "unit": "s", "cores": 1, "kind": "reference",
+               "sample": "LAPACK DTGSEN (IJOB 0, scipy's OpenBLAS) on the same Schur form, one call",
+               "m": int(out[7])}
+    # the windows' factor updates: each window of k rows updates k rows of
+    # S, T to its right, k columns of S, T above it and k columns of Q, Z
+    # (read + write, 16 bytes per element); at most 80 rows per window
+    upd_bytes = 16.0 * int(cnt[1]) * 80 * (2 * n + 2 * n)
+    peak = peaks.get("hbm_gbs")
+    line = {"metric": "reorder_seconds", "value": t, "unit": "s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "tgsen: DTGSEN IJOB 0, Schur form of random_ht(n=%d, seed 6), eigenvalues "
+                                   "of modulus below the median selected" % n, "n": n, "m": m,
+                       "swaps": int(cnt[0]), "windows": int(cnt[1])},
+            "e2e": {"value": float(np.mean(te)), "unit": "s", "h2d_bytes_per_step": 32 * n * n,
+                    "d2h_bytes_per_step": 32 * n * n + 24 * n},
+            "roofline": {"bound": "hbm", "achieved": upd_bytes / t / 1e9, "peak": peak, "unit": "GB/s",
+                         "frac": (upd_bytes / t / 1e9 / peak) if peak else None, "traffic": None,
+                         "peak_source": "%s HBM copy bandwidth" % peak_kind,
+                         "note": "factor-update bytes of the windows over the whole call; the swap chains "
+                                 "inside each window are latency-bound on one CTA"},
+            "cpu_baseline": cpu, "clocks": clk, "gpu_launches": 3 * int(cnt[1]) + 2}
+    print(json.dumps(line), flush=True)
+    solver.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -612,6 +791,13 @@ def main():
         return
     if args.workload == "c5":
         run_batched(args, pkg, rank, world, local)
+        return
+    if args.workload in ("ggbal", "tgsen"):
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the ggbal/tgsen workloads time LAPACK "
+                              "beside the GPU call in their own line (cpu_baseline)"}))
+        elif rank == 0:
+            run_post(args, pkg)
         return
     if args.impl == "reference":
         run_reference(args, pkg, rank)

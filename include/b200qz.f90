@@ -38,5 +38,54 @@ module b200qz
        import :: c_double
        real(c_double), intent(in) :: eps
      end subroutine b200qz_kkqzconf
+
+     ! context for the native entries below (one per device and host thread)
+     integer(c_int) function b200qz_create(ctx, device) bind(C, name="b200qz_create")
+       import :: c_int, c_ptr
+       type(c_ptr), intent(out) :: ctx
+       integer(c_int), value :: device
+     end function b200qz_create
+     subroutine b200qz_destroy(ctx) bind(C, name="b200qz_destroy")
+       import :: c_ptr
+       type(c_ptr), value :: ctx
+     end subroutine b200qz_destroy
+
+     ! balancing with DGGBAL's arguments (host arrays), the ILO/IHI producer
+     ! the driver takes (PDHGEQZ.f:155-161); returns 0 or -i / 10001
+     integer(c_int) function b200qz_ggbal_host(ctx, job, n, a, lda, b, ldb, ilo, ihi, lscale, rscale) &
+          bind(C, name="b200qz_ggbal_host")
+       import :: c_int, c_double, c_char, c_ptr
+       type(c_ptr), value :: ctx
+       character(kind=c_char), value :: job
+       integer(c_int), value :: n, lda, ldb
+       real(c_double), intent(inout) :: a(*), b(*)
+       integer(c_int), intent(out) :: ilo, ihi
+       real(c_double), intent(out) :: lscale(*), rscale(*)
+     end function b200qz_ggbal_host
+
+     ! back transformation with DGGBAK's arguments (host array v, n x m)
+     integer(c_int) function b200qz_ggbak_host(ctx, job, side, n, ilo, ihi, lscale, rscale, m, v, ldv) &
+          bind(C, name="b200qz_ggbak_host")
+       import :: c_int, c_double, c_char, c_ptr
+       type(c_ptr), value :: ctx
+       character(kind=c_char), value :: job, side
+       integer(c_int), value :: n, ilo, ihi, m, ldv
+       real(c_double), intent(in) :: lscale(*), rscale(*)
+       real(c_double), intent(inout) :: v(*)
+     end function b200qz_ggbak_host
+
+     ! reordering of the Schur form with DTGSEN's arguments (IJOB 0 or 1);
+     ! the role of PDTGSEN (src/reorder/PDTGSEN.f:1)
+     integer(c_int) function b200qz_tgsen_host(ctx, ijob, wantq, wantz, select, n, s, lds, t, ldt, q, ldq, &
+          z, ldz, alphar, alphai, beta, m, pl, pr, info) bind(C, name="b200qz_tgsen_host")
+       import :: c_int, c_double, c_ptr
+       type(c_ptr), value :: ctx
+       integer(c_int), value :: ijob, wantq, wantz, n, lds, ldt, ldq, ldz
+       integer(c_int), intent(in) :: select(*)
+       real(c_double), intent(inout) :: s(*), t(*), q(*), z(*)
+       real(c_double), intent(out) :: alphar(*), alphai(*), beta(*)
+       integer(c_int), intent(out) :: m, info
+       real(c_double), intent(out) :: pl, pr
+     end function b200qz_tgsen_host
   end interface
 end module b200qz
