@@ -192,6 +192,124 @@ QZ_HD int cta_small_qz_ms(X& x, WinState& w, int maxit, double* scr) {
 // applied.  When nothing deflates the window is left in Schur form but the
 // caller discards it (the pencil is unchanged).
 // ---------------------------------------------------------------------------
+// ---------------------------------------------------------------------------
+// Hessenberg-triangular re-reduction of the leading m x m block of a window
+// whose T is upper triangular and whose H is full in that block, by Givens
+// rotations (the job of DGGHRD at qzearly.f:449).  Pair (jc, jr): the row
+// rotation G on rows jr-1, jr zeros H(jr, jc); the T(jr, jr-1) it creates
+// is removed by the column rotation Z on columns jr, jr-1.
+//
+// One barrier per pair, with one pair of lookahead: in the phase of pair
+// k, every thread applies pair k-1 to its indices of the far parts while
+// the block thread (a) applies pair k-1 to the few entries pair k reads --
+// row jr-2 at columns jr-1, jr (Z) and column jr-2 at rows jr-1, jr (G) --
+// (b) stores pair k-1's 2x2 blocks of H and T, except the entries pair k
+// recomputes, and (c) forms pair k's rotations and 2x2 blocks from them
+// and publishes the rotations.  The far parts of pair k-1 exclude exactly
+// the entries of (a) and (b), so each entry sees the same rotations in the
+// same order as with a barrier between compute and apply.  A column ends
+// with a phase that applies its last pair; the next column's first pair
+// reads everything from memory.
+// ---------------------------------------------------------------------------
+struct HrPair {
+  int jc, jr;             // pair; jr < 0: none
+  double c, sn, cz, sz;   // G and Z
+  double r, rz;           // new H(jr-1, jc), T(jr, jr)
+  double h00, h10, h01, h11, t00, t01;  // 2x2 blocks of H and T(jr-1, .) after the pair
+};
+
+template <class X>
+QZ_HD void cta_hessred(X& x, WinState& w, int m) {
+  const int n = w.n;
+  const bool bt = block_thread(x);
+  double* slot = x.sd;  // two slots of 4 rotation values (the far threads' copy)
+  HrPair p;             // pending pair (block thread: all fields; others: jc, jr)
+  p.jc = -1; p.jr = -1;
+  int phase = 0;
+  // one phase: far parts of the pending pair p, and on the block thread its
+  // stores and the next pair (kjc, kjr) (kjr < 0: none)
+  auto run_phase = [&](int kjc, int kjr) {
+    const bool nextsame = p.jr >= 0 && kjr >= 0 && kjc == p.jc;
+    if (p.jr >= 0) {
+      const int J = p.jr, jc = p.jc;
+      const double* sl = slot + 4 * ((phase - 1) & 1);
+      const double c = sl[0], sn = sl[1], cz = sl[2], sz = sl[3];
+      for (int t = x.tid; t < n; t += x.nt) {
+        if ((t >= jc + 1 && t <= J - 3) || t >= J + 1) rot_vec(c, sn, &w.H(J - 1, t), 1);
+        if (t >= J + 1) rot_vec(c, sn, &w.T(J - 1, t), 1);
+        if (w.wantq) rot_vec(c, sn, &w.Q(t, J - 1), w.Q.ld);
+        if (t <= J - 3 || (t >= J + 1 && t < m)) rot_vec(cz, sz, &w.H(t, J), -(int64_t)w.H.ld);
+        if (t <= J - 3) rot_vec(cz, sz, &w.T(t, J), -(int64_t)w.T.ld);
+        if (w.wantz) rot_vec(cz, sz, &w.Z(t, J), -(int64_t)w.Z.ld);
+      }
+    }
+    if (bt) {
+      // (a) pair p on row J-2 (Z) and column J-2 (G); (b) p's stores
+      double a_h01 = 0.0, a_t01 = 0.0, a_h10 = 0.0;
+      if (p.jr >= 0) {
+        const int J = p.jr, R = J - 2;
+        double hJ = w.H(R, J), hJm = w.H(R, J - 1), tJ = w.T(R, J), tJm = w.T(R, J - 1);
+        rot2(p.cz, p.sz, hJ, hJm);
+        rot2(p.cz, p.sz, tJ, tJm);
+        w.H(R, J) = hJ;
+        w.T(R, J) = tJ;
+        w.H(J, p.jc) = 0.0;
+        if (R == p.jc) {
+          // the column's last pair: H(J-2, J-1), T(J-2, J-1) final; column jc done
+          w.H(R, J - 1) = hJm;
+          w.T(R, J - 1) = tJm;
+          w.H(J - 1, p.jc) = p.r;
+        } else {
+          double x0 = w.H(J - 1, R), x1 = w.H(J, R);
+          rot2(p.c, p.sn, x0, x1);
+          w.H(J, R) = x1;
+          a_h01 = hJm; a_t01 = tJm; a_h10 = x0;  // entries of the next pair's blocks
+        }
+        if (!nextsame) { w.H(J - 1, J - 1) = p.h00; w.T(J - 1, J - 1) = p.t00; }
+        w.H(J, J - 1) = p.h10; w.H(J - 1, J) = p.h01; w.H(J, J) = p.h11;
+        w.T(J - 1, J) = p.t01; w.T(J, J - 1) = 0.0; w.T(J, J) = p.rz;
+      }
+      // (c) the next pair
+      if (kjr >= 0) {
+        const int J = kjr, jc = kjc;
+        double a0, b0, t00, t01, t11, h00, h10, h01, h11;
+        a0 = w.H(J - 1, jc);
+        t00 = w.T(J - 1, J - 1);
+        h00 = w.H(J - 1, J - 1);
+        if (nextsame) {
+          b0 = p.r; t01 = a_t01; t11 = p.t00; h10 = a_h10; h01 = a_h01; h11 = p.h00;
+        } else {
+          b0 = w.H(J, jc); t01 = w.T(J - 1, J); t11 = w.T(J, J);
+          h10 = w.H(J, J - 1); h01 = w.H(J - 1, J); h11 = w.H(J, J);
+        }
+        HrPair q;
+        q.jc = jc; q.jr = J;
+        lartg(a0, b0, q.c, q.sn, q.r);
+        const double u10 = -q.sn * t00, u11 = -q.sn * t01 + q.c * t11;
+        lartg(u11, u10, q.cz, q.sz, q.rz);
+        rot2(q.c, q.sn, h00, h10);
+        rot2(q.c, q.sn, h01, h11);
+        rot2(q.cz, q.sz, h01, h00);
+        rot2(q.cz, q.sz, h11, h10);
+        q.h00 = h00; q.h10 = h10; q.h01 = h01; q.h11 = h11;
+        double u00 = q.c * t00, u01 = q.c * t01 + q.sn * t11;
+        rot2(q.cz, q.sz, u01, u00);
+        q.t00 = u00; q.t01 = u01;
+        double* sl = slot + 4 * (phase & 1);
+        sl[0] = q.c; sl[1] = q.sn; sl[2] = q.cz; sl[3] = q.sz;
+        p = q;
+      }
+    }
+    if (kjr >= 0) { p.jc = kjc; p.jr = kjr; x.count(2); } else { p.jc = -1; p.jr = -1; }
+    x.sync();
+    ++phase;
+  };
+  for (int jc = 0; jc < m - 2; ++jc) {
+    for (int jr = m - 1; jr >= jc + 2; --jr) run_phase(jc, jr);
+    run_phase(-1, -1);  // the column's last pair
+  }
+}
+
 template <class X>
 QZ_HD void cta_aed(X& x, WinState& w, double s, double* sr, double* si_, double* sb, int maxit, int nskip = 0,
                    bool swapfail = false, double* msscr = nullptr) {
@@ -413,60 +531,7 @@ QZ_HD void cta_aed(X& x, WinState& w, double s, double* sr, double* si_, double*
     x.sync();
   }
   x.stamp(3);
-  // ---- Hessenberg-triangular re-reduction of the leading m x m block
-  //      by Givens rotations (the job of DGGHRD at qzearly.f:449).  Each
-  //      pair (row rotation zeroing H(jr, jc), column rotation removing the
-  //      T(jr, jr-1) it creates) is computed by every thread from the 2x2
-  //      block of T; the block thread transforms the 2x2 blocks of H and T
-  //      that both rotations touch, every thread its indices of the disjoint
-  //      rest: two barriers per pair ----
-  for (int jc = 0; jc < m - 2; ++jc) {
-    for (int jr = m - 1; jr >= jc + 2; --jr) {
-      x.count(2);
-      double c, sn, r;
-      lartg(w.H(jr - 1, jc), w.H(jr, jc), c, sn, r);
-      // T after the row rotation: (jr, jr-1) fill, (jr, jr) updated
-      const double t00 = w.T(jr - 1, jr - 1), t01 = w.T(jr - 1, jr), t11 = w.T(jr, jr);
-      const double u10 = -sn * t00, u11 = -sn * t01 + c * t11;
-      double cz, sz, rz;
-      lartg(u11, u10, cz, sz, rz);  // pair (col jr, col jr-1): zero T(jr, jr-1)
-      double hb[4], tb2[2];
-      const bool bt = block_thread(x);
-      if (bt) {
-        // H(jr-1..jr, jr-1..jr): row rotation, then column rotation
-        double h00 = w.H(jr - 1, jr - 1), h10 = w.H(jr, jr - 1), h01 = w.H(jr - 1, jr), h11 = w.H(jr, jr);
-        rot2(c, sn, h00, h10);
-        rot2(c, sn, h01, h11);
-        rot2(cz, sz, h01, h00);
-        rot2(cz, sz, h11, h10);
-        hb[0] = h00; hb[1] = h10; hb[2] = h01; hb[3] = h11;
-        // T(jr-1, jr-1..jr) after both (row jr of the block is (0, rz))
-        double u00 = c * t00, u01 = c * t01 + sn * t11;
-        rot2(cz, sz, u01, u00);
-        tb2[0] = u00; tb2[1] = u01;
-      }
-      x.sync();
-      // far parts by index.  Row rotation: H rows jr-1, jr at columns
-      // jc+1..jr-2 and jr+1..n-1, T rows jr-1, jr at columns jr+1..n-1, Q
-      // columns jr-1, jr.  Column rotation (col jr, col jr-1): H rows 0..jr-2
-      // and jr+1..m-1, T rows 0..jr-2, Z columns.
-      for (int t = x.tid; t < n; t += x.nt) {
-        if ((t >= jc + 1 && t <= jr - 2) || t >= jr + 1) rot_vec(c, sn, &w.H(jr - 1, t), 1);
-        if (t >= jr + 1) rot_vec(c, sn, &w.T(jr - 1, t), 1);
-        if (w.wantq) rot_vec(c, sn, &w.Q(t, jr - 1), w.Q.ld);
-        if (t <= jr - 2 || (t >= jr + 1 && t < m)) rot_vec(cz, sz, &w.H(t, jr), -(int64_t)w.H.ld);
-        if (t <= jr - 2) rot_vec(cz, sz, &w.T(t, jr), -(int64_t)w.T.ld);
-        if (w.wantz) rot_vec(cz, sz, &w.Z(t, jr), -(int64_t)w.Z.ld);
-      }
-      if (bt) {
-        w.H(jr - 1, jc) = r; w.H(jr, jc) = 0.0;
-        w.H(jr - 1, jr - 1) = hb[0]; w.H(jr, jr - 1) = hb[1]; w.H(jr - 1, jr) = hb[2]; w.H(jr, jr) = hb[3];
-        w.T(jr - 1, jr - 1) = tb2[0]; w.T(jr - 1, jr) = tb2[1];
-        w.T(jr, jr - 1) = 0.0; w.T(jr, jr) = rz;
-      }
-      x.sync();
-    }
-  }
+  cta_hessred(x, w, m);
   x.stamp(4);
 }
 
