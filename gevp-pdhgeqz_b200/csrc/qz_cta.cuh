@@ -941,6 +941,92 @@ QZ_HD void small_qr_q(double* X, double* Q) {
   }
 }
 
+// Double-double arithmetic (a value is hi + lo with |lo| <= ulp(hi)/2),
+// built from the error-free transformations TwoSum (Knuth) and TwoProd by
+// FMA (Dekker's product in its FMA form).  Used only where a swap of
+// nearby eigenvalues needs its orthogonal factors to more than working
+// precision.
+struct DD {
+  double hi, lo;
+};
+QZ_HD DD dd_from(double a) { return DD{a, 0.0}; }
+QZ_HD DD dd_add(DD a, DD b) {
+  const double s = a.hi + b.hi, z = s - a.hi;
+  const double e = (a.hi - (s - z)) + (b.hi - z) + a.lo + b.lo;
+  const double h = s + e;
+  return DD{h, e - (h - s)};
+}
+QZ_HD DD dd_neg(DD a) { return DD{-a.hi, -a.lo}; }
+QZ_HD DD dd_mul(DD a, DD b) {
+  const double p = a.hi * b.hi;
+  const double e = fma(a.hi, b.hi, -p) + (a.hi * b.lo + a.lo * b.hi);
+  const double h = p + e;
+  return DD{h, e - (h - p)};
+}
+// quotient: the double quotient corrected by one Newton step on the residual
+QZ_HD DD dd_div(DD a, DD b) {
+  const double q = a.hi / b.hi;
+  const DD r = dd_add(a, dd_neg(dd_mul(b, dd_from(q))));
+  const double q2 = r.hi / b.hi;
+  const double h = q + q2;
+  return DD{h, q2 - (h - q)};
+}
+QZ_HD DD dd_sqrt(DD a) {
+  if (!(a.hi > 0.0)) return DD{0.0, 0.0};
+  const double x = sqrt(a.hi);
+  const DD r = dd_add(a, dd_neg(dd_mul(dd_from(x), dd_from(x))));
+  const double c = r.hi / (2.0 * x);
+  const double h = x + c;
+  return DD{h, c - (h - x)};
+}
+
+// small_qr_q in double-double: Householder QR of the M x K matrix X
+// (double input), Q (M x M) accumulated in double-double and rounded.
+template <int M, int K>
+QZ_HD void small_qr_q_dd(const double* X0, double* Qout) {
+  DD X[M * K], Q[M * M];
+#pragma unroll
+  for (int i = 0; i < M * K; ++i) X[i] = dd_from(X0[i]);
+#pragma unroll
+  for (int i = 0; i < M * M; ++i) Q[i] = dd_from((i % (M + 1) == 0) ? 1.0 : 0.0);
+#pragma unroll
+  for (int c = 0; c < K; ++c) {
+    DD nrm2 = dd_from(0.0);
+#pragma unroll
+    for (int i = c; i < M; ++i) nrm2 = dd_add(nrm2, dd_mul(X[i + M * c], X[i + M * c]));
+    if (nrm2.hi == 0.0) continue;
+    const DD nrm = dd_sqrt(nrm2);
+    const DD alpha = X[c + M * c];
+    const DD beta = (alpha.hi >= 0.0) ? dd_neg(nrm) : nrm;
+    const DD am = dd_add(alpha, dd_neg(beta));
+    DD v[M];
+    v[0] = dd_from(1.0);
+#pragma unroll
+    for (int i = c + 1; i < M; ++i) v[i - c] = dd_div(X[i + M * c], am);
+    const DD tau = dd_div(dd_add(beta, dd_neg(alpha)), beta);
+#pragma unroll
+    for (int j = c; j < K; ++j) {
+      DD t = dd_from(0.0);
+#pragma unroll
+      for (int i = c; i < M; ++i) t = dd_add(t, dd_mul(v[i - c], X[i + M * j]));
+      t = dd_mul(t, tau);
+#pragma unroll
+      for (int i = c; i < M; ++i) X[i + M * j] = dd_add(X[i + M * j], dd_neg(dd_mul(t, v[i - c])));
+    }
+#pragma unroll
+    for (int i = 0; i < M; ++i) {
+      DD t = dd_from(0.0);
+#pragma unroll
+      for (int r = c; r < M; ++r) t = dd_add(t, dd_mul(Q[i + M * r], v[r - c]));
+      t = dd_mul(t, tau);
+#pragma unroll
+      for (int r = c; r < M; ++r) Q[i + M * r] = dd_add(Q[i + M * r], dd_neg(dd_mul(t, v[r - c])));
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < M * M; ++i) Qout[i] = Q[i].hi + Q[i].lo;
+}
+
 // Gaussian elimination with row pivoting on an S x S system (S <= 8,
 // column-major, ld S): the pivot of column k is the largest entry of that
 // column at or below the diagonal, so the search is S - k compares (complete
@@ -1011,62 +1097,61 @@ QZ_HD bool small_solve_cp(double* A, double* rhs, double smin) {
 // Qs^T (Hb, Tb) Zs with the new lower-left N1 x N2 block exactly zero.
 // Returns false if the swap fails the weak stability test (then nothing
 // is applied).
+// The Kronecker form of the swap's Sylvester system: unknowns vec(R),
+// vec(L) (N1 x N2 each), rows of the A- then the B-equations.
 template <int N1, int N2>
-QZ_HD bool swap_compute(MatV Hb, MatV Tb, double* S2, double* T2, double* Qs, double* Zs, double ulp,
-                        double smlnum) {
-  constexpr int M = N1 + N2, NQ = N1 * N2, NS = 2 * NQ;
-  double fn = 0.0;
+QZ_HD void swap_system(MatV Hb, MatV Tb, double* A, double* rhs) {
+  constexpr int NQ = N1 * N2, NS = 2 * NQ;
 #pragma unroll
-  for (int c = 0; c < M; ++c)
+  for (int i = 0; i < NS * NS; ++i) A[i] = 0.0;
 #pragma unroll
-    for (int r = 0; r < M; ++r) fn += Hb(r, c) * Hb(r, c) + Tb(r, c) * Tb(r, c);
-  fn = sqrt(fn);
-  const double thresh = dmax(20.0 * ulp * fn, smlnum);
+  for (int j = 0; j < N2; ++j)
+#pragma unroll
+    for (int i = 0; i < N1; ++i) {
+      const int row = i + N1 * j;
+#pragma unroll
+      for (int k = 0; k < N1; ++k) {
+        A[row + NS * (k + N1 * j)] += Hb(i, k);
+        A[(row + NQ) + NS * (k + N1 * j)] += Tb(i, k);
+      }
+#pragma unroll
+      for (int k = 0; k < N2; ++k) {
+        A[row + NS * (NQ + i + N1 * k)] -= Hb(N1 + k, N1 + j);
+        A[(row + NQ) + NS * (NQ + i + N1 * k)] -= Tb(N1 + k, N1 + j);
+      }
+      rhs[row] = -Hb(i, N1 + j);
+      rhs[row + NQ] = -Tb(i, N1 + j);
+    }
+}
+
+// From the solution x = [vec R; vec L]: Zs, Qs (orthogonal factors of [R; I]
+// and [L; I]) and S2 = Qs^T Hb Zs, T2 = Qs^T Tb Zs; returns the squared
+// Frobenius norm of the new lower-left N1 x N2 blocks.
+template <int N1, int N2>
+QZ_HD double swap_apply(MatV Hb, MatV Tb, const double* x, double* S2, double* T2, double* Qs, double* Zs,
+                        bool dd = false) {
+  constexpr int M = N1 + N2, NQ = N1 * N2;
   double XR[M * N2], XL[M * N2];
-  {
-    double A[NS * NS];
-    double rhs[NS];
 #pragma unroll
-    for (int i = 0; i < NS * NS; ++i) A[i] = 0.0;
+  for (int j = 0; j < N2; ++j) {
 #pragma unroll
-    for (int j = 0; j < N2; ++j)
+    for (int i = 0; i < N1; ++i) {
+      XR[i + M * j] = x[i + N1 * j];
+      XL[i + M * j] = x[NQ + i + N1 * j];
+    }
 #pragma unroll
-      for (int i = 0; i < N1; ++i) {
-        const int row = i + N1 * j;
-#pragma unroll
-        for (int k = 0; k < N1; ++k) {
-          A[row + NS * (k + N1 * j)] += Hb(i, k);
-          A[(row + NQ) + NS * (k + N1 * j)] += Tb(i, k);
-        }
-#pragma unroll
-        for (int k = 0; k < N2; ++k) {
-          A[row + NS * (NQ + i + N1 * k)] -= Hb(N1 + k, N1 + j);
-          A[(row + NQ) + NS * (NQ + i + N1 * k)] -= Tb(N1 + k, N1 + j);
-        }
-        rhs[row] = -Hb(i, N1 + j);
-        rhs[row + NQ] = -Tb(i, N1 + j);
-      }
-    small_solve_cp<NS>(A, rhs, dmax(ulp * fn * 1e-3, smlnum));
-#pragma unroll
-    for (int i = 0; i < NS; ++i)
-      if (!isfinite(rhs[i])) return false;
-    // [R; I] and [L; I] (M x N2)
-#pragma unroll
-    for (int j = 0; j < N2; ++j) {
-#pragma unroll
-      for (int i = 0; i < N1; ++i) {
-        XR[i + M * j] = rhs[i + N1 * j];
-        XL[i + M * j] = rhs[NQ + i + N1 * j];
-      }
-#pragma unroll
-      for (int i = 0; i < N2; ++i) {
-        XR[N1 + i + M * j] = (i == j) ? 1.0 : 0.0;
-        XL[N1 + i + M * j] = (i == j) ? 1.0 : 0.0;
-      }
+    for (int i = 0; i < N2; ++i) {
+      XR[N1 + i + M * j] = (i == j) ? 1.0 : 0.0;
+      XL[N1 + i + M * j] = (i == j) ? 1.0 : 0.0;
     }
   }
-  small_qr_q<M, N2>(XR, Zs);
-  small_qr_q<M, N2>(XL, Qs);
+  if (dd) {
+    small_qr_q_dd<M, N2>(XR, Zs);
+    small_qr_q_dd<M, N2>(XL, Qs);
+  } else {
+    small_qr_q<M, N2>(XR, Zs);
+    small_qr_q<M, N2>(XL, Qs);
+  }
   double blk[M * M], tmp[M * M];
 #pragma unroll
   for (int c = 0; c < M; ++c)
@@ -1085,11 +1170,136 @@ QZ_HD bool swap_compute(MatV Hb, MatV Tb, double* S2, double* T2, double* Qs, do
   for (int j = 0; j < N2; ++j)
 #pragma unroll
     for (int i = N2; i < M; ++i) ll += S2[i + M * j] * S2[i + M * j] + T2[i + M * j] * T2[i + M * j];
+  return ll;
+}
+
+// The retry of a swap that failed the weak stability test (rare), from
+// the block itself: the Sylvester solution refined once with its residual
+// b - K x in twice the working precision (exact products by FMA,
+// compensated summation: the Dot2 algorithm of Ogita, Rump and Oishi,
+// SIAM J. Sci. Comput. 26 (2005)), and the orthogonal factors formed in
+// double-double.  For nearby eigenvalues |x| is large: in working
+// precision the residual cannot fall below eps |K| |x|, and a Householder
+// QR of [R; I] loses the subspace by about eps |R|, either of which can
+// push an acceptable swap over the threshold.  Not inlined, and its
+// outputs go straight to the caller's (shared) arrays, so its temporaries
+// do not weigh on the registers of the kernels that swap.
+template <int N1, int N2>
+QZ_NOINLINE bool swap_retry(MatV Hb, MatV Tb, double* S2, double* T2, double* Qs, double* Zs, double ulp,
+                            double smlnum) {
+  constexpr int M = N1 + N2, NQ = N1 * N2, NS = 2 * NQ;
+  double fn = 0.0;
+  for (int c = 0; c < M; ++c)
+    for (int r = 0; r < M; ++r) fn += Hb(r, c) * Hb(r, c) + Tb(r, c) * Tb(r, c);
+  fn = sqrt(fn);
+  const double thresh = dmax(20.0 * ulp * fn, smlnum);
+  const double smin = dmax(ulp * fn * 1e-3, smlnum);
+  double x[NS], A[NS * NS], r[NS];
+  swap_system<N1, N2>(Hb, Tb, A, x);
+  small_solve_cp<NS>(A, x, smin);
+  swap_system<N1, N2>(Hb, Tb, A, r);
+  for (int i = 0; i < NS; ++i) {
+    double sum = r[i], comp = 0.0;
+    for (int j = 0; j < NS; ++j) {
+      const double p = -A[i + NS * j] * x[j];
+      const double q = fma(-A[i + NS * j], x[j], -p);
+      const double t = sum + p, z = t - sum;
+      comp += ((sum - (t - z)) + (p - z)) + q;
+      sum = t;
+    }
+    r[i] = sum + comp;
+  }
+  small_solve_cp<NS>(A, r, smin);
+  for (int i = 0; i < NS; ++i) {
+    x[i] += r[i];
+    if (!isfinite(x[i])) return false;
+  }
+  const double ll = swap_apply<N1, N2>(Hb, Tb, x, S2, T2, Qs, Zs, true);
   if (!(sqrt(ll) <= thresh)) return false;
+  for (int j = 0; j < N2; ++j)
+    for (int i = N2; i < M; ++i) { S2[i + M * j] = 0.0; T2[i + M * j] = 0.0; }
+  return true;
+}
+
+// 1: accepted; 0: rejected; -1: failed the stability test in working
+// precision (swap_retry may still accept it)
+template <int N1, int N2>
+QZ_HD int swap_compute_try(MatV Hb, MatV Tb, double* S2, double* T2, double* Qs, double* Zs, double ulp,
+                           double smlnum) {
+  constexpr int M = N1 + N2, NQ = N1 * N2, NS = 2 * NQ;
+  double fn = 0.0;
+#pragma unroll
+  for (int c = 0; c < M; ++c)
+#pragma unroll
+    for (int r = 0; r < M; ++r) fn += Hb(r, c) * Hb(r, c) + Tb(r, c) * Tb(r, c);
+  fn = sqrt(fn);
+  const double thresh = dmax(20.0 * ulp * fn, smlnum);
+  const double smin = dmax(ulp * fn * 1e-3, smlnum);
+  double x[NS];
+  {
+    double A[NS * NS];
+    swap_system<N1, N2>(Hb, Tb, A, x);
+    small_solve_cp<NS>(A, x, smin);
+  }
+#pragma unroll
+  for (int i = 0; i < NS; ++i)
+    if (!isfinite(x[i])) return 0;
+  double ll = swap_apply<N1, N2>(Hb, Tb, x, S2, T2, Qs, Zs);
+  if (!(sqrt(ll) <= thresh)) return -1;
 #pragma unroll
   for (int j = 0; j < N2; ++j)
 #pragma unroll
     for (int i = N2; i < M; ++i) { S2[i + M * j] = 0.0; T2[i + M * j] = 0.0; }
+  return 1;
+}
+
+template <int N1, int N2>
+QZ_HD bool swap_compute(MatV Hb, MatV Tb, double* S2, double* T2, double* Qs, double* Zs, double ulp,
+                        double smlnum) {
+  const int r = swap_compute_try<N1, N2>(Hb, Tb, S2, T2, Qs, Zs, ulp, smlnum);
+  if (r < 0) return swap_retry<N1, N2>(Hb, Tb, S2, T2, Qs, Zs, ulp, smlnum);
+  return r > 0;
+}
+
+// Swap of two 1x1 blocks by two rotations (the direct 1x1 case of
+// Kagstrom and Poromaa's swapping): for the block pencil ([a b; 0 c],
+// [d e; 0 f]) the right rotation's first column is the eigenvector of the
+// trailing eigenvalue, (f S - c T) z = 0, i.e. z ~ (f b - c e, -(f a - c d));
+// S z and T z are then parallel and the left rotation maps the larger
+// (relative to its matrix) onto e1.  The weak stability test of the
+// general path decides acceptance; close eigenvalues make z inaccurate, and
+// the caller then takes the generalized Sylvester path.  Same outputs as
+// swap_compute<1, 1>.
+QZ_HD bool swap_compute11(MatV Hb, MatV Tb, double* S2, double* T2, double* Qs, double* Zs, double ulp,
+                          double smlnum) {
+  const double a = Hb(0, 0), b = Hb(0, 1), c = Hb(1, 1), d = Tb(0, 0), e = Tb(0, 1), f = Tb(1, 1);
+  const double fn = sqrt(a * a + b * b + c * c + Hb(1, 0) * Hb(1, 0) + d * d + e * e + f * f + Tb(1, 0) * Tb(1, 0));
+  const double thresh = dmax(20.0 * ulp * fn, smlnum);
+  double hm = dmax(fabs(a), dmax(fabs(b), fabs(c))), tm = dmax(fabs(d), dmax(fabs(e), fabs(f)));
+  hm = (hm > 0.0 && isfinite(hm)) ? 1.0 / hm : 1.0;
+  tm = (tm > 0.0 && isfinite(tm)) ? 1.0 / tm : 1.0;
+  const double as = a * hm, bs = b * hm, cs = c * hm, ds = d * tm, es = e * tm, fs = f * tm;
+  const double F = fs * as - cs * ds, G = fs * bs - cs * es;
+  double cz, sz, rr;
+  lartg(G, -F, cz, sz, rr);
+  // S z, T z (scaled)
+  const double s0 = as * cz + bs * sz, s1 = cs * sz, t0 = ds * cz + es * sz, t1 = fs * sz;
+  const bool use_s = s0 * s0 + s1 * s1 >= t0 * t0 + t1 * t1;
+  double cq, sq, rq;
+  lartg(use_s ? s0 : t0, use_s ? s1 : t1, cq, sq, rq);
+  Zs[0] = cz; Zs[1] = sz; Zs[2] = -sz; Zs[3] = cz;
+  Qs[0] = cq; Qs[1] = sq; Qs[2] = -sq; Qs[3] = cq;
+  // S2 = Q^T S Z, T2 = Q^T T Z (S, T upper triangular 2x2 blocks)
+  const double sz0 = a * cz + b * sz, sz1 = c * sz, sz2 = -a * sz + b * cz, sz3 = c * cz;  // S Z columns
+  const double tz0 = d * cz + e * sz, tz1 = f * sz, tz2 = -d * sz + e * cz, tz3 = f * cz;
+  S2[0] = cq * sz0 + sq * sz1; S2[1] = -sq * sz0 + cq * sz1;
+  S2[2] = cq * sz2 + sq * sz3; S2[3] = -sq * sz2 + cq * sz3;
+  T2[0] = cq * tz0 + sq * tz1; T2[1] = -sq * tz0 + cq * tz1;
+  T2[2] = cq * tz2 + sq * tz3; T2[3] = -sq * tz2 + cq * tz3;
+  const double ll = S2[1] * S2[1] + T2[1] * T2[1];
+  if (!(sqrt(ll) <= thresh)) return false;
+  S2[1] = 0.0;
+  T2[1] = 0.0;
   return true;
 }
 
@@ -1106,11 +1316,21 @@ QZ_HD bool cta_swap_t(X& x, WinState& w, int j1, bool restd) {
   x.count(1);
   if (x.tid == 0) {
     double S2[M * M], T2[M * M], Qs[M * M], Zs[M * M];
-    bool ok = swap_compute<N1, N2>(MatV{&w.H(j1, j1), w.H.ld}, MatV{&w.T(j1, j1), w.T.ld}, S2, T2, Qs, Zs,
-                                   w.tol.ulp, w.tol.smlnum);
+    const MatV hb{&w.H(j1, j1), w.H.ld}, tb{&w.T(j1, j1), w.T.ld};
+    int res;
+    if constexpr (N1 == 1 && N2 == 1)
+      // two rotations; the Sylvester path where they fail the stability test
+      res = swap_compute11(hb, tb, S2, T2, Qs, Zs, w.tol.ulp, w.tol.smlnum)
+                ? 1
+                : swap_compute_try<1, 1>(hb, tb, S2, T2, Qs, Zs, w.tol.ulp, w.tol.smlnum);
+    else
+      res = swap_compute_try<N1, N2>(hb, tb, S2, T2, Qs, Zs, w.tol.ulp, w.tol.smlnum);
+    bool ok = res > 0;
     if (ok) {
 #pragma unroll
       for (int i = 0; i < M * M; ++i) { sQ[i] = Qs[i]; sZ[i] = Zs[i]; sS[i] = S2[i]; sT[i] = T2[i]; }
+    } else if (res < 0) {
+      ok = swap_retry<N1, N2>(hb, tb, sS, sT, sQ, sZ, w.tol.ulp, w.tol.smlnum);
     }
     x.si[2] = ok ? 1 : 0;
   }

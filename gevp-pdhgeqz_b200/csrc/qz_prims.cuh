@@ -15,8 +15,10 @@
 
 #if defined(__CUDACC__)
 #define QZ_HD __host__ __device__ __forceinline__
+#define QZ_NOINLINE __host__ __device__ __noinline__
 #else
 #define QZ_HD inline
+#define QZ_NOINLINE inline
 #endif
 
 namespace qz {

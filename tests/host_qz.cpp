@@ -248,6 +248,18 @@ struct HostBK {
 extern "C" {
 
 void host_set_pipe(int on) { g_pipe = on != 0; }
+
+// Swap of the 1x1 blocks of the 2x2 pencil (S, T) (column-major, upper
+// triangular): out = {ok, S2[4], T2[4], Q[4], Z[4]}; general = 1 takes the
+// generalized Sylvester path, 0 the two-rotation path.
+void host_swap11(const double* S, const double* T, int general, double* out) {
+  double S2[4], T2[4], Qs[4], Zs[4];
+  double s[4] = {S[0], S[1], S[2], S[3]}, t[4] = {T[0], T[1], T[2], T[3]};
+  const bool ok = general ? swap_compute<1, 1>(MatV{s, 2}, MatV{t, 2}, S2, T2, Qs, Zs, DBL_EPSILON, DBL_MIN)
+                          : swap_compute11(MatV{s, 2}, MatV{t, 2}, S2, T2, Qs, Zs, DBL_EPSILON, DBL_MIN);
+  out[0] = ok ? 1.0 : 0.0;
+  for (int i = 0; i < 4; ++i) { out[1 + i] = S2[i]; out[5 + i] = T2[i]; out[9 + i] = Qs[i]; out[13 + i] = Zs[i]; }
+}
 // steps of the last pipelined sweep that the far part completed (far_done)
 int host_pipe_far_done() { return g_pipebuf.far_done; }
 

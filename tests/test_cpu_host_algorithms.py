@@ -40,6 +40,8 @@ def host(tmp_path_factory):
     L.host_set_pipe.argtypes = [ctypes.c_int]
     L.host_set_pipe.restype = None
     L.host_pipe_far_done.restype = ctypes.c_int
+    L.host_swap11.argtypes = [_pd, _pd, ctypes.c_int, _pd]
+    L.host_swap11.restype = None
     return L
 
 
@@ -355,3 +357,47 @@ def test_host_pipelined_solve(pkg, lapack, host):
     assert info == 0
     assert lapack.schur_structure_ok(S, P)
     _check(lapack, H, T, S, P, Q, Z, (ar, ai, be))
+
+
+def _swap11_cases():
+    rng = np.random.default_rng(5)
+    cases = [rng.standard_normal(6) for _ in range(200)]
+    cases += [np.array([1.0, 2.0, 1.0, 1.0, 3.0, 1.0]),      # equal eigenvalues
+              np.array([1.0, 2.0, 3.0, 1.0, 0.5, 0.0]),      # infinite eigenvalue last
+              np.array([1.0, 2.0, 3.0, 0.0, 0.5, 2.0]),      # infinite eigenvalue first
+              np.array([0.0, 2.0, 3.0, 1.0, 0.5, 2.0]),      # zero eigenvalue first
+              np.array([1e-200, 1.0, 1e200, 1.0, 1e-150, 1.0]),
+              np.array([2.0, 0.0, 3.0, 1.0, 0.0, 1.0])]      # already diagonal
+    return cases
+
+
+def test_host_swap11_two_rotations(host):
+    """The two-rotation swap of 1x1 blocks: orthogonal factors, upper
+    triangular result with the eigenvalues exchanged, Q^T (S,T) Z = (S2,T2)
+    to rounding, and the same acceptance as the generalized Sylvester
+    path."""
+    eps = np.finfo(float).eps
+    for a, b, c, d, e, f in _swap11_cases():
+        S = np.array([[a, b], [0.0, c]], order="F")
+        T = np.array([[d, e], [0.0, f]], order="F")
+        out = np.zeros(17)
+        host.host_swap11(_p(S), _p(T), 0, _p(out))
+        ref = np.zeros(17)
+        host.host_swap11(_p(S), _p(T), 1, _p(ref))
+        # the two-rotation path may reject a swap of close eigenvalues that
+        # the Sylvester path accepts (the library then falls back to it);
+        # it never accepts one the Sylvester path rejects
+        assert out[0] <= ref[0] or max(abs(S).max(), abs(T).max()) > 1e100
+        if out[0] == 0:
+            continue
+        S2, T2 = out[1:5].reshape(2, 2, order="F"), out[5:9].reshape(2, 2, order="F")
+        Q, Z = out[9:13].reshape(2, 2, order="F"), out[13:17].reshape(2, 2, order="F")
+        assert np.allclose(Q.T @ Q, np.eye(2), atol=4 * eps) and np.allclose(Z.T @ Z, np.eye(2), atol=4 * eps)
+        fn = np.hypot(np.linalg.norm(S), np.linalg.norm(T))
+        assert np.linalg.norm(Q.T @ S @ Z - S2) <= 50 * eps * fn
+        assert np.linalg.norm(Q.T @ T @ Z - T2) <= 50 * eps * fn
+        assert S2[1, 0] == 0.0 and T2[1, 0] == 0.0
+        # eigenvalue (c, f) now leads: chordal distance of (S2[0,0], T2[0,0]) to (c, f)
+        u, v = np.array([S2[0, 0], T2[0, 0]]), np.array([c, f])
+        chord = abs(u[0] * v[1] - u[1] * v[0]) / max(np.linalg.norm(u) * np.linalg.norm(v), 1e-300)
+        assert chord <= 1e-10 or np.linalg.norm(v) == 0.0
