@@ -61,6 +61,7 @@ EXPORTS = (
     "b200qz_batched_seconds", "b200qz_batched_autotune", "b200qz_batched_config",
     "b200qz_solve_batched_noalloc", "b200qz_policy_nparams", "b200qz_set_policy", "b200qz_policy_features",
     "b200qz_mlp_forward", "b200qz_mlp_backward", "b200qz_mlp_train", "b200qz_update_split",
+    "b200qz_gghrd_dev", "b200qz_gghrd_host", "pdgghrd_",
 )
 
 STAT_NAMES = ("seconds", "iters", "aeds", "aed_deflations", "sweeps", "chains", "windows",
@@ -145,6 +146,12 @@ def lib() -> ctypes.CDLL:
     for f in ("b200qz_ggbak_dev", "b200qz_ggbak_host"):
         getattr(L, f).argtypes = [_vp, _c, _c, _i, _i, _i, _pd, _pd, _i, _vp, _i]
         getattr(L, f).restype = _i
+    for f in ("b200qz_gghrd_dev", "b200qz_gghrd_host"):
+        getattr(L, f).argtypes = [_vp, _c, _c, _i, _i, _i] + [_vp, _i] * 4
+        getattr(L, f).restype = _i
+    L.pdgghrd_.argtypes = [ctypes.c_char_p, ctypes.c_char_p, _pi, _pi, _pi, _vp, _pi, _vp, _pi, _vp, _pi, _vp, _pi,
+                           _pd, _pi, _pi, ctypes.c_size_t, ctypes.c_size_t]
+    L.pdgghrd_.restype = None
     _lib = L
     return L
 
@@ -337,6 +344,28 @@ class Solver:
                                       max(1, Za.shape[0]), _p(ar), _p(ai), _p(be), ctypes.byref(m),
                                       ctypes.byref(pl), ctypes.byref(pr), ctypes.byref(info))
         return ar[:n], ai[:n], be[:n], m.value, pl.value, pr.value, info.value, ret
+
+    def gghrd(self, A, B, Q=None, Z=None, compq="I", compz="I", ilo=1, ihi=None):
+        """Reduce the host pencil (A, B), B upper triangular, to
+        Hessenberg-triangular form in place on the GPU (DGGHRD semantics):
+        Q^T A Z = H, Q^T B Z = T.  compq/compz 'N', 'I' or 'V' (Q, Z
+        updated in place; with 'I' they need not be set).  Returns the C
+        return code (0, -i for an illegal argument, 10001)."""
+        n = A.shape[0]
+        ihi = n if ihi is None else ihi
+        dummy = np.zeros((1, 1), order="F")
+        Qa = Q if Q is not None else dummy
+        Za = Z if Z is not None else dummy
+        return lib().b200qz_gghrd_host(self._h, compq.encode(), compz.encode(), n, ilo, ihi, _vp(A.ctypes.data),
+                                       max(1, A.shape[0]), _vp(B.ctypes.data), max(1, B.shape[0]),
+                                       _vp(Qa.ctypes.data), max(1, Qa.shape[0]), _vp(Za.ctypes.data),
+                                       max(1, Za.shape[0]))
+
+    def gghrd_device(self, a_ptr, b_ptr, q_ptr, z_ptr, n, ld, compq="I", compz="I", ilo=1, ihi=None):
+        """The same on device arrays (column-major, leading dimension ld)."""
+        ihi = n if ihi is None else ihi
+        return lib().b200qz_gghrd_dev(self._h, compq.encode(), compz.encode(), n, ilo, ihi, _vp(a_ptr), ld,
+                                      _vp(b_ptr), ld, _vp(q_ptr), ld, _vp(z_ptr), ld)
 
     def ggbak(self, V, ilo, ihi, lscale, rscale, side="R", job="B"):
         """Back-transform the host matrix V (n x m) in place (DGGBAK

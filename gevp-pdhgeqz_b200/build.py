@@ -18,7 +18,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libb200qz.so")
-SOURCES = ["kernels.cu", "batched.cu", "policy.cu", "ozaki.cu", "balance.cu", "reorder.cu", "capi.cu"]
+SOURCES = ["kernels.cu", "batched.cu", "policy.cu", "ozaki.cu", "balance.cu", "reorder.cu", "hessred.cu", "capi.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -16,6 +16,7 @@
 
 #include "../../include/b200qz.h"
 #include "balance.h"
+#include "hessred.h"
 #include "reorder.h"
 #include "kernels.h"
 #include "ozaki.h"
@@ -126,6 +127,7 @@ struct b200qz_ctx {
   double seconds = 0.0;
   int ka = 0;  // size of the AED factors in Ua/Va
   int kc = 0;  // size of the chase factors in Uc/Vc
+  int hr_win = 128;  // pairs per window of the Hessenberg-triangular reduction
   cudaError_t err = cudaSuccess;
   PhaseTimer timer;
   unsigned long long* dts = nullptr;  // AED phase timestamps (device)
@@ -663,6 +665,7 @@ int b200qz_set_param(b200qz_ctx* c, const char* name, double value) {
   else if (k == "aed_threads") { if (v != 32 && v != 64 && v != 128) return -3; P.aed_threads = v; }
   else if (k == "aed_swap_fail") { if (v != 0 && v != 1) return -3; P.aed_swap_fail = v; }
   else if (k == "aed_ms") { if (v != 0 && v != 1) return -3; P.aed_ms = v; }
+  else if (k == "hr_win") { if (v < 2 || v > qz::kHrMaxWin) return -3; c->hr_win = v; }
   else return -2;
   return 0;
 }
@@ -1309,6 +1312,122 @@ int b200qz_tgsen_host(b200qz_ctx* c, int ijob, int wantq, int wantz, const int* 
   *pr = o.pr;
   *info = o.info;
   return 0;
+}
+
+// ---------------------------------------------------------------------------
+// Hessenberg-triangular reduction (DGGHRD semantics; the reference's
+// PDGGHRD, src/ab2ht/PDGGHRD.f:13).
+// ---------------------------------------------------------------------------
+static int comp_code(char c) { return is(c, 'N') ? 0 : is(c, 'V') ? 1 : is(c, 'I') ? 2 : -1; }
+
+// Argument numbering of DGGHRD: COMPQ 1, COMPZ 2, N 3, ILO 4, IHI 5, LDA 7,
+// LDB 9, LDQ 11, LDZ 13.
+static int gghrd_args(char compq, char compz, int n, int ilo, int ihi, int lda, int ldb, int ldq, int ldz) {
+  const int cq = comp_code(compq), cz = comp_code(compz);
+  if (cq < 0) return -1;
+  if (cz < 0) return -2;
+  if (n < 0) return -3;
+  if (ilo < 1) return -4;
+  if (ihi > n || ihi < ilo - 1) return -5;
+  if (lda < std::max(1, n)) return -7;
+  if (ldb < std::max(1, n)) return -9;
+  if ((cq > 0 && ldq < n) || ldq < 1) return -11;
+  if ((cz > 0 && ldz < n) || ldz < 1) return -13;
+  return 0;
+}
+
+static int gghrd_run(b200qz_ctx* c, int cq, int cz, bool qrows, int n, int ilo, int ihi, double* a, int lda, double* b,
+                     int ldb, double* q, int ldq, double* z, int ldz) {
+  qz::GghrdOut o;
+  const cudaError_t e =
+      qz::gghrd_device(c->stream, cq, cz, qrows, n, ilo - 1, ihi - 1, a, lda, b, ldb, q, ldq, z, ldz, c->hr_win, &o);
+  return e == cudaSuccess ? 0 : 10001;
+}
+
+int b200qz_gghrd_dev(b200qz_ctx* c, char compq, char compz, int n, int ilo, int ihi, double* a, int lda, double* b,
+                     int ldb, double* q, int ldq, double* z, int ldz) {
+  if (!c) return 10001;
+  const int bad = gghrd_args(compq, compz, n, ilo, ihi, lda, ldb, ldq, ldz);
+  if (bad) return bad;
+  if (n == 0) return 0;
+  if (cudaSetDevice(c->device) != cudaSuccess) return 10001;
+  return gghrd_run(c, comp_code(compq), comp_code(compz), false, n, ilo, ihi, a, lda, b, ldb, q, ldq, z, ldz);
+}
+
+// Host arrays: copied in, reduced, copied out (Q, Z only when referenced;
+// an input Q, Z only for COMPQ, COMPZ = 'V').
+static int gghrd_host_impl(b200qz_ctx* c, int cq, int cz, bool qrows, int n, int ilo, int ihi, double* a, int lda,
+                           double* b, int ldb, double* q, int ldq, double* z, int ldz) {
+  if (cudaSetDevice(c->device) != cudaSuccess) return 10001;
+  const size_t nn = (size_t)n * n, w = (size_t)n * sizeof(double);
+  double* d = nullptr;
+  if (cudaMalloc(&d, 4 * nn * sizeof(double)) != cudaSuccess) return 10001;
+  double *da = d, *db = d + nn, *dq = d + 2 * nn, *dz = d + 3 * nn;
+  auto h2d = [&](double* dst, const double* src, int ld) {
+    return cudaMemcpy2DAsync(dst, w, src, (size_t)ld * sizeof(double), w, n, cudaMemcpyHostToDevice, c->stream);
+  };
+  auto d2h = [&](double* dst, int ld, const double* src) {
+    return cudaMemcpy2DAsync(dst, (size_t)ld * sizeof(double), src, w, w, n, cudaMemcpyDeviceToHost, c->stream);
+  };
+  cudaError_t e = h2d(da, a, lda);
+  if (e == cudaSuccess) e = h2d(db, b, ldb);
+  if (e == cudaSuccess && cq == 1) e = h2d(dq, q, ldq);
+  if (e == cudaSuccess && cz == 1) e = h2d(dz, z, ldz);
+  int r = 10001;
+  if (e == cudaSuccess) r = gghrd_run(c, cq, cz, qrows, n, ilo, ihi, da, n, db, n, dq, n, dz, n);
+  if (r == 0) {
+    e = d2h(a, lda, da);
+    if (e == cudaSuccess) e = d2h(b, ldb, db);
+    if (e == cudaSuccess && cq > 0) e = d2h(q, ldq, dq);
+    if (e == cudaSuccess && cz > 0) e = d2h(z, ldz, dz);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) r = 10001;
+  }
+  cudaFree(d);
+  return r;
+}
+
+int b200qz_gghrd_host(b200qz_ctx* c, char compq, char compz, int n, int ilo, int ihi, double* a, int lda, double* b,
+                      int ldb, double* q, int ldq, double* z, int ldz) {
+  if (!c) return 10001;
+  const int bad = gghrd_args(compq, compz, n, ilo, ihi, lda, ldb, ldq, ldz);
+  if (bad) return bad;
+  if (n == 0) return 0;
+  return gghrd_host_impl(c, comp_code(compq), comp_code(compz), false, n, ilo, ihi, a, lda, b, ldb, q, ldq, z, ldz);
+}
+
+// PDGGHRD on a 1x1 grid (src/ab2ht/PDGGHRD.f:13-31): the same argument
+// list with descriptors, a workspace query that returns MB_ in WORK(1)
+// (PDGGHRD.f:243-250), Q returned transposed (row rotations accumulated
+// from the left, as the reference's callers expect: examples/EXRAND2.f:
+// 352-356 transposes it back) and INFO numbering of PDGGHRD.f:278-296.
+void pdgghrd_(const char* compq, const char* compz, const int* n, const int* ilo, const int* ihi, double* a,
+              const int* desca, double* b, const int* descb, double* q, const int* descq, double* z, const int* descz,
+              double* work, const int* lwork, int* info, size_t len_compq, size_t len_compz) {
+  (void)len_compq; (void)len_compz;
+  const int N = *n, ILO = *ilo, IHI = *ihi;
+  *info = 0;
+  if (N <= 1) return;  // quick return before any check (PDGGHRD.f:198)
+  const int mb = desca[4], nb = desca[5];
+  if (*lwork == -1) { work[0] = (double)mb; return; }
+  const int cq = comp_code(*compq), cz = comp_code(*compz);
+  if (cq < 0) *info = -1;
+  else if (cz < 0) *info = -2;
+  else if (N < 0) *info = -3;
+  else if (ILO < 1) *info = -4;
+  else if (IHI > N || IHI < ILO - 1) *info = -5;
+  else if (nb != mb) *info = -6;
+  else if (*lwork < mb) *info = -7;
+  if (*info != 0) return;
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (!g_ctx) {
+    int dev = 0;
+    const char* e = std::getenv("B200QZ_DEVICE");
+    if (e) dev = std::atoi(e);
+    if (b200qz_create(&g_ctx, dev) != 0) { g_ctx = nullptr; *info = 10001; return; }
+  }
+  const int r = gghrd_host_impl(g_ctx, cq, cz, true, N, ILO, IHI, a, desca[8], b, descb[8], q, descq[8], z, descz[8]);
+  if (r != 0) *info = r;
 }
 
 }  // extern "C"

@@ -331,6 +331,37 @@ int b200qz_tgsen_host(b200qz_ctx* ctx, int ijob, int wantq, int wantz, const int
                       double* t, int ldt, double* q, int ldq, double* z, int ldz, double* alphar, double* alphai,
                       double* beta, int* m, double* pl, double* pr, int* info);
 
+/* Hessenberg-triangular reduction (LAPACK DGGHRD semantics; replaces the
+ * reference's PDGGHRD, src/ab2ht/PDGGHRD.f:13, the step before the solve
+ * at examples/EXRAND2.f:334).  B must be upper triangular on entry (its
+ * strict lower triangle is set to zero).  Reduces A to upper Hessenberg
+ * form in columns ilo..ihi-2 (1-based; A is assumed upper triangular
+ * outside rows/columns ilo..ihi) by Givens rotations in LAPACK's order and
+ * sign convention, keeping B upper triangular: Q^T A Z = H, Q^T B Z = T.
+ * compq / compz: 'N' Q / Z not referenced, 'I' set to the orthogonal
+ * factor, 'V' multiplied into the given matrix (Q1 Q, Z1 Z).  The _dev
+ * form takes device arrays, the _host form host arrays.  Returns 0;
+ * -1 compq, -2 compz, -3 n, -4 ilo, -5 ihi, -7 lda, -9 ldb, -11 ldq,
+ * -13 ldz (DGGHRD's argument positions); 10001 on a CUDA error.  The
+ * parameter "hr_win" (b200qz_set_param, 2..160, default 128) sets the
+ * rotation pairs per shared-memory window. */
+int b200qz_gghrd_dev(b200qz_ctx* ctx, char compq, char compz, int n, int ilo, int ihi, double* a, int lda, double* b,
+                     int ldb, double* q, int ldq, double* z, int ldz);
+int b200qz_gghrd_host(b200qz_ctx* ctx, char compq, char compz, int n, int ilo, int ihi, double* a, int lda, double* b,
+                      int ldb, double* q, int ldq, double* z, int ldz);
+
+/* Drop-in for the reference's PDGGHRD on a 1x1 process grid
+ * (src/ab2ht/PDGGHRD.f:13-31): host arrays with ScaLAPACK descriptors
+ * (LLD_ = desc[8]), hidden CHARACTER lengths.  Like the reference, N <= 1
+ * returns at once; LWORK = -1 returns DESCA(MB_) in WORK(1); INFO -1
+ * COMPQ, -2 COMPZ, -3 N, -4 ILO, -5 IHI, -6 MB_ != NB_, -7 LWORK < MB_.
+ * Q is returned transposed, as the reference returns it: on exit Q holds
+ * G Q_in, where G is the product of the row rotations (so with COMPQ = 'I'
+ * the caller's A = Q^T H Z^T). */
+void pdgghrd_(const char* compq, const char* compz, const int* n, const int* ilo, const int* ihi, double* a,
+              const int* desca, double* b, const int* descb, double* q, const int* descq, double* z, const int* descz,
+              double* work, const int* lwork, int* info, size_t len_compq, size_t len_compz);
+
 #ifdef __cplusplus
 }
 #endif

@@ -15,7 +15,9 @@ names:
   eigenvalue-set oracle.
 * ``DTGEVC`` + ``DTGSNA`` -- eigenvectors and reciprocal eigenvalue
   condition numbers used to scale the eigenvalue matching tolerance.
-* ``DGGHRD``  -- Hessenberg-triangular reduction (``qzearly.f:449``).
+* ``DGGHRD``  -- Hessenberg-triangular reduction (``qzearly.f:449``; the
+  semantics of the reference's PDGGHRD, ``src/ab2ht/PDGGHRD.f:13``), and
+  ``DGGHD3``, its blocked form, as the host timing baseline.
 * ``DTGSEN`` -- reordering of a generalized Schur form and the
   projection norms PL/PR (the role of the reference's PDTGSEN,
   ``src/reorder/PDTGSEN.f:1``), through scipy's wrapper of the same
@@ -104,8 +106,26 @@ def dhgeqz(H, T, job="S", compq="I", compz="I", Q=None, Z=None, ilo=1, ihi=None)
     return S, P, ar, ai, be, Qm, Zm, info.value
 
 
-def dgghrd(A, B, compq="I", compz="I"):
-    """LAPACK DGGHRD on (A, B) with B already upper triangular."""
+def dgghrd(A, B, compq="I", compz="I", ilo=1, ihi=None, Q=None, Z=None):
+    """LAPACK DGGHRD on (A, B) with B already upper triangular (1-based
+    ilo/ihi; Q, Z are the input matrices for compq/compz = 'V')."""
+    n = A.shape[0]
+    ihi = n if ihi is None else ihi
+    H = np.array(A, dtype=np.float64, order="F", copy=True)
+    T = np.array(B, dtype=np.float64, order="F", copy=True)
+    Q = np.array(Q if Q is not None else np.eye(n), dtype=np.float64, order="F", copy=True)
+    Z = np.array(Z if Z is not None else np.eye(n), dtype=np.float64, order="F", copy=True)
+    info = ctypes.c_int(0)
+    ld = max(1, n)
+    lib().scipy_dgghrd_(_c(compq.encode()), _c(compz.encode()), _ip(n), _ip(ilo), _ip(ihi),
+                        _dp(H), _ip(ld), _dp(T), _ip(ld), _dp(Q), _ip(ld), _dp(Z), _ip(ld),
+                        ctypes.byref(info), ctypes.c_size_t(1), ctypes.c_size_t(1))
+    return H, T, Q, Z, info.value
+
+
+def dgghd3(A, B, compq="I", compz="I"):
+    """LAPACK DGGHD3 (the blocked Hessenberg-triangular reduction, the
+    host baseline for timing) on (A, B) with B upper triangular."""
     n = A.shape[0]
     H = np.array(A, dtype=np.float64, order="F", copy=True)
     T = np.array(B, dtype=np.float64, order="F", copy=True)
@@ -113,9 +133,16 @@ def dgghrd(A, B, compq="I", compz="I"):
     Z = np.eye(n, order="F")
     info = ctypes.c_int(0)
     ld = max(1, n)
-    lib().scipy_dgghrd_(_c(compq.encode()), _c(compz.encode()), _ip(n), _ip(1), _ip(n),
-                        _dp(H), _ip(ld), _dp(T), _ip(ld), _dp(Q), _ip(ld), _dp(Z), _ip(ld),
-                        ctypes.byref(info), ctypes.c_size_t(1), ctypes.c_size_t(1))
+
+    def call(work, lwork):
+        lib().scipy_dgghd3_(_c(compq.encode()), _c(compz.encode()), _ip(n), _ip(1), _ip(n), _dp(H), _ip(ld),
+                            _dp(T), _ip(ld), _dp(Q), _ip(ld), _dp(Z), _ip(ld), _dp(work), ctypes.byref(lwork),
+                            ctypes.byref(info), ctypes.c_size_t(1), ctypes.c_size_t(1))
+
+    w = np.zeros(1)
+    call(w, ctypes.c_int(-1))
+    lw = max(1, int(w[0]))
+    call(np.zeros(lw), ctypes.c_int(lw))
     return H, T, Q, Z, info.value
 
 

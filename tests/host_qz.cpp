@@ -16,6 +16,7 @@
 #include <vector>
 
 #include "../gevp-pdhgeqz_b200/csrc/qz_solver.h"
+#include "../gevp-pdhgeqz_b200/csrc/hessred.cuh"
 
 using namespace qz;
 
@@ -47,6 +48,7 @@ struct HostExec {
     if (k == 0) ++g_barriers[5];
   }
   void count(int) {}
+  bool wait(const int*, int) { return true; }
 };
 
 Tol make_tol(const double* H, const double* T, int ld, int o, int nh) {
@@ -391,4 +393,70 @@ int host_solve_p(int n, double* H, double* T, double* Q, double* Z, const int* i
   return info;
 }
 
+// Hessenberg-triangular reduction with the device's launch sequence
+// (hessred.cu): per column, window launches (CTA 0 part and helper walks),
+// the last window's walks, the column-end walks.  order 0 runs a launch's
+// CTA 0 part before its helper items, 1 after them, 2 after them in
+// reverse order: the parts touch disjoint entries, so all three give the
+// same bits.  icompq/icompz 0 none, 1 update, 2 identity first.
+int host_gghrd(int n, int ilo, int ihi, double* A, double* B, double* Q, double* Z, int W, int icompq, int icompz,
+               int qrows, int order) {
+  if (icompq == 2)
+    for (int j = 0; j < n; ++j)
+      for (int i = 0; i < n; ++i) Q[i + (size_t)j * n] = (i == j);
+  if (icompz == 2)
+    for (int j = 0; j < n; ++j)
+      for (int i = 0; i < n; ++i) Z[i + (size_t)j * n] = (i == j);
+  if (n <= 1) return 0;
+  for (int j = 0; j < n; ++j)
+    for (int i = j + 1; i < n; ++i) B[i + (size_t)j * n] = 0.0;
+  std::vector<double> rot(4 * (size_t)n, 0.0), sm(hr_smem_doubles(W) + 8, 0.0);
+  int err = 0;
+  HrArgs a{A, n, B, n, Q, n, Z, n, rot.data(), &err, n, ihi, icompq != 0, icompz != 0, qrows != 0};
+  HostExec x;
+  int launches = 0;
+  auto items = [&](int cnt, auto&& f) {
+    if (order == 2)
+      for (int i = cnt - 1; i >= 0; --i) f(i);
+    else
+      for (int i = 0; i < cnt; ++i) f(i);
+  };
+  // CTA 0 of a window launch (hessred.cu hr_window_cta), one host thread
+  auto window = [&](int jc, int lo, int hi, int plo, int phi) {
+    const int o = lo - 1, m = hi - lo + 2, ldw = hr_ldw(m);
+    const HrSmem L = hr_layout(sm.data(), W);
+    if (plo >= 0)
+      for (int r = o; r <= hi - 1; ++r) hr_walk_z(B + r, n, phi, plo, rot.data());
+    for (int j = 0; j < m; ++j)
+      for (int i = 0; i < m; ++i) L.Tw[i + j * ldw] = (i <= j) ? B[(o + i) + (size_t)(o + j) * n] : 0.0;
+    for (int i = 0; i < m; ++i) L.acol[i] = A[(o + i) + (size_t)jc * n];
+    *L.gready = 0;
+    hr_g_chain(m, L.acol, L.gbuf, L.gready);
+    cta_hr_zchain(x, L.Tw, ldw, m, L.gbuf, L.gready, L.slot);
+    for (int i = 4; i < 4 * m; ++i) rot[4 * o + i] = L.gbuf[i];
+    for (int j = 0; j < m; ++j)
+      for (int i = 0; i <= j; ++i) B[(o + i) + (size_t)(o + j) * n] = L.Tw[i + j * ldw];
+    for (int i = 0; i < m; ++i) A[(o + i) + (size_t)jc * n] = L.acol[i];
+  };
+  for (int jc = ilo; jc <= ihi - 2; ++jc) {
+    int plo = -1, phi = -1;
+    for (int hi = ihi; hi >= jc + 2;) {
+      const int lo = hr_win_lo(jc, hi, W);
+      auto helpers = [&]() {
+        if (plo >= 0) items(hr_win_items(a, lo - 1, phi), [&](int i) { hr_win_item(a, i, lo - 1, plo, phi); });
+      };
+      if (order != 0) helpers();
+      window(jc, lo, hi, plo, phi);
+      if (order == 0) helpers();
+      ++launches;
+      plo = lo; phi = hi; hi = lo - 1;
+    }
+    items(hr_win_items(a, plo - 1, phi), [&](int i) { hr_win_item(a, i, plo - 1, plo, phi); });
+    items(hr_col_items(a, jc), [&](int i) { hr_col_item(a, i, jc); });
+    launches += 2;
+  }
+  return launches;
+}
+
 }  // extern "C"
+

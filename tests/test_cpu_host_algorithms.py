@@ -37,6 +37,8 @@ def host(tmp_path_factory):
     L.host_solve_p.restype = ctypes.c_int
     L.host_barriers.argtypes = [ctypes.POINTER(ctypes.c_long), ctypes.c_int]
     L.host_barriers.restype = None
+    L.host_gghrd.argtypes = [ctypes.c_int] * 3 + [_pd] * 4 + [ctypes.c_int] * 5
+    L.host_gghrd.restype = ctypes.c_int
     L.host_set_pipe.argtypes = [ctypes.c_int]
     L.host_set_pipe.restype = None
     L.host_pipe_far_done.restype = ctypes.c_int
@@ -401,3 +403,66 @@ def test_host_swap11_two_rotations(host):
         u, v = np.array([S2[0, 0], T2[0, 0]]), np.array([c, f])
         chord = abs(u[0] * v[1] - u[1] * v[0]) / max(np.linalg.norm(u) * np.linalg.norm(v), 1e-300)
         assert chord <= 1e-10 or np.linalg.norm(v) == 0.0
+
+
+# ---------------------------------------------------------------------------
+# Hessenberg-triangular reduction: the device's launch sequence on the host
+# ---------------------------------------------------------------------------
+def _host_gghrd(host, A, B, ilo, ihi, W, order, cq=2, cz=2, qrows=0, Q=None, Z=None):
+    n = A.shape[0]
+    H, T = np.array(A, order="F", copy=True), np.array(B, order="F", copy=True)
+    Q = np.array(Q if Q is not None else np.zeros((n, n)), order="F", copy=True)
+    Z = np.array(Z if Z is not None else np.zeros((n, n)), order="F", copy=True)
+    host.host_gghrd(n, ilo, ihi, _p(H), _p(T), _p(Q), _p(Z), W, cq, cz, qrows, order)
+    return H, T, Q, Z
+
+
+@pytest.mark.parametrize("n,W", [(2, 4), (5, 2), (12, 3), (40, 7), (40, 128), (150, 16), (260, 64)])
+def test_host_gghrd_matches_dgghrd(host, lapack, n, W):
+    """Windows of W pairs, with each launch's parts run in three orders:
+    identical bits (the parts touch disjoint entries), and LAPACK DGGHRD's
+    H, T, Q, Z to rounding (same rotations in the same order), exact
+    Hessenberg-triangular structure, backward errors within 50 n eps."""
+    rng = np.random.default_rng(100 + n + W)
+    A = rng.standard_normal((n, n))
+    B = np.triu(rng.standard_normal((n, n)))
+    outs = [_host_gghrd(host, A, B, 0, n - 1, W, o) for o in (0, 1, 2)]
+    for o in (1, 2):
+        for k in range(4):
+            assert np.array_equal(outs[0][k], outs[o][k])
+    H, T, Q, Z = outs[0]
+    H0, T0, Q0, Z0, info = lapack.dgghrd(A, B)
+    assert info == 0
+    assert not np.any(np.tril(H, -2)) and not np.any(np.tril(T, -1))
+    tol = 1e-12 * max(1, n)
+    assert np.abs(H - H0).max() <= tol * np.abs(H0).max()
+    assert np.abs(T - T0).max() <= tol * np.abs(T0).max()
+    assert np.abs(Q - Q0).max() <= tol and np.abs(Z - Z0).max() <= tol
+    r = lapack.residuals(A, B, H, T, Q, Z)
+    for key in ("h", "t", "q", "z"):
+        assert r[key] <= 50 * r["neps"], (key, r[key] / r["neps"])
+
+
+def test_host_gghrd_ilo_ihi_and_modes(host, lapack):
+    """ILO/IHI sub-block, COMPQ/COMPZ in {N, V, I}, and the transposed Q
+    the reference's PDGGHRD returns (Q <- G Q)."""
+    rng = np.random.default_rng(7)
+    n, ilo, ihi = 60, 10, 49  # 0-based block rows/columns 10..49
+    A = np.triu(rng.standard_normal((n, n)))
+    A[ilo:ihi + 1, ilo:ihi + 1] = rng.standard_normal((ihi - ilo + 1,) * 2)
+    B = np.triu(rng.standard_normal((n, n)))
+    Qi, _ = np.linalg.qr(rng.standard_normal((n, n)))
+    Zi, _ = np.linalg.qr(rng.standard_normal((n, n)))
+    codes = {0: "N", 1: "V", 2: "I"}
+    for cq, cz in ((1, 1), (0, 2), (2, 0)):
+        H, T, Q, Z = _host_gghrd(host, A, B, ilo, ihi, 9, 0, cq, cz, 0, Qi, Zi)
+        Hl, Tl, Ql, Zl, info = lapack.dgghrd(A, B, codes[cq], codes[cz], ilo + 1, ihi + 1, Qi, Zi)
+        assert info == 0
+        assert np.abs(H - Hl).max() <= 1e-11 and np.abs(T - Tl).max() <= 1e-11
+        if cq:
+            assert np.abs(Q - Ql).max() <= 1e-12
+        if cz:
+            assert np.abs(Z - Zl).max() <= 1e-12
+    Qt = _host_gghrd(host, A, B, ilo, ihi, 9, 0, 1, 1, 1, Qi.T.copy(), Zi)[2]
+    Qn = _host_gghrd(host, A, B, ilo, ihi, 9, 0, 1, 1, 0, Qi, Zi)[2]
+    assert np.array_equal(Qt.T, Qn)
