@@ -2,6 +2,7 @@
 
     python tests/golden/make_port_fixtures.py c3      # n=10000 graded, seed 2
     python tests/golden/make_port_fixtures.py c2      # n=4000, 5% zero T diagonal, seed 1
+    python tests/golden/make_port_fixtures.py c4      # n=16000, seed 3 (about 75 min, mostly DTGSNA)
 
 Test infrastructure.  For each workload the oracle's C restatement of the
 reference path (oracle/qzref.c, the PDHGEQZ0 regime above n=6000, PDHGEQZ1

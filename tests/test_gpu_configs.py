@@ -85,7 +85,8 @@ def _match_port(lapack, fx, de, n):
     return ok, ratio, be
 
 
-@pytest.mark.parametrize("workload,fixture", [("c2", "port_c2_n4000.npz"), ("c3", "port_c3_n10000.npz")])
+@pytest.mark.parametrize("workload,fixture", [("c2", "port_c2_n4000.npz"), ("c3", "port_c3_n10000.npz"),
+                                              ("c4", "port_c4_n16000.npz")])
 def test_benchmark_pencil_matches_port(pkg, lapack, workload, fixture):
     fx = _fixture(fixture)
     H, T = pkg.pencils.workload(workload)
