@@ -2,7 +2,8 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--n 10000] [--workload c3] [--mode plain|split|learned|split+learned]
-       python bench.py --workload ggbal|tgsen   (balancing / reordering, LAPACK timed beside)
+       python bench.py --workload ggbal|tgsen|gghrd   (balancing / reordering / HT reduction,
+                                                    LAPACK timed beside)
 
 One step = one complete reduction of a Hessenberg-triangular pencil to
 generalized real Schur form with Q and Z (JOB='S', COMPQ=COMPZ='I').
@@ -684,6 +685,10 @@ def run_post(args, pkg):
         print(json.dumps(line), flush=True)
         solver.close()
         return
+    if args.workload == "gghrd":
+        run_gghrd(args, pkg, solver, peaks, peak_kind, clocks)
+        solver.close()
+        return
     # tgsen: reorder the GPU's Schur form of a random pencil so that the
     # eigenvalues of modulus below the median lead (n = 2000 unless --n
     # is given: LAPACK's DTGSEN beside it takes minutes above that)
@@ -762,6 +767,98 @@ def run_post(args, pkg):
     solver.close()
 
 
+def run_gghrd(args, pkg, solver, peaks, peak_kind, clocks):
+    """Hessenberg-triangular reduction of a dense A with upper triangular B
+    (n = 2000 unless --n is given; the reference's own example pair is of
+    order 4800): device time, end-to-end time through the host entry, and
+    LAPACK DGGHD3 (the blocked reduction) on one host core beside it."""
+    import time
+    import torch
+    from oracle import lapack as L
+    n = args.n if args.n != 10000 else 2000
+    dev = torch.cuda.current_device()
+    rng = np.random.default_rng(7)
+    A = rng.standard_normal((n, n))
+    B = np.triu(rng.standard_normal((n, n)))
+    dA0 = torch.from_numpy(np.ascontiguousarray(A.T)).to(dev)
+    dB0 = torch.from_numpy(np.ascontiguousarray(B.T)).to(dev)
+    dA, dB = torch.empty_like(dA0), torch.empty_like(dB0)
+    dQ, dZ = torch.empty_like(dA0), torch.empty_like(dA0)
+    win = 128
+    for p in args.param:
+        k, v = p.split("=")
+        if k == "hr_win":
+            win = int(float(v))
+            solver.set_param("hr_win", win)
+
+    def step():
+        dA.copy_(dA0)
+        dB.copy_(dB0)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        rc = solver.gghrd_device(dA.data_ptr(), dB.data_ptr(), dQ.data_ptr(), dZ.data_ptr(), n, n)
+        e1.record()
+        torch.cuda.synchronize()
+        if rc != 0:
+            raise RuntimeError("gghrd returned %d" % rc)
+        return e0.elapsed_time(e1) / 1e3
+
+    for _ in range(args.warmup):
+        step()
+    clocks.start()
+    ts = [step() for _ in range(args.steps)]
+    clk = clocks.stop()
+    t = float(np.mean(ts))
+    # backward errors of the last reduction (FP64 products on the GPU)
+    Hm, Tm, Qm, Zm, A0m, B0m = dA.T, dB.T, dQ.T, dZ.T, dA0.T, dB0.T
+    eps = np.finfo(np.float64).eps
+    res = {"a": float(torch.linalg.norm(Qm @ Hm @ Zm.T - A0m) / torch.linalg.norm(A0m)) / (n * eps),
+           "b": float(torch.linalg.norm(Qm @ Tm @ Zm.T - B0m) / torch.linalg.norm(B0m)) / (n * eps)}
+    # end to end: host arrays in, the reduced pencil and Q, Z out
+    te = []
+    for _ in range(args.steps):
+        Ah, Bh = np.array(A, order="F"), np.array(B, order="F")
+        Qh, Zh = np.empty((n, n), order="F"), np.empty((n, n), order="F")
+        t0 = time.perf_counter()
+        if solver.gghrd(Ah, Bh, Qh, Zh) != 0:
+            raise RuntimeError("gghrd (host) failed")
+        te.append(time.perf_counter() - t0)
+    cpu = None
+    if not args.no_cpu_baseline:
+        L.set_threads(1)
+        t0 = time.perf_counter()
+        _, _, _, _, linfo = L.dgghd3(A, B)
+        cpu_t = time.perf_counter() - t0
+        cpu = {"value": cpu_t, "unit": "s", "cores": 1, "kind": "reference",
+               "sample": "LAPACK DGGHD3 (blocked Hessenberg-triangular reduction, scipy's OpenBLAS, one "
+                         "thread) on the same pencil, one call", "info": int(linfo)}
+    pairs = (n - 1) * (n - 2) // 2
+    windows = sum(-(-(n - 2 - jc) // win) for jc in range(n - 2))
+    # algorithmic bytes of the rotation walks: per column jc every touched
+    # entry of A, B, Q, Z is read and written once (about
+    # 2 (n-jc)^2 + 3 n (n-jc) entries, 16 bytes each)
+    alg = 16.0 * sum(2.0 * (n - jc) ** 2 + 3.0 * n * (n - jc) for jc in range(n - 2))
+    peak = peaks.get("hbm_gbs")
+    ach = alg / t / 1e9
+    line = {"metric": "ht_reduction_seconds", "value": t, "unit": "s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "gghrd: DGGHRD COMPQ=COMPZ=I, A dense N(0,1), B upper triangular N(0,1), "
+                                   "n=%d (seed 7)" % n, "n": n, "pairs": pairs, "windows": windows,
+                       "hr_win": win, "backward_error_n_eps": res,
+                       "inputs": "device-resident copies, 2 x %.2f GB" % (8e-9 * n * n)},
+            "e2e": {"value": float(np.mean(te)), "unit": "s", "h2d_bytes_per_step": 16 * n * n,
+                    "d2h_bytes_per_step": 32 * n * n},
+            "roofline": {"bound": "latency", "achieved": ach, "peak": peak, "unit": "GB/s",
+                         "frac": (ach / peak) if peak else None, "traffic": None,
+                         "peak_source": "%s HBM copy bandwidth" % peak_kind,
+                         "note": "the walks' algorithmic bytes over the whole call; the bound is the chain "
+                                 "of %d dependent rotation pairs on one SM (FP64 latency)" % pairs},
+            "cpu_baseline": cpu, "clocks": clk, "gpu_launches": windows + 2 * (n - 2) + 4}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -792,9 +889,9 @@ def main():
     if args.workload == "c5":
         run_batched(args, pkg, rank, world, local)
         return
-    if args.workload in ("ggbal", "tgsen"):
+    if args.workload in ("ggbal", "tgsen", "gghrd"):
         if args.impl == "reference":
-            print(json.dumps({"impl": "reference", "unavailable": "the ggbal/tgsen workloads time LAPACK "
+            print(json.dumps({"impl": "reference", "unavailable": "the ggbal/tgsen/gghrd workloads time LAPACK "
                               "beside the GPU call in their own line (cpu_baseline)"}))
         elif rank == 0:
             run_post(args, pkg)

@@ -25,7 +25,7 @@
 namespace qz {
 namespace {
 
-constexpr int kHrChain = 128;               // chain threads of a window CTA
+constexpr int kHrChain = 128;               // chain threads: 96 far threads and the block thread's warp
 constexpr int kHrThreads = kHrChain + 32;   // plus the producer's warp
 constexpr int kHrSpin = 1 << 22;            // polls before a wait gives up
 

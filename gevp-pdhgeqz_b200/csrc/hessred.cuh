@@ -202,24 +202,28 @@ QZ_HD void hr_g_chain(int m, double* acol, double* gbuf, int* gready) {
 // Tw is the block after the window's rotations and gbuf[4J+2..4J+3] holds
 // pair J's (cz, sz).  slot: 8 doubles of shared scratch.
 //
-// Phase k computes pair J = m-1-k on the block thread while every thread
-// applies the pending pair P = J+1 to its entries of the block: G on rows
-// P-1, P at columns >= P+1 and Z on columns P, P-1 at rows <= P-3.  The
-// block thread applies P's Z to row P-2 (which pair J reads) and stores
-// P's 2x2 block, so each entry sees the rotations in the order of the
-// sequential algorithm.
+// Phase k computes pair J = m-1-k on the block thread while the far
+// threads apply the pending pair P = J+1 to their entries of the block: G
+// on rows P-1, P at columns >= P+1 and Z on columns P, P-1 at rows <= P-3.
+// The block thread applies P's Z to row P-2 (which pair J reads) and
+// stores P's 2x2 block, so each entry sees the rotations in the order of
+// the sequential algorithm.  On the device the block thread is lane 0 of
+// the last warp (x.nt - 32 far threads before it, the rest of its warp
+// idle), so that its pair is the only work on the chain's critical path;
+// with one host thread (x.nt == 1) that thread does both parts.
 template <class X>
 QZ_HD void cta_hr_zchain(X& x, double* Tw, int ldw, int m, double* gbuf, const int* gready, double* slot) {
-  auto T = [&](int i, int j) -> double& { return Tw[i + (int64_t)j * ldw]; };
-  const bool bt = x.tid == x.nt - 1;
+  auto T = [&](int i, int j) -> double& { return Tw[i + j * ldw]; };
+  const int nfar = x.nt > 32 ? x.nt - 32 : x.nt;
+  const bool bt = x.nt > 32 ? x.tid == nfar : true;
   const int np = m - 1;
   double pcz = 0.0, psz = 0.0, pt00 = 0.0, pt01 = 0.0, prz = 0.0;
   for (int k = 0; k <= np; ++k) {
     const int J = m - 1 - k, P = J + 1;
-    if (k >= 1) {
+    if (k >= 1 && x.tid < nfar) {
       const double* sl = slot + 4 * ((k - 1) & 1);
       const double c = sl[0], s = sl[1], cz = sl[2], sz = sl[3];
-      for (int t = x.tid; t < m; t += x.nt) {
+      for (int t = x.tid; t < m; t += nfar) {
         if (t >= P + 1) rot2(c, s, T(P - 1, t), T(P, t));
         else if (t <= P - 3) rot2(cz, sz, T(t, P), T(t, P - 1));
       }

@@ -76,6 +76,14 @@ module b200qz
 
      ! reordering of the Schur form with DTGSEN's arguments (IJOB 0 or 1);
      ! the role of PDTGSEN (src/reorder/PDTGSEN.f:1)
+     integer(c_int) function b200qz_gghrd_host(ctx, compq, compz, n, ilo, ihi, a, lda, b, ldb, q, ldq, z, ldz) &
+          bind(C, name="b200qz_gghrd_host")
+       import :: c_ptr, c_int, c_double, c_char
+       type(c_ptr), value :: ctx
+       character(kind=c_char), value :: compq, compz
+       integer(c_int), value :: n, ilo, ihi, lda, ldb, ldq, ldz
+       real(c_double), intent(inout) :: a(lda, *), b(ldb, *), q(ldq, *), z(ldz, *)
+     end function b200qz_gghrd_host
      integer(c_int) function b200qz_tgsen_host(ctx, ijob, wantq, wantz, select, n, s, lds, t, ldt, q, ldq, &
           z, ldz, alphar, alphai, beta, m, pl, pr, info) bind(C, name="b200qz_tgsen_host")
        import :: c_int, c_double, c_ptr
