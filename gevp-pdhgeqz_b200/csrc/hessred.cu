@@ -66,13 +66,15 @@ __device__ void hr_window_cta(const HrArgs& a, int jc, int lo, int hi, int plo, 
   if (plo >= 0) {
     // (a) the previous window's Z on rows lo-1..hi-1 of B, columns
     // hi..phi, staged in the block's buffer
+    // (its rotation records staged too: every row walks all of them)
     const int mp = phi - hi + 1, rows = m - 1;
     double* S = L.Tw;
     for (int j = 0; j < mp; ++j)
       for (int i = tid; i < rows; i += nt) cp_async8(&S[i + j * ldw], a.B + (o + i) + (int64_t)(hi + j) * a.ldb);
+    for (int i = 4 + tid; i < 4 * mp; i += nt) cp_async8(&L.gbuf[i], a.rot + 4 * hi + i);
     cp_async_wait_all();
     __syncthreads();
-    for (int i = tid; i < rows; i += nt) hr_walk_z(S + i, ldw, phi - hi, plo - hi, a.rot + 4 * hi);
+    for (int i = tid; i < rows; i += nt) hr_walk_z(S + i, ldw, phi - hi, plo - hi, L.gbuf);
     __syncthreads();
     for (int j = 0; j < mp; ++j)
       for (int i = tid; i < rows; i += nt) a.B[(o + i) + (int64_t)(hi + j) * a.ldb] = S[i + j * ldw];

@@ -110,26 +110,30 @@ QZ_HD double hr_rsqrt(double q) {
 // where the squares neither overflow nor underflow (the chain's latency is
 // two of these per pair).
 QZ_HD void hr_lartg(double f, double g, double& c, double& s, double& r) {
-  if (g == 0.0) {
+  const double af = fabs(f), ag = fabs(g), mx = af > ag ? af : ag;
+  if (mx > kSafeLo && mx < kSafeHi) {
+    // in range: selects instead of branches for the exact cases g = 0
+    // (identity) and f = 0 (a swap), as LAPACK returns them
+    const double q = f * f + g * g, inv = hr_rsqrt(q);
+    const double sg = f < 0.0 ? -1.0 : 1.0;
+    const bool g0 = g == 0.0, f0 = f == 0.0;
+    c = g0 ? 1.0 : (f0 ? 0.0 : af * inv);
+    s = g0 ? 0.0 : (f0 ? (g > 0.0 ? 1.0 : -1.0) : sg * g * inv);
+    r = g0 ? f : (f0 ? ag : sg * (q * inv));
+  } else if (mx == 0.0) {
     c = 1.0; s = 0.0; r = f;
-  } else if (f == 0.0) {
-    c = 0.0; s = (g > 0.0) ? 1.0 : -1.0; r = fabs(g);
   } else {
-    const double af = fabs(f), ag = fabs(g), mx = af > ag ? af : ag;
-    double d;
-    if (mx > kSafeLo && mx < kSafeHi) {
-      const double q = f * f + g * g, inv = hr_rsqrt(q);
-      c = af * inv;
-      s = g * inv;
-      d = q * inv;
+    const double fs = f / mx, gs = g / mx, q = fs * fs + gs * gs, inv = hr_rsqrt(q);
+    if (g == 0.0) {
+      c = 1.0; s = 0.0; r = f;
+    } else if (f == 0.0) {
+      c = 0.0; s = (g > 0.0) ? 1.0 : -1.0; r = ag;
     } else {
-      const double fs = f / mx, gs = g / mx, q = fs * fs + gs * gs, inv = hr_rsqrt(q);
+      const double sg = f < 0.0 ? -1.0 : 1.0;
       c = fabs(fs) * inv;
-      s = gs * inv;
-      d = q * inv * mx;
+      s = sg * gs * inv;
+      r = sg * (q * inv * mx);
     }
-    r = dsign(d, f);
-    if (f < 0.0) s = -s;
   }
 }
 
@@ -207,10 +211,13 @@ QZ_HD void hr_g_chain(int m, double* acol, double* gbuf, int* gready) {
 // on rows P-1, P at columns >= P+1 and Z on columns P, P-1 at rows <= P-3.
 // The block thread applies P's Z to row P-2 (which pair J reads) and
 // stores P's 2x2 block, so each entry sees the rotations in the order of
-// the sequential algorithm.  On the device the block thread is lane 0 of
-// the last warp (x.nt - 32 far threads before it, the rest of its warp
-// idle), so that its pair is the only work on the chain's critical path;
-// with one host thread (x.nt == 1) that thread does both parts.
+// the sequential algorithm.  The entries pair J reads that no thread
+// changes before it (its diagonal entry of the block, the original
+// T(J-1, J), its row rotation once published) are loaded one phase
+// ahead, so that after the barrier the block thread waits on one shared
+// load, T(J-1, J+1).  On the device the block thread is lane 0 of the last
+// warp (x.nt - 32 far threads before it, the rest of its warp idle); with
+// one host thread (x.nt == 1) that thread does both parts.
 template <class X>
 QZ_HD void cta_hr_zchain(X& x, double* Tw, int ldw, int m, double* gbuf, const int* gready, double* slot) {
   auto T = [&](int i, int j) -> double& { return Tw[i + j * ldw]; };
@@ -218,6 +225,17 @@ QZ_HD void cta_hr_zchain(X& x, double* Tw, int ldw, int m, double* gbuf, const i
   const bool bt = x.nt > 32 ? x.tid == nfar : true;
   const int np = m - 1;
   double pcz = 0.0, psz = 0.0, pt00 = 0.0, pt01 = 0.0, prz = 0.0;
+  // block thread: the next pair's entries loaded ahead, and the count of
+  // published row rotations last seen
+  double nt00 = 0.0, nv = 0.0, nc = 0.0, ns = 0.0;
+  int avail = 0;
+  if (bt && np >= 1) {
+    const int J = m - 1;
+    nt00 = T(J - 1, J - 1);
+    while (avail < 1) avail = x.wait(gready, 1) ? hr_ld_acq(gready) : 1;
+    nc = gbuf[4 * J];
+    ns = gbuf[4 * J + 1];
+  }
   for (int k = 0; k <= np; ++k) {
     const int J = m - 1 - k, P = J + 1;
     if (k >= 1 && x.tid < nfar) {
@@ -232,7 +250,7 @@ QZ_HD void cta_hr_zchain(X& x, double* Tw, int ldw, int m, double* gbuf, const i
       double a_t01 = 0.0;
       if (k >= 1) {
         if (P >= 2) {
-          double u = T(P - 2, P), v = T(P - 2, P - 1);
+          double u = T(P - 2, P), v = nv;
           rot2(pcz, psz, u, v);
           T(P - 2, P) = u;
           a_t01 = v;
@@ -243,11 +261,10 @@ QZ_HD void cta_hr_zchain(X& x, double* Tw, int ldw, int m, double* gbuf, const i
         if (k == np) T(P - 1, P - 1) = pt00;
       }
       if (k < np) {
-        const double t00 = T(J - 1, J - 1);
+        const double t00 = nt00;
         const double t01 = (k == 0) ? T(J - 1, J) : a_t01;
         const double t11 = (k == 0) ? T(J, J) : pt00;
-        x.wait(gready, k + 1);
-        const double c = gbuf[4 * J], s = gbuf[4 * J + 1];
+        const double c = nc, s = ns;
         double cz, sz, rz;
         const double u10 = -s * t00, u11 = -s * t01 + c * t11;
         double u00 = c * t00, u01 = c * t01 + s * t11;
@@ -258,6 +275,14 @@ QZ_HD void cta_hr_zchain(X& x, double* Tw, int ldw, int m, double* gbuf, const i
         sl[0] = c; sl[1] = s; sl[2] = cz; sl[3] = sz;
         gbuf[4 * J + 2] = cz;
         gbuf[4 * J + 3] = sz;
+        // ahead: what pair J-1 reads and nobody changes before it
+        if (J >= 2) {
+          nt00 = T(J - 2, J - 2);
+          nv = T(J - 2, J - 1);
+          if (avail < k + 2) avail = x.wait(gready, k + 2) ? hr_ld_acq(gready) : k + 2;
+          nc = gbuf[4 * (J - 1)];
+          ns = gbuf[4 * (J - 1) + 1];
+        }
       }
     }
     x.sync();

@@ -458,5 +458,9 @@ int host_gghrd(int n, int ilo, int ihi, double* A, double* B, double* Q, double*
   return launches;
 }
 
+// The reduction's Givens rotation (hessred.cuh hr_lartg) for a test
+// against LAPACK's DLARTG convention.
+void host_hr_lartg(double f, double g, double* out) { hr_lartg(f, g, out[0], out[1], out[2]); }
+
 }  // extern "C"
 

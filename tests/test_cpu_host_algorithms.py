@@ -39,6 +39,8 @@ def host(tmp_path_factory):
     L.host_barriers.restype = None
     L.host_gghrd.argtypes = [ctypes.c_int] * 3 + [_pd] * 4 + [ctypes.c_int] * 5
     L.host_gghrd.restype = ctypes.c_int
+    L.host_hr_lartg.argtypes = [ctypes.c_double, ctypes.c_double, _pd]
+    L.host_hr_lartg.restype = None
     L.host_set_pipe.argtypes = [ctypes.c_int]
     L.host_set_pipe.restype = None
     L.host_pipe_far_done.restype = ctypes.c_int
@@ -466,3 +468,19 @@ def test_host_gghrd_ilo_ihi_and_modes(host, lapack):
     Qt = _host_gghrd(host, A, B, ilo, ihi, 9, 0, 1, 1, 1, Qi.T.copy(), Zi)[2]
     Qn = _host_gghrd(host, A, B, ilo, ihi, 9, 0, 1, 1, 0, Qi, Zi)[2]
     assert np.array_equal(Qt.T, Qn)
+
+
+def test_host_hr_lartg_matches_dlartg(host):
+    """The reduction's rotation against LAPACK's DLARTG (the convention its
+    H, T, Q, Z inherit): c >= 0, r with the sign of f, exact results for a
+    zero f or g, rescaling far outside the unit range."""
+    from scipy.linalg import lapack as sl
+    vals = [0.0, 1.0, -1.0, 3.0, -4.0, 1e-200, -1e-200, 1e200, -1e200, 1e-310, 2.5e-150, 7e149]
+    out = np.zeros(3)
+    for f in vals:
+        for g in vals:
+            host.host_hr_lartg(f, g, _p(out))
+            c, s, r = sl.dlartg(f, g)
+            assert np.allclose(out, [c, s, r], rtol=4e-16, atol=0.0), (f, g, out, (c, s, r))
+            if f == 0.0 or g == 0.0:
+                assert tuple(out) == (c, s, r), (f, g, out, (c, s, r))

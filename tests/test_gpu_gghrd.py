@@ -5,8 +5,10 @@ DGGHRD on the same inputs: the same H, T, Q, Z to rounding (the same
 rotations in the same order and sign convention), exact Hessenberg-
 triangular structure, backward errors and orthogonality within 50 n eps;
 the ILO/IHI and COMPQ/COMPZ modes; the PDGGHRD drop-in with its
-transposed Q; and a general pencil reduced and solved on the GPU, whose
-eigenvalues match LAPACK's within the condition-scaled tolerance."""
+transposed Q; a general pencil reduced and solved on the GPU, whose
+eigenvalues match LAPACK's within the condition-scaled tolerance; and the
+same for the reference's own example pencil (examples/sparseA.mtx,
+sparseB.mtx, n = 4800)."""
 import numpy as np
 import pytest
 
@@ -201,4 +203,55 @@ def test_general_pencil_reduced_and_solved_on_gpu(solver, lapack, pkg):
     assert linfo == 0
     tol = lapack.eig_tolerance(So, Po, Hl, Tl)
     ok, ratio, _ = lapack.match_eigenvalues((lar, lai, lbe), (ar, ai, be), tol)
+    assert ok, ratio
+
+
+def test_reference_example_pencil_reduced_and_solved_on_gpu(solver, lapack, pkg):
+    """The reference's own example pair (examples/sparseA.mtx, sparseB.mtx,
+    4800 x 4800, read by examples/EXRAND3.f:297-316; entries committed in
+    tests/golden/mhd4800.npz by tests/golden/make_mhd_fixture.py): QR of B
+    on the host, then the Hessenberg-triangular reduction and the QZ solve
+    on the GPU.  The result is a generalized Schur form of the original
+    pencil within 50 n eps, and its eigenvalues match LAPACK's (DGGHD3 +
+    DHGEQZ of the same pencil) within the condition-scaled tolerance."""
+    import os
+    import torch
+    fx = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "mhd4800.npz"))
+    n = 4800
+    A0 = np.zeros((n, n))
+    np.add.at(A0, (fx["a_i"], fx["a_j"]), fx["a_v"])
+    B0 = np.zeros((n, n))
+    np.add.at(B0, (fx["b_i"], fx["b_j"]), fx["b_v"])
+    off = fx["b_i"] != fx["b_j"]
+    np.add.at(B0, (fx["b_j"][off], fx["b_i"][off]), fx["b_v"][off])
+    qb, rb = np.linalg.qr(B0)
+    dev = torch.device("cuda:0")
+    # device buffers hold the transposes of the column-major matrices
+    tA = torch.tensor((qb.T @ A0).T.copy(), dtype=torch.float64, device=dev)
+    tB = torch.tensor(np.triu(rb).T.copy(), dtype=torch.float64, device=dev)
+    tQ = torch.tensor(qb.T.copy(), dtype=torch.float64, device=dev)
+    tZ = torch.empty((n, n), dtype=torch.float64, device=dev)
+    torch.cuda.synchronize()
+    assert solver.gghrd_device(tA.data_ptr(), tB.data_ptr(), tQ.data_ptr(), tZ.data_ptr(), n, n,
+                               compq="V", compz="I") == 0
+    de = torch.empty(3 * n, dtype=torch.float64, device=dev)
+    info = solver.solve_device(tA.data_ptr(), tB.data_ptr(), tQ.data_ptr(), tZ.data_ptr(), n, n, de.data_ptr(),
+                               de.data_ptr() + 8 * n, de.data_ptr() + 16 * n, compq="V", compz="V")
+    torch.cuda.synchronize()
+    assert info == 0
+    S, P, Q, Z = tA.T, tB.T, tQ.T, tZ.T
+    gA0 = torch.tensor(A0, dtype=torch.float64, device=dev)
+    gB0 = torch.tensor(B0, dtype=torch.float64, device=dev)
+    eps = np.finfo(np.float64).eps
+    I = torch.eye(n, dtype=torch.float64, device=dev)
+    r = {"a": float(torch.linalg.norm(Q @ S @ Z.T - gA0) / torch.linalg.norm(gA0)),
+         "b": float(torch.linalg.norm(Q @ P @ Z.T - gB0) / torch.linalg.norm(gB0)),
+         "q": float(torch.linalg.norm(Q.T @ Q - I)), "z": float(torch.linalg.norm(Z.T @ Z - I))}
+    for key, v in r.items():
+        assert v <= 50 * n * eps, (key, v / (n * eps))
+    assert not bool(torch.any(torch.tril(S, -2))) and not bool(torch.any(torch.tril(P, -1)))
+    e = de.cpu().numpy()
+    tol = np.clip(50.0 * n * eps * float(fx["norm"]) / np.maximum(fx["rcond"], 1e-300), 50.0 * n * eps, 2.0)
+    ok, ratio, _ = lapack.match_eigenvalues((fx["alphar"], fx["alphai"], fx["beta"]), (e[:n], e[n:2 * n], e[2 * n:]),
+                                            tol)
     assert ok, ratio
