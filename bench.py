@@ -717,7 +717,7 @@ def run_post(args, pkg):
                                   pkg._vp(dw[2].data_ptr()), n, pkg._vp(dw[3].data_ptr()), n,
                                   pkg._vp(de.data_ptr()), pkg._vp(de.data_ptr() + 8 * n),
                                   pkg._vp(de.data_ptr() + 16 * n), pkg.ctypes.byref(m), pkg.ctypes.byref(pl),
-                                  pkg.ctypes.byref(pr), pkg.ctypes.byref(inf), cnt.ctypes.data_as(pkg._pi))
+                                  pkg.ctypes.byref(pr), None, pkg.ctypes.byref(inf), cnt.ctypes.data_as(pkg._pi))
         t = time.perf_counter() - t0
         if rc != 0 or inf.value != 0:
             raise RuntimeError("tgsen returned %d / info %d" % (rc, inf.value))

@@ -139,9 +139,9 @@ def lib() -> ctypes.CDLL:
     for f in ("b200qz_ggbal_dev", "b200qz_ggbal_host"):
         getattr(L, f).argtypes = [_vp, _c, _i, _vp, _i, _vp, _i, _pi, _pi, _pd, _pd]
         getattr(L, f).restype = _i
-    L.b200qz_tgsen_host.argtypes = [_vp, _i, _i, _i, _pi, _i] + [_vp, _i] * 4 + [_pd] * 3 + [_pi, _pd, _pd, _pi]
+    L.b200qz_tgsen_host.argtypes = [_vp, _i, _i, _i, _pi, _i] + [_vp, _i] * 4 + [_pd] * 3 + [_pi, _pd, _pd, _pd, _pi]
     L.b200qz_tgsen_host.restype = _i
-    L.b200qz_tgsen_dev.argtypes = [_vp, _i, _i, _i, _pi, _i] + [_vp, _i] * 4 + [_vp] * 3 + [_pi, _pd, _pd, _pi, _pi]
+    L.b200qz_tgsen_dev.argtypes = [_vp, _i, _i, _i, _pi, _i] + [_vp, _i] * 4 + [_vp] * 3 + [_pi, _pd, _pd, _pd, _pi, _pi]
     L.b200qz_tgsen_dev.restype = _i
     for f in ("b200qz_ggbak_dev", "b200qz_ggbak_host"):
         getattr(L, f).argtypes = [_vp, _c, _c, _i, _i, _i, _pd, _pd, _i, _vp, _i]
@@ -326,23 +326,26 @@ class Solver:
                                       ctypes.byref(ihi), _p(ls), _p(rs))
         return ilo.value, ihi.value, ls[:n], rs[:n], info
 
-    def tgsen(self, S, T, Q, Z, select, ijob=0, wantq=True, wantz=True):
+    def tgsen(self, S, T, Q, Z, select, ijob=0, wantq=True, wantz=True, dif=None):
         """Reorder the host generalized Schur form (S, T) and Q, Z in place
         on the GPU so that the selected eigenvalues lead (DTGSEN
-        semantics, ijob 0 or 1).  Returns (alphar, alphai, beta, m, pl,
-        pr, info, ret) with ret the C return code."""
+        semantics, ijob 0, 1, 3 or 5).  Returns (alphar, alphai, beta, m,
+        pl, pr, info, ret) with ret the C return code; for ijob 3 and 5 the
+        Difu, Difl estimates go to ``dif`` (a float64 array of 2) when
+        given."""
         n = S.shape[0]
         sel = np.ascontiguousarray(np.asarray(select, dtype=np.int32).reshape(-1))
         ar, ai, be = np.zeros(max(1, n)), np.zeros(max(1, n)), np.zeros(max(1, n))
         m, info = ctypes.c_int(0), ctypes.c_int(0)
         pl, pr = ctypes.c_double(0), ctypes.c_double(0)
+        d = dif if dif is not None else np.zeros(2)
         Qa = Q if Q is not None else np.zeros((1, 1), order="F")
         Za = Z if Z is not None else np.zeros((1, 1), order="F")
         ret = lib().b200qz_tgsen_host(self._h, ijob, int(wantq), int(wantz),
                                       sel.ctypes.data_as(_pi), n, _vp(S.ctypes.data), max(1, n), _vp(T.ctypes.data),
                                       max(1, n), _vp(Qa.ctypes.data), max(1, Qa.shape[0]), _vp(Za.ctypes.data),
                                       max(1, Za.shape[0]), _p(ar), _p(ai), _p(be), ctypes.byref(m),
-                                      ctypes.byref(pl), ctypes.byref(pr), ctypes.byref(info))
+                                      ctypes.byref(pl), ctypes.byref(pr), _p(d), ctypes.byref(info))
         return ar[:n], ai[:n], be[:n], m.value, pl.value, pr.value, info.value, ret
 
     def gghrd(self, A, B, Q=None, Z=None, compq="I", compz="I", ilo=1, ihi=None):

@@ -1241,7 +1241,7 @@ int b200qz_ggbak_host(b200qz_ctx* c, char job, char side, int n, int ilo, int ih
 // Reordering of a generalized Schur form (DTGSEN semantics, IJOB 0 and 1).
 // ---------------------------------------------------------------------------
 static int tgsen_args(int ijob, int wantq, int wantz, int n, int lds, int ldt, int ldq, int ldz) {
-  if (ijob < 0 || ijob > 1) return -1;
+  if (ijob != 0 && ijob != 1 && ijob != 3 && ijob != 5) return -1;
   if (n < 0) return -5;
   if (lds < std::max(1, n)) return -7;
   if (ldt < std::max(1, n)) return -9;
@@ -1252,7 +1252,7 @@ static int tgsen_args(int ijob, int wantq, int wantz, int n, int lds, int ldt, i
 
 int b200qz_tgsen_dev(b200qz_ctx* c, int ijob, int wantq, int wantz, const int* select, int n, double* s, int lds,
                      double* t, int ldt, double* q, int ldq, double* z, int ldz, double* alphar, double* alphai,
-                     double* beta, int* m, double* pl, double* pr, int* info, int* counts) {
+                     double* beta, int* m, double* pl, double* pr, double* dif, int* info, int* counts) {
   if (!c) return 10001;
   const int bad = tgsen_args(ijob, wantq, wantz, n, lds, ldt, ldq, ldz);
   if (bad) return bad;
@@ -1264,6 +1264,7 @@ int b200qz_tgsen_dev(b200qz_ctx* c, int ijob, int wantq, int wantz, const int* s
   *m = o.m;
   *pl = o.pl;
   *pr = o.pr;
+  if (dif && (ijob == 3 || ijob == 5)) { dif[0] = o.dif[0]; dif[1] = o.dif[1]; }
   *info = o.info;
   if (counts) { counts[0] = o.swaps; counts[1] = o.windows; }
   return 0;
@@ -1271,11 +1272,15 @@ int b200qz_tgsen_dev(b200qz_ctx* c, int ijob, int wantq, int wantz, const int* s
 
 int b200qz_tgsen_host(b200qz_ctx* c, int ijob, int wantq, int wantz, const int* select, int n, double* s, int lds,
                       double* t, int ldt, double* q, int ldq, double* z, int ldz, double* alphar, double* alphai,
-                      double* beta, int* m, double* pl, double* pr, int* info) {
+                      double* beta, int* m, double* pl, double* pr, double* dif, int* info) {
   if (!c) return 10001;
   const int bad = tgsen_args(ijob, wantq, wantz, n, lds, ldt, ldq, ldz);
   if (bad) return bad;
-  if (n == 0) { *m = 0; *pl = *pr = 1.0; *info = 0; return 0; }
+  if (n == 0) {
+    *m = 0; *pl = *pr = 1.0; *info = 0;
+    if (dif && (ijob == 3 || ijob == 5)) dif[0] = dif[1] = 0.0;
+    return 0;
+  }
   if (cudaSetDevice(c->device) != cudaSuccess) return 10001;
   const size_t nn = (size_t)n * n;
   double* d = nullptr;
@@ -1310,6 +1315,7 @@ int b200qz_tgsen_host(b200qz_ctx* c, int ijob, int wantq, int wantz, const int* 
   *m = o.m;
   *pl = o.pl;
   *pr = o.pr;
+  if (dif && (ijob == 3 || ijob == 5)) { dif[0] = o.dif[0]; dif[1] = o.dif[1]; }
   *info = o.info;
   return 0;
 }

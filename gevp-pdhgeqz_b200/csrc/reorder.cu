@@ -41,6 +41,7 @@
 #include <vector>
 
 #include "kernels.h"
+#include "onenorm.h"
 
 namespace qz {
 namespace {
@@ -302,6 +303,148 @@ __global__ void k_ssq_final(const double* part, int np, double* out) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// General generalized Sylvester solve for the Dif estimates (the role of
+// LAPACK DTGSYL with IJOB = 0 inside DTGSEN IJOB 3 and 5): (A, D) is an
+// m x m and (B, E) an n x n upper quasi-triangular pair, (C, F) an m x n
+// right-hand side overwritten by the solution (R, L) of
+//   trans 0:  A R - L B = C,        D R - L E = F
+//   trans 1:  A^T R + D^T L = C,    R B^T + L E^T = -F
+// Block pairs (i, j) of the diagonal blocks are solved on anti-diagonal
+// waves, a warp per pair: trans 0 from the bottom-left corner (blocks below
+// and to the left first), trans 1 from the top-right corner.
+// ---------------------------------------------------------------------------
+struct SylvGen {
+  const double *A, *D, *B, *E;
+  int64_t lda, ldd, ldb, lde;
+  double *C, *F;  // m x n, leading dimension m
+  int m, n;
+  const int *as, *az, *bs, *bz;  // diagonal blocks: starts, sizes
+  int na, nb;
+  int trans;
+};
+
+template <int P, int Q>
+__device__ void sylv_gen_solve(const SylvGen& g, int i0, int j0, const double* ce, const double* fe) {
+  constexpr int NQ = P * Q, NS = 2 * NQ;
+  double M[NS * NS], rhs[NS];
+#pragma unroll
+  for (int k = 0; k < NS * NS; ++k) M[k] = 0.0;
+  auto A = [&](int r, int c) { return g.A[(i0 + r) + (int64_t)(i0 + c) * g.lda]; };
+  auto D = [&](int r, int c) { return g.D[(i0 + r) + (int64_t)(i0 + c) * g.ldd]; };
+  auto B = [&](int r, int c) { return g.B[(j0 + r) + (int64_t)(j0 + c) * g.ldb]; };
+  auto E = [&](int r, int c) { return g.E[(j0 + r) + (int64_t)(j0 + c) * g.lde]; };
+#pragma unroll
+  for (int b = 0; b < Q; ++b)
+#pragma unroll
+    for (int a = 0; a < P; ++a) {
+      const int r1 = a + P * b, r2 = NQ + a + P * b;
+#pragma unroll
+      for (int c = 0; c < P; ++c) {
+        if (g.trans) {
+          M[r1 + NS * (c + P * b)] += A(c, a);
+          M[r1 + NS * (NQ + c + P * b)] += D(c, a);
+        } else {
+          M[r1 + NS * (c + P * b)] += A(a, c);
+          M[r2 + NS * (c + P * b)] += D(a, c);
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < Q; ++c) {
+        if (g.trans) {
+          M[r2 + NS * (a + P * c)] += B(b, c);
+          M[r2 + NS * (NQ + a + P * c)] += E(b, c);
+        } else {
+          M[r1 + NS * (NQ + a + P * c)] -= B(c, b);
+          M[r2 + NS * (NQ + a + P * c)] -= E(c, b);
+        }
+      }
+      rhs[r1] = ce[a + 2 * b];
+      rhs[r2] = fe[a + 2 * b];
+    }
+  small_solve_cp<NS>(M, rhs, DBL_MIN);
+#pragma unroll
+  for (int b = 0; b < Q; ++b)
+#pragma unroll
+    for (int a = 0; a < P; ++a) {
+      g.C[(i0 + a) + (int64_t)(j0 + b) * g.m] = rhs[a + P * b];
+      g.F[(i0 + a) + (int64_t)(j0 + b) * g.m] = rhs[NQ + a + P * b];
+    }
+}
+
+__global__ void k_sylv_gen_wave(SylvGen g, int d) {
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  int bi, bj;
+  if (!g.trans) {
+    const int jlo = d - (g.na - 1) > 0 ? d - (g.na - 1) : 0;
+    const int jhi = d < g.nb - 1 ? d : g.nb - 1;
+    bj = jlo + warp;
+    if (bj > jhi) return;
+    bi = g.na - 1 - (d - bj);
+  } else {
+    const int ilo = d - (g.nb - 1) > 0 ? d - (g.nb - 1) : 0;
+    const int ihi = d < g.na - 1 ? d : g.na - 1;
+    bi = ilo + warp;
+    if (bi > ihi) return;
+    bj = g.nb - 1 - (d - bi);
+  }
+  const int i0 = g.as[bi], p = g.az[bi], j0 = g.bs[bj], q = g.bz[bj];
+  const int m = g.m, n = g.n;
+  double s1[4] = {0, 0, 0, 0}, s2[4] = {0, 0, 0, 0};
+  if (!g.trans) {
+    // rows below (solved R) and columns to the left (solved L)
+    for (int k = i0 + p + lane; k < m; k += 32)
+      for (int b = 0; b < q; ++b) {
+        const double r = g.C[k + (int64_t)(j0 + b) * m];
+        for (int a = 0; a < p; ++a) {
+          s1[a + 2 * b] -= g.A[(i0 + a) + (int64_t)k * g.lda] * r;
+          s2[a + 2 * b] -= g.D[(i0 + a) + (int64_t)k * g.ldd] * r;
+        }
+      }
+    for (int k = lane; k < j0; k += 32)
+      for (int a = 0; a < p; ++a) {
+        const double l = g.F[(i0 + a) + (int64_t)k * m];
+        for (int b = 0; b < q; ++b) {
+          s1[a + 2 * b] += l * g.B[k + (int64_t)(j0 + b) * g.ldb];
+          s2[a + 2 * b] += l * g.E[k + (int64_t)(j0 + b) * g.lde];
+        }
+      }
+  } else {
+    // rows above (solved R, L) and columns to the right (solved R, L)
+    for (int k = lane; k < i0; k += 32)
+      for (int b = 0; b < q; ++b) {
+        const double r = g.C[k + (int64_t)(j0 + b) * m], l = g.F[k + (int64_t)(j0 + b) * m];
+        for (int a = 0; a < p; ++a)
+          s1[a + 2 * b] -= g.A[k + (int64_t)(i0 + a) * g.lda] * r + g.D[k + (int64_t)(i0 + a) * g.ldd] * l;
+      }
+    for (int k = j0 + q + lane; k < n; k += 32)
+      for (int a = 0; a < p; ++a) {
+        const double r = g.C[(i0 + a) + (int64_t)k * m], l = g.F[(i0 + a) + (int64_t)k * m];
+        for (int b = 0; b < q; ++b)
+          s2[a + 2 * b] -= r * g.B[(j0 + b) + (int64_t)k * g.ldb] + l * g.E[(j0 + b) + (int64_t)k * g.lde];
+      }
+  }
+#pragma unroll
+  for (int e = 0; e < 4; ++e)
+    for (int o = 16; o; o >>= 1) {
+      s1[e] += __shfl_xor_sync(0xffffffffu, s1[e], o);
+      s2[e] += __shfl_xor_sync(0xffffffffu, s2[e], o);
+    }
+  if (lane != 0) return;
+  double ce[4], fe[4];
+  for (int b = 0; b < q; ++b)
+    for (int a = 0; a < p; ++a) {
+      const double c0 = g.C[(i0 + a) + (int64_t)(j0 + b) * m], f0 = g.F[(i0 + a) + (int64_t)(j0 + b) * m];
+      ce[a + 2 * b] = c0 + s1[a + 2 * b];
+      fe[a + 2 * b] = (g.trans ? -f0 : f0) + s2[a + 2 * b];
+    }
+  if (p == 1 && q == 1) sylv_gen_solve<1, 1>(g, i0, j0, ce, fe);
+  else if (p == 1) sylv_gen_solve<1, 2>(g, i0, j0, ce, fe);
+  else if (q == 1) sylv_gen_solve<2, 1>(g, i0, j0, ce, fe);
+  else sylv_gen_solve<2, 2>(g, i0, j0, ce, fe);
+}
+
 struct DevMem {
   void* p = nullptr;
   ~DevMem() {
@@ -314,6 +457,62 @@ void add_job(UpdBatch& B, double* M, int64_t ld, int r0, int c0, int len, const 
   UpdJob& j = B.job[B.njobs++];
   j.M = M; j.ld = ld; j.r0 = r0; j.c0 = c0; j.len = len; j.W = W; j.ldw = k; j.k = k;
   j.tiles = (len + update_tile(k) - 1) / update_tile(k);
+}
+
+// Difu and Difl of the reordered pencil by the 1-norm estimates of DTGSEN
+// IJOB 3/5: Difu = 1 / est(Zu^-1), Zu the Sylvester operator of (S11, T11)
+// and (S22, T22); Difl the same with the blocks exchanged.  b1/b2: the
+// diagonal blocks of S11 and of S22 (starts relative to their block, then
+// sizes).
+cudaError_t dif_estimates(cudaStream_t st, const double* S, int64_t lds, const double* T, int64_t ldt, int m1,
+                          int m2, const std::vector<int>& b1s, const std::vector<int>& b1z,
+                          const std::vector<int>& b2s, const std::vector<int>& b2z, double* dif) {
+  const int n1 = (int)b1s.size(), n2 = (int)b2s.size();
+  const size_t mn = (size_t)m1 * m2;
+  DevMem mem;
+  cudaError_t e = cudaMalloc(&mem.p, 2 * mn * sizeof(double) + 2 * (size_t)(n1 + n2) * sizeof(int));
+  if (e != cudaSuccess) return e;
+  double* X = (double*)mem.p;
+  int* dbl = (int*)(X + 2 * mn);
+  std::vector<int> hb;
+  hb.insert(hb.end(), b1s.begin(), b1s.end());
+  hb.insert(hb.end(), b1z.begin(), b1z.end());
+  hb.insert(hb.end(), b2s.begin(), b2s.end());
+  hb.insert(hb.end(), b2z.begin(), b2z.end());
+  e = cudaMemcpyAsync(dbl, hb.data(), hb.size() * sizeof(int), cudaMemcpyHostToDevice, st);
+  if (e != cudaSuccess) return e;
+  const double* S22 = S + m1 + (int64_t)m1 * lds;
+  const double* T22 = T + m1 + (int64_t)m1 * ldt;
+  for (int which = 0; which < 2; ++which) {
+    SylvGen g;
+    if (which == 0) {
+      g.A = S; g.D = T; g.B = S22; g.E = T22; g.m = m1; g.n = m2;
+      g.as = dbl; g.az = dbl + n1; g.bs = dbl + 2 * n1; g.bz = dbl + 2 * n1 + n2; g.na = n1; g.nb = n2;
+    } else {
+      g.A = S22; g.D = T22; g.B = S; g.E = T; g.m = m2; g.n = m1;
+      g.as = dbl + 2 * n1; g.az = dbl + 2 * n1 + n2; g.bs = dbl; g.bz = dbl + n1; g.na = n2; g.nb = n1;
+    }
+    g.lda = g.ldb = lds;
+    g.ldd = g.lde = ldt;
+    g.C = X;
+    g.F = X + mn;
+    auto apply = [&](int kind, std::vector<double>& x) {
+      g.trans = kind == 2 ? 1 : 0;
+      if (cudaMemcpyAsync(X, x.data(), 2 * mn * sizeof(double), cudaMemcpyHostToDevice, st) != cudaSuccess)
+        return false;
+      const int waves = g.na + g.nb - 1, width = g.na < g.nb ? g.na : g.nb;
+      for (int d = 0; d < waves; ++d) k_sylv_gen_wave<<<(width + 7) / 8, 256, 0, st>>>(g, d);
+      if (cudaGetLastError() != cudaSuccess) return false;
+      if (cudaMemcpyAsync(x.data(), X, 2 * mn * sizeof(double), cudaMemcpyDeviceToHost, st) != cudaSuccess)
+        return false;
+      return cudaStreamSynchronize(st) == cudaSuccess;
+    };
+    bool ok = true;
+    const double est = onenorm_est((int)(2 * mn), apply, ok);
+    if (!ok) return cudaErrorUnknown;
+    dif[which] = 1.0 / est;
+  }
+  return cudaSuccess;
 }
 
 }  // namespace
@@ -419,7 +618,7 @@ cudaError_t tgsen_device(cudaStream_t st, int ijob, bool wantq, bool wantz, cons
     return cudaStreamSynchronize(st);
   }
   const int m1 = out->m, m2 = n - out->m;
-  if (ijob >= 1 && m1 > 0 && m2 > 0) {
+  if ((ijob == 1 || ijob == 5) && m1 > 0 && m2 > 0) {
     // diagonal blocks of S11 and S22 (the selected blocks lead)
     std::vector<int> blk(2 * (size_t)nb);
     int nb1 = 0, nb2 = 0;
@@ -469,6 +668,30 @@ cudaError_t tgsen_device(cudaStream_t st, int ijob, bool wantq, bool wantz, cons
     if (e != cudaSuccess) return e;
     out->pl = 1.0 / sqrt(1.0 + hn[0]);
     out->pr = 1.0 / sqrt(1.0 + hn[1]);
+  }
+  if (ijob == 3 || ijob == 5) {
+    if (m1 == 0 || m2 == 0) {
+      // nothing to separate: both estimates are ||(S, T)||_F, as DTGSEN sets them
+      DevMem nm;
+      e = cudaMalloc(&nm.p, (592 + 2) * sizeof(double));
+      if (e != cudaSuccess) return e;
+      double* part = (double*)nm.p;
+      launch_sumsq(st, S, lds, 0, n, part + 592, part);
+      launch_sumsq(st, T, ldt, 0, n, part + 593, part);
+      double hn[2];
+      e = cudaMemcpyAsync(hn, part + 592, sizeof(hn), cudaMemcpyDeviceToHost, st);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+      if (e != cudaSuccess) return e;
+      out->dif[0] = out->dif[1] = sqrt(hn[0] + hn[1]);
+    } else {
+      std::vector<int> b1s, b1z, b2s, b2z;
+      for (int k = 0, p = 0; k < nb; p += sz[k], ++k) {
+        if (p < m1) { b1s.push_back(p); b1z.push_back(sz[k]); }
+        else { b2s.push_back(p - m1); b2z.push_back(sz[k]); }
+      }
+      e = dif_estimates(st, S, lds, T, ldt, m1, m2, b1s, b1z, b2s, b2z, out->dif);
+      if (e != cudaSuccess) return e;
+    }
   }
   return cudaStreamSynchronize(st);
 }

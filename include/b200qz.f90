@@ -85,7 +85,7 @@ module b200qz
        real(c_double), intent(inout) :: a(lda, *), b(ldb, *), q(ldq, *), z(ldz, *)
      end function b200qz_gghrd_host
      integer(c_int) function b200qz_tgsen_host(ctx, ijob, wantq, wantz, select, n, s, lds, t, ldt, q, ldq, &
-          z, ldz, alphar, alphai, beta, m, pl, pr, info) bind(C, name="b200qz_tgsen_host")
+          z, ldz, alphar, alphai, beta, m, pl, pr, dif, info) bind(C, name="b200qz_tgsen_host")
        import :: c_int, c_double, c_ptr
        type(c_ptr), value :: ctx
        integer(c_int), value :: ijob, wantq, wantz, n, lds, ldt, ldq, ldz
@@ -94,6 +94,7 @@ module b200qz
        real(c_double), intent(out) :: alphar(*), alphai(*), beta(*)
        integer(c_int), intent(out) :: m, info
        real(c_double), intent(out) :: pl, pr
+       real(c_double), intent(out) :: dif(2)
      end function b200qz_tgsen_host
   end interface
 end module b200qz

@@ -308,28 +308,33 @@ int b200qz_ggbak_host(b200qz_ctx* ctx, char job, char side, int n, int ilo, int 
  * solve returns it) and its Schur vectors so that the eigenvalues
  * flagged in select (host array of n ints; a 2x2 block moves when either
  * of its flags is set) lead, with the semantics of LAPACK DTGSEN for
- * IJOB 0 and 1 (the role of the reference's PDTGSEN / PDTGORD,
+ * IJOB 0, 1, 3 and 5 (the role of the reference's PDTGSEN / PDTGORD,
  * src/reorder/PDTGSEN.f:1, PDTGORD.f:1).  Selected blocks move up by
  * adjacent block swaps inside windows of up to 80 rows on one CTA; the
  * windows' orthogonal factors are applied to the rest of S, T, Q, Z on the
  * tensor cores.  1x1 blocks with a negative T entry then have their rows
  * of S and T and column of Q negated.  alphar/alphai/beta receive the
  * reordered eigenvalues; m the dimension of the selected deflating
- * subspaces; for ijob = 1, pl/pr the reciprocal norms of the projections
- * onto the left/right deflating subspaces (from the generalized Sylvester
- * equation S11 R - L S22 = S12, T11 R - L T22 = T12), else 1.  info = 1
- * when a swap was rejected (the pair is then partly reordered).  ijob 2..5
- * (the Dif estimates) are not provided (-1).  The _dev form takes device
+ * subspaces; for ijob = 1 and 5, pl/pr the reciprocal norms of the
+ * projections onto the left/right deflating subspaces (from the
+ * generalized Sylvester equation S11 R - L S22 = S12, T11 R - L T22 =
+ * T12), else 1; for ijob = 3 and 5, dif[0..1] the 1-norm estimates of
+ * Difu and Difl (DTGSEN's DIF: the separations of (S11, T11) and
+ * (S22, T22), from Higham's 1-norm estimator over generalized Sylvester
+ * solves and their transposes; ||(S, T)||_F when m is 0 or n), else dif
+ * (may be NULL) is not written.  info = 1 when a swap was rejected (the
+ * pair is then partly reordered).  ijob 2 and 4 (the Frobenius-norm Dif
+ * estimates) are not provided (-1).  The _dev form takes device
  * arrays (alphar/alphai/beta on the device too), the _host form host
  * arrays; counts (may be NULL) receives {swaps, windows}.  Returns 0;
  * -1 ijob, -5 n, -7 lds, -9 ldt, -14 ldq, -16 ldz (DTGSEN's argument
  * positions); 10001 on a CUDA error. */
 int b200qz_tgsen_dev(b200qz_ctx* ctx, int ijob, int wantq, int wantz, const int* select, int n, double* s, int lds,
                      double* t, int ldt, double* q, int ldq, double* z, int ldz, double* alphar, double* alphai,
-                     double* beta, int* m, double* pl, double* pr, int* info, int* counts);
+                     double* beta, int* m, double* pl, double* pr, double* dif, int* info, int* counts);
 int b200qz_tgsen_host(b200qz_ctx* ctx, int ijob, int wantq, int wantz, const int* select, int n, double* s, int lds,
                       double* t, int ldt, double* q, int ldq, double* z, int ldz, double* alphar, double* alphai,
-                      double* beta, int* m, double* pl, double* pr, int* info);
+                      double* beta, int* m, double* pl, double* pr, double* dif, int* info);
 
 /* Hessenberg-triangular reduction (LAPACK DGGHRD semantics; replaces the
  * reference's PDGGHRD, src/ab2ht/PDGGHRD.f:13, the step before the solve

@@ -17,6 +17,7 @@
 
 #include "../gevp-pdhgeqz_b200/csrc/qz_solver.h"
 #include "../gevp-pdhgeqz_b200/csrc/hessred.cuh"
+#include "../gevp-pdhgeqz_b200/csrc/onenorm.h"
 
 using namespace qz;
 
@@ -461,6 +462,23 @@ int host_gghrd(int n, int ilo, int ihi, double* A, double* B, double* Q, double*
 // The reduction's Givens rotation (hessred.cuh hr_lartg) for a test
 // against LAPACK's DLARTG convention.
 void host_hr_lartg(double f, double g, double* out) { hr_lartg(f, g, out[0], out[1], out[2]); }
+
+// The 1-norm estimator of DTGSEN's Dif (onenorm.h) on an explicit
+// column-major n x n matrix M: the estimate of ||M||_1.
+double host_onenorm_est(int n, const double* M) {
+  auto apply = [&](int kind, std::vector<double>& x) {
+    std::vector<double> y(n, 0.0);
+    for (int j = 0; j < n; ++j)
+      for (int i = 0; i < n; ++i) {
+        if (kind == 1) y[i] += M[i + (size_t)j * n] * x[j];
+        else y[j] += M[i + (size_t)j * n] * x[i];
+      }
+    x = y;
+    return true;
+  };
+  bool ok = true;
+  return onenorm_est(n, apply, ok);
+}
 
 }  // extern "C"
 

@@ -41,6 +41,8 @@ def host(tmp_path_factory):
     L.host_gghrd.restype = ctypes.c_int
     L.host_hr_lartg.argtypes = [ctypes.c_double, ctypes.c_double, _pd]
     L.host_hr_lartg.restype = None
+    L.host_onenorm_est.argtypes = [ctypes.c_int, _pd]
+    L.host_onenorm_est.restype = ctypes.c_double
     L.host_set_pipe.argtypes = [ctypes.c_int]
     L.host_set_pipe.restype = None
     L.host_pipe_far_done.restype = ctypes.c_int
@@ -484,3 +486,37 @@ def test_host_hr_lartg_matches_dlartg(host):
             assert np.allclose(out, [c, s, r], rtol=4e-16, atol=0.0), (f, g, out, (c, s, r))
             if f == 0.0 or g == 0.0:
                 assert tuple(out) == (c, s, r), (f, g, out, (c, s, r))
+
+
+def _dlacn2_estimate(lapack, M):
+    """LAPACK DLACN2 by reverse communication on an explicit matrix."""
+    n = M.shape[0]
+    v = np.zeros(n)
+    x = np.zeros(n)
+    isgn = np.zeros(n, dtype=np.int32)
+    isave = np.zeros(3, dtype=np.int32)
+    est = ctypes.c_double(0.0)
+    kase = ctypes.c_int(0)
+    nn = ctypes.c_int(n)
+    f = lapack.lib().scipy_dlacn2_
+    while True:
+        f(ctypes.byref(nn), _p(v), _p(x), isgn.ctypes.data_as(_pi), ctypes.byref(est), ctypes.byref(kase),
+          isave.ctypes.data_as(_pi))
+        if kase.value == 0:
+            return est.value
+        x[:] = M @ x if kase.value == 1 else M.T @ x
+
+
+@pytest.mark.parametrize("n,seed", [(1, 1), (2, 2), (7, 3), (40, 4), (120, 5)])
+def test_host_onenorm_estimator_matches_dlacn2(host, lapack, n, seed):
+    """The host restatement of the 1-norm estimator behind DTGSEN's Dif
+    (onenorm.h) takes LAPACK DLACN2's steps: the same estimate on explicit
+    matrices, random and with a dominant column, a lower bound of the true
+    1-norm."""
+    rng = np.random.default_rng(seed)
+    for M in (rng.standard_normal((n, n)), np.linalg.inv(np.triu(rng.standard_normal((n, n))) + 3 * np.eye(n))):
+        M = np.array(M, order="F")
+        mine = host.host_onenorm_est(n, _p(M))
+        ref = _dlacn2_estimate(lapack, M)
+        assert abs(mine - ref) <= 1e-12 * ref, (mine, ref)
+        assert mine <= np.abs(M).sum(axis=0).max() * (1 + 1e-12)

@@ -4,7 +4,8 @@ against LAPACK DTGSEN on the same Schur form: the same dimension m, the
 selected eigenvalues leading in the same order, the same deflating
 subspaces (principal angles), backward errors and orthogonality within
 50 n eps of the original pencil, Schur structure with non-negative 1x1
-T entries, and the projection norms PL, PR (IJOB = 1)."""
+T entries, the projection norms PL, PR (IJOB = 1, 5) and the 1-norm Dif
+estimates (IJOB = 3, 5)."""
 import numpy as np
 import pytest
 
@@ -128,11 +129,53 @@ def test_tgsen_argument_errors(solver, pkg):
     def call(ijob, n, lds, ldt, ldq, ldz):
         return L.b200qz_tgsen_host(solver.handle, ijob, 1, 1, sel.ctypes.data_as(pkg._pi), n, vp, lds, vp, ldt, vp,
                                    ldq, vp, ldz, pkg._p(v), pkg._p(v), pkg._p(v), pkg.ctypes.byref(m),
-                                   pkg.ctypes.byref(pl), pkg.ctypes.byref(pr), pkg.ctypes.byref(info))
+                                   pkg.ctypes.byref(pl), pkg.ctypes.byref(pr), pkg._p(v), pkg.ctypes.byref(info))
 
     assert call(2, 4, 4, 4, 4, 4) == -1
+    assert call(4, 4, 4, 4, 4, 4) == -1
+    assert call(6, 4, 4, 4, 4, 4) == -1
     assert call(0, -1, 4, 4, 4, 4) == -5
     assert call(0, 4, 3, 4, 4, 4) == -7
     assert call(0, 4, 4, 3, 4, 4) == -9
     assert call(0, 4, 4, 4, 3, 4) == -14
     assert call(0, 4, 4, 4, 4, 3) == -16
+
+
+@pytest.mark.parametrize("n,seed,rule,ijob", [(12, 21, "small", 3), (40, 22, "random", 5), (14, 4, "small", 5),
+                                               (30, 24, "bottom", 3), (60, 25, "all", 5), (60, 26, "none", 3)])
+def test_tgsen_dif_estimates(solver, lapack, pkg, n, seed, rule, ijob):
+    """Difu and Difl by Higham's 1-norm estimator over generalized Sylvester
+    solves and their transposes (DTGSEN IJOB 3 and 5).  The estimator is
+    LAPACK DLACN2's (pinned by the host test against DLACN2 itself); its
+    sign-vector iteration can take another path when a solution entry that
+    is zero in exact arithmetic comes out +0 in one solve and -1e-17 in
+    another, so against LAPACK's DTGSEN the estimates agree within a factor
+    of 3 (exactly in most cases), and each is checked against the true
+    value it estimates: 1/Dif <= ||Z^-1||_1 for the Sylvester operator Z,
+    i.e. the estimate is never below the true 1-norm separation.  With
+    nothing or everything selected DTGSEN returns ||(S, T)||_F, to rounding."""
+    H, T, S, P, Q, Z, ar, ai, be = _schur(lapack, pkg, n, seed)
+    sel = _select(ar, ai, be, rule, seed)
+    La, Lb, lar, lai, lbe, Lq, Lz, lm, lpl, lpr, ldif, linfo = lapack.dtgsen(S, P, Q, Z, sel, ijob=ijob)
+    assert linfo == 0
+    Gs, Gt, Gq, Gz = (np.array(M, order="F", copy=True) for M in (S, P, Q, Z))
+    dif = np.zeros(2)
+    gar, gai, gbe, m, pl, pr, info, ret = solver.tgsen(Gs, Gt, Gq, Gz, sel, ijob=ijob, dif=dif)
+    assert ret == 0 and info == 0 and m == lm
+    if m == 0 or m == n:
+        assert np.allclose(dif, ldif, rtol=1e-12), (dif, ldif)
+        return
+    assert np.all(dif > 0)
+    assert np.all(dif >= ldif / 3) and np.all(dif <= 3 * ldif), (dif, ldif)
+
+    def op(A, D, B, E):
+        p_, q_ = A.shape[0], B.shape[0]
+        return np.block([[np.kron(np.eye(q_), A), -np.kron(B.T, np.eye(p_))],
+                         [np.kron(np.eye(q_), D), -np.kron(E.T, np.eye(p_))]])
+
+    S11, T11, S22, T22 = Gs[:m, :m], Gt[:m, :m], Gs[m:, m:], Gt[m:, m:]
+    for k, Zop in enumerate((op(S11, T11, S22, T22), op(S22, T22, S11, T11))):
+        true_sep = 1.0 / np.abs(np.linalg.inv(Zop)).sum(axis=0).max()
+        assert dif[k] >= true_sep * (1 - 1e-9), (k, dif[k], true_sep)
+    if ijob == 5:
+        assert abs(pl - lpl) <= 1e-9 * lpl and abs(pr - lpr) <= 1e-9 * lpr
