@@ -57,6 +57,87 @@ __global__ void __launch_bounds__(kHrThreads) k_hr_zero_lower(double* B, int64_t
   }
 }
 
+// Warp walks: the 32 lanes take 32 consecutive rotations of a walk at once.
+// The carried value follows a first-order linear recurrence, carry ->
+// a carry + b per rotation, so the carries of the 32 steps come from one
+// warp scan of the affine maps (five shuffle rounds) instead of 32
+// dependent steps, and the 32 loads of a chunk are in flight together.
+// The results differ from the one-thread walks only by rounding.
+constexpr unsigned kFull = 0xffffffffu;
+
+__device__ void affine_scan(double& a, double& b, int lane) {
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const double ap = __shfl_up_sync(kFull, a, off), bp = __shfl_up_sync(kFull, b, off);
+    if (lane >= off) {
+      b = a * bp + b;
+      a = a * ap;
+    }
+  }
+}
+
+// hr_walk_g by a warp: entries (J-1, J), carry = entry J side.
+__device__ void hr_wwalk_g(double* v, int64_t st, int Jhi, int Jlo, const double* rot, int lane) {
+  double y = v[(int64_t)Jhi * st];
+  for (int J0 = Jhi; J0 >= Jlo; J0 -= 32) {
+    const int J = J0 - lane;
+    const bool act = J >= Jlo;
+    double x = 0.0, c = 1.0, s = 0.0;
+    if (act) {
+      x = v[(int64_t)(J - 1) * st];
+      c = rot[4 * J];
+      s = rot[4 * J + 1];
+    }
+    double a = act ? s : 1.0, b = act ? c * x : 0.0;
+    affine_scan(a, b, lane);
+    const double ynew = a * y + b;
+    double yprev = __shfl_up_sync(kFull, ynew, 1);
+    if (lane == 0) yprev = y;
+    if (act) v[(int64_t)J * st] = -s * x + c * yprev;
+    y = __shfl_sync(kFull, ynew, 31);
+  }
+  if (lane == 0) v[(int64_t)(Jlo - 1) * st] = y;
+}
+
+// hr_walk_z by a warp: columns (J, J-1), carry = column J side.
+__device__ void hr_wwalk_z(double* row, int64_t st, int Jhi, int Jlo, const double* rot, int lane) {
+  double x = row[(int64_t)Jhi * st];
+  for (int J0 = Jhi; J0 >= Jlo; J0 -= 32) {
+    const int J = J0 - lane;
+    const bool act = J >= Jlo;
+    double y = 0.0, cz = 1.0, sz = 0.0;
+    if (act) {
+      y = row[(int64_t)(J - 1) * st];
+      cz = rot[4 * J + 2];
+      sz = rot[4 * J + 3];
+    }
+    double a = act ? -sz : 1.0, b = act ? cz * y : 0.0;
+    affine_scan(a, b, lane);
+    const double xnew = a * x + b;
+    double xprev = __shfl_up_sync(kFull, xnew, 1);
+    if (lane == 0) xprev = x;
+    if (act) row[(int64_t)J * st] = cz * xprev + sz * y;
+    x = __shfl_sync(kFull, xnew, 31);
+  }
+  if (lane == 0) row[(int64_t)(Jlo - 1) * st] = x;
+}
+
+// hr_col_item with a warp per item (the column-end walks are long: the
+// scan's 32 steps per round trip matter more there than the number of
+// walks in flight).
+__device__ void hr_col_item_w(const HrArgs& a, int i, int jc, int lane) {
+  const int na = a.n - 1 - jc, nq = a.wantq ? a.n : 0;
+  if (i < na) {
+    hr_wwalk_g(a.A + (int64_t)(jc + 1 + i) * a.lda, 1, a.ihi, jc + 2, a.rot, lane);
+  } else if (i < na + nq) {
+    const int r = i - na;
+    if (a.qrows) hr_wwalk_g(a.Q + (int64_t)r * a.ldq, 1, a.ihi, jc + 2, a.rot, lane);
+    else hr_wwalk_g(a.Q + r, a.ldq, a.ihi, jc + 2, a.rot, lane);
+  } else {
+    hr_wwalk_z(a.Z + (i - na - nq), a.ldz, a.ihi, jc + 2, a.rot, lane);
+  }
+}
+
 // CTA 0 of a window launch: window (lo, hi) of column jc, previous window
 // (plo, phi) of the column (plo < 0: none).
 __device__ void hr_window_cta(const HrArgs& a, int jc, int lo, int hi, int plo, int phi, double* sm, int wmax) {
@@ -110,6 +191,8 @@ __device__ void hr_window_cta(const HrArgs& a, int jc, int lo, int hi, int plo, 
 __global__ void __launch_bounds__(kHrThreads) k_hr_win(HrArgs a, int jc, int lo, int hi, int plo, int phi, int wmax) {
   extern __shared__ double sm[];
   if (blockIdx.x > 0) {
+    // short walks (one window): a thread per walk keeps the most of them in
+    // flight on CTAs that carry the window's shared memory
     const int e_end = lo - 1, items = hr_win_items(a, e_end, phi);
     for (int i = (blockIdx.x - 1) * blockDim.x + threadIdx.x; i < items; i += (gridDim.x - 1) * blockDim.x)
       hr_win_item(a, i, e_end, plo, phi);
@@ -128,11 +211,14 @@ __global__ void __launch_bounds__(kHrThreads) k_hr_flush(HrArgs a, int plo, int 
 
 // Column jc's G on A (columns jc+1..n-1) and both factors on Q, Z.
 __global__ void __launch_bounds__(kHrThreads) k_hr_colend(HrArgs a, int jc) {
-  const int items = hr_col_items(a, jc);
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < items; i += gridDim.x * blockDim.x) hr_col_item(a, i, jc);
+  const int items = hr_col_items(a, jc), wpb = blockDim.x >> 5;
+  for (int i = blockIdx.x * wpb + (threadIdx.x >> 5); i < items; i += gridDim.x * wpb)
+    hr_col_item_w(a, i, jc, threadIdx.x & 31);
 }
 
 int blocks_for(int items) { return std::max(1, (items + kHrThreads - 1) / kHrThreads); }
+// a warp per walk item
+int warp_blocks_for(int items) { return std::max(1, (items + kHrThreads / 32 - 1) / (kHrThreads / 32)); }
 
 }  // namespace
 
@@ -170,7 +256,7 @@ cudaError_t gghrd_device(cudaStream_t st, int icompq, int icompz, bool qrows, in
       hi = lo - 1;
     }
     k_hr_flush<<<blocks_for(hr_win_items(a, plo - 1, phi)), kHrThreads, 0, st>>>(a, plo, phi);
-    k_hr_colend<<<blocks_for(hr_col_items(a, jc)), kHrThreads, 0, st>>>(a, jc);
+    k_hr_colend<<<warp_blocks_for(hr_col_items(a, jc)), kHrThreads, 0, st>>>(a, jc);
     launches += 2;
     e = cudaGetLastError();
   }
