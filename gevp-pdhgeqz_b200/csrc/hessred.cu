@@ -122,9 +122,15 @@ __device__ void hr_wwalk_z(double* row, int64_t st, int Jhi, int Jlo, const doub
   if (lane == 0) row[(int64_t)(Jlo - 1) * st] = x;
 }
 
-// hr_col_item with a warp per item (the column-end walks are long: the
-// scan's 32 steps per round trip matter more there than the number of
-// walks in flight).
+// hr_win_item / hr_col_item with a warp per item, for the launches without
+// shared memory (the last window's walks and the column-end walks), where
+// every walk can have its own warp resident.
+__device__ void hr_win_item_w(const HrArgs& a, int i, int e_end, int plo, int phi, int lane) {
+  const int nf = a.n - 1 - phi;
+  if (i < e_end) hr_wwalk_z(a.B + i, a.ldb, phi, plo, a.rot, lane);
+  else if (i < e_end + nf) hr_wwalk_g(a.B + (int64_t)(phi + 1 + i - e_end) * a.ldb, 1, phi, plo, a.rot, lane);
+  else hr_wwalk_z(a.A + (i - e_end - nf), a.lda, phi, plo, a.rot, lane);
+}
 __device__ void hr_col_item_w(const HrArgs& a, int i, int jc, int lane) {
   const int na = a.n - 1 - jc, nq = a.wantq ? a.n : 0;
   if (i < na) {
@@ -204,9 +210,9 @@ __global__ void __launch_bounds__(kHrThreads) k_hr_win(HrArgs a, int jc, int lo,
 // The walks of column jc's last window (plo, phi): rows above it in B,
 // columns right of it in B, rows of A.
 __global__ void __launch_bounds__(kHrThreads) k_hr_flush(HrArgs a, int plo, int phi) {
-  const int e_end = plo - 1, items = hr_win_items(a, e_end, phi);
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < items; i += gridDim.x * blockDim.x)
-    hr_win_item(a, i, e_end, plo, phi);
+  const int e_end = plo - 1, items = hr_win_items(a, e_end, phi), wpb = blockDim.x >> 5;
+  for (int i = blockIdx.x * wpb + (threadIdx.x >> 5); i < items; i += gridDim.x * wpb)
+    hr_win_item_w(a, i, e_end, plo, phi, threadIdx.x & 31);
 }
 
 // Column jc's G on A (columns jc+1..n-1) and both factors on Q, Z.
@@ -255,7 +261,7 @@ cudaError_t gghrd_device(cudaStream_t st, int icompq, int icompz, bool qrows, in
       phi = hi;
       hi = lo - 1;
     }
-    k_hr_flush<<<blocks_for(hr_win_items(a, plo - 1, phi)), kHrThreads, 0, st>>>(a, plo, phi);
+    k_hr_flush<<<warp_blocks_for(hr_win_items(a, plo - 1, phi)), kHrThreads, 0, st>>>(a, plo, phi);
     k_hr_colend<<<warp_blocks_for(hr_col_items(a, jc)), kHrThreads, 0, st>>>(a, jc);
     launches += 2;
     e = cudaGetLastError();
