@@ -268,8 +268,24 @@ QZ_HD void cta_hr_zchain(X& x, double* Tw, int ldw, int m, double* gbuf, const i
         double cz, sz, rz;
         const double u10 = -s * t00, u11 = -s * t01 + c * t11;
         double u00 = c * t00, u01 = c * t01 + s * t11;
-        hr_lartg(u11, u10, cz, sz, rz);
-        rot2(cz, sz, u01, u00);
+        const double af = fabs(u11), ag = fabs(u10), mx = af > ag ? af : ag;
+        if (u10 != 0.0 && u11 != 0.0 && mx > kSafeLo && mx < kSafeHi) {
+          // the column rotation and its action on row J-1 of the block:
+          // cz u01 + sz u00 = sg (u11 u01 + u10 u00) / d and -sz u01 + cz u00
+          // = sg (u11 u00 - u10 u01) / d, whose numerators are formed while
+          // the reciprocal square root of d^2 runs
+          const double q = u11 * u11 + u10 * u10;
+          const double n0 = u11 * u00 - u10 * u01, n1 = u11 * u01 + u10 * u00;
+          const double inv = hr_rsqrt(q), si = (u11 < 0.0 ? -inv : inv);
+          cz = af * inv;
+          sz = u10 * si;
+          rz = q * si;
+          u00 = n0 * si;
+          u01 = n1 * si;
+        } else {
+          hr_lartg(u11, u10, cz, sz, rz);
+          rot2(cz, sz, u01, u00);
+        }
         pcz = cz; psz = sz; pt00 = u00; pt01 = u01; prz = rz;
         double* sl = slot + 4 * (k & 1);
         sl[0] = c; sl[1] = s; sl[2] = cz; sl[3] = sz;
