@@ -57,6 +57,44 @@ def test_pdhgeqz_argument_errors_need_no_gpu(pkg):
     assert np.array_equal(H, H0)
 
 
+def test_pdgghrd_argument_errors_need_no_gpu(pkg):
+    """The PDGGHRD drop-in's quick return, workspace query and argument
+    checks (src/ab2ht/PDGGHRD.f:198, 243-250, 278-296) run before any
+    device work."""
+    import ctypes
+    import numpy as np
+    n, nb = 6, 4
+    A = np.array(np.arange(n * n, dtype=np.float64).reshape(n, n), order="F")
+    A0 = A.copy()
+    d = pkg.descriptor(n, nb, n)
+    dp = d.ctypes.data_as(pkg._pi)
+    work = np.zeros(nb)
+    L = pkg.lib()
+
+    def call(cq, cz, nn, ilo, ihi, desca, lwork):
+        info = ctypes.c_int(99)
+        L.pdgghrd_(cq, cz, pkg._ip(nn), pkg._ip(ilo), pkg._ip(ihi), pkg._vp(A.ctypes.data),
+                   desca.ctypes.data_as(pkg._pi), pkg._vp(A.ctypes.data), dp, pkg._vp(A.ctypes.data), dp,
+                   pkg._vp(A.ctypes.data), dp, pkg._p(work), ctypes.byref(ctypes.c_int(lwork)), ctypes.byref(info),
+                   1, 1)
+        return info.value
+
+    # N <= 1: returns before any check
+    assert call(b"X", b"X", 1, 1, 1, d, 0) == 0
+    # workspace query: DESCA(MB_) in WORK(1)
+    assert call(b"I", b"I", n, 1, n, d, -1) == 0 and work[0] == nb
+    assert call(b"X", b"I", n, 1, n, d, nb) == -1
+    assert call(b"I", b"X", n, 1, n, d, nb) == -2
+    assert call(b"I", b"I", n, 0, n, d, nb) == -4
+    assert call(b"I", b"I", n, 1, n + 1, d, nb) == -5
+    assert call(b"I", b"I", n, 3, 1, d, nb) == -5
+    bad = d.copy()
+    bad[4] = nb + 1
+    assert call(b"I", b"I", n, 1, n, bad, nb) == -6
+    assert call(b"I", b"I", n, 1, n, d, nb - 1) == -7
+    assert np.array_equal(A, A0)
+
+
 def test_header_compiles_as_c99_and_links(tmp_path, pkg):
     """include/b200qz.h is plain C: a C99 program (pedantic, warnings as
     errors) includes it, links libb200qz.so and calls an entry point that
