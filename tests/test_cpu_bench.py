@@ -54,6 +54,14 @@ def test_reference_arm_batched():
     assert d["unit"] == "pencils/s" and d["higher_is_better"] is True and d["value"] > 0
 
 
+def test_reference_arm_of_the_steps_beside_the_solve():
+    """The balancing, reordering and HT-reduction workloads time LAPACK in
+    their own line (cpu_baseline); their reference arm says so and exits 0."""
+    for w in ("ggbal", "tgsen", "gghrd"):
+        d = _run(["--impl", "reference", "--workload", w, "--steps", "1", "--warmup", "0"], timeout=120)
+        assert d["impl"] == "reference" and "unavailable" in d and "LAPACK" in d["unavailable"]
+
+
 def test_cpu_baseline_sample_is_bounded_and_scaled(pkg, monkeypatch):
     """The bounded sample stops the port after K AEDs of the real pencil
     and divides by the share those AEDs took in the committed profile."""

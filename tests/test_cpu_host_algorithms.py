@@ -520,3 +520,21 @@ def test_host_onenorm_estimator_matches_dlacn2(host, lapack, n, seed):
         ref = _dlacn2_estimate(lapack, M)
         assert abs(mine - ref) <= 1e-12 * ref, (mine, ref)
         assert mine <= np.abs(M).sum(axis=0).max() * (1 + 1e-12)
+
+
+@pytest.mark.parametrize("n,ilo,ihi,W", [(2, 0, 1, 2), (3, 0, 2, 160), (9, 0, 8, 160), (9, 3, 3, 4), (9, 3, 4, 4),
+                                          (9, 2, 5, 2), (33, 0, 32, 31), (33, 0, 32, 32)])
+def test_host_gghrd_edge_cases(host, lapack, n, ilo, ihi, W):
+    """Windows longer than a column, windows of two pairs, a column that
+    exactly fills or just overflows a window, and ILO/IHI ranges with no
+    column or one column to reduce: the same H, T, Q, Z as DGGHRD."""
+    rng = np.random.default_rng(1000 + n + ilo + ihi + W)
+    A = np.triu(rng.standard_normal((n, n)))
+    A[ilo:ihi + 1, ilo:ihi + 1] = rng.standard_normal((ihi - ilo + 1,) * 2)
+    B = np.triu(rng.standard_normal((n, n)))
+    H, T, Q, Z = _host_gghrd(host, A, B, ilo, ihi, W, 0)
+    H0, T0, Q0, Z0, info = lapack.dgghrd(A, B, "I", "I", ilo + 1, ihi + 1)
+    assert info == 0
+    for X, X0 in ((H, H0), (T, T0), (Q, Q0), (Z, Z0)):
+        assert np.abs(X - X0).max() <= 1e-12 * max(1.0, np.abs(X0).max())
+    assert not np.any(np.tril(H, -2)) and not np.any(np.tril(T, -1))
