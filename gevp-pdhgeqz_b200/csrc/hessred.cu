@@ -6,10 +6,12 @@
 // its own diagonal block holds (walk (a)), then loads the block and runs
 // the chain; the other CTAs of the launch apply the previous window's
 // rotations elsewhere (walks (e), (f), (g)), on entries CTA 0 does not
-// touch.  After the column's last window, one launch applies that window's
-// walks and one applies the column's G rotations to A (columns jc+1..n-1)
-// and both factors to Q and Z.  The rotations of a column are kept in a
-// 4n-double array indexed by pair.
+// touch (a thread per walk: these CTAs carry the block's shared memory, so
+// one fits per SM).  After the column's last window, one launch applies
+// that window's walks and one applies the column's G rotations to A
+// (columns jc+1..n-1) and both factors to Q and Z, a warp per walk (32
+// rotations per affine scan of the carried value).  The rotations of a
+// column are kept in a 4n-double array indexed by pair.
 //
 // Bounds: the chain is a dependent sequence of two rotations per pair on
 // one SM (about n^2/2 pairs); the walks stream each touched entry once per
