@@ -11,6 +11,12 @@
  * S quasi upper triangular with standardised 2x2 blocks, P upper
  * triangular with non-negative diagonal (2x2 blocks: diagonal, positive),
  * and lambda_j = (ALPHAR(j) + i*ALPHAI(j)) / BETA(j).
+ *
+ * The steps either side of the solve have entries of their own:
+ * balancing (b200qz_ggbal_*, b200qz_ggbak_*; DGGBAL/DGGBAK semantics),
+ * Hessenberg-triangular reduction (b200qz_gghrd_*, DGGHRD semantics, and
+ * the pdgghrd_ drop-in for the reference's PDGGHRD) and reordering of the
+ * Schur form (b200qz_tgsen_*, DTGSEN semantics).
  */
 #ifndef B200QZ_H
 #define B200QZ_H
