@@ -57,3 +57,30 @@ def test_residuals_detect_perturbation(lapack, pkg):
     S[0, 5] += 1e-10
     r = lapack.residuals(H, T, S, P, Q, Z)
     assert r["h"] > 50 * r["neps"]
+
+
+@pytest.mark.parametrize("n", [30, 150])
+def test_lapack_ht_reductions_agree(lapack, n):
+    """The two LAPACK Hessenberg-triangular reductions the tests and the
+    bench use: DGGHRD (the parity oracle of the GPU reduction) and DGGHD3
+    (the blocked form timed as its CPU baseline) both return a
+    Hessenberg-triangular form of the same pencil within 50 n eps, with
+    the same eigenvalues."""
+    rng = np.random.default_rng(n)
+    A = rng.standard_normal((n, n))
+    B = np.triu(rng.standard_normal((n, n)))
+    forms = []
+    for f in (lapack.dgghrd, lapack.dgghd3):
+        H, T, Q, Z, info = f(A, B)
+        assert info == 0
+        assert not np.any(np.tril(H, -2)) and not np.any(np.tril(T, -1))
+        r = lapack.residuals(A, B, H, T, Q, Z)
+        for key in ("h", "t", "q", "z"):
+            assert r[key] <= 50 * r["neps"], (f.__name__, key, r[key] / r["neps"])
+        forms.append((H, T))
+    S0, P0, ar0, ai0, be0, _, _, i0 = lapack.dhgeqz(*forms[0])
+    _, _, ar1, ai1, be1, _, _, i1 = lapack.dhgeqz(*forms[1])
+    assert i0 == 0 and i1 == 0
+    tol = lapack.eig_tolerance(S0, P0, *forms[0])
+    ok, ratio, _ = lapack.match_eigenvalues((ar0, ai0, be0), (ar1, ai1, be1), tol)
+    assert ok, ratio
